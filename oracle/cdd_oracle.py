@@ -1,0 +1,373 @@
+"""CPU oracle for the continuum-dislocation-dynamics time step -- TEST INFRASTRUCTURE ONLY.
+
+This module restates, in vectorised numpy FP64, the reference's Python time-step path of
+mattbierbaum/cuda-plasticity. It is the checker for the CUDA library: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it, and never as
+the thing measured or shipped. The product path (``cdd`` and ``Plasticity`` packages) does not
+import it.
+
+Parity is pinned: ``tests/test_oracle_golden.py`` checks every function here against golden
+vectors in ``tests/golden/*.npz``, which ``tests/golden/make_golden.py`` produced by running the
+reference's own (mechanically Python-3-patched) modules on the same seeded inputs.
+
+Every function follows the operation order of the reference code it cites, so that on the same
+inputs it reproduces the reference to the last bit or within a few ulps.
+
+Layout: a 9-component field is an array ``(9,) + grid`` with components in the reference's
+sorted order xx, xy, xz, yx, yy, yz, zx, zy, zz; grid axis 0 is the reference's x.
+"""
+import numpy as np
+
+ME = np.finfo(float).eps          # Plasticity/NumericalMethods.py L4
+XYZ = "xyz"
+COMPONENTS = [(a, b) for a in XYZ for b in XYZ]   # Fields.py L247-249 (sorted)
+
+
+def ci(i, j):
+    """Index of component (i, j) in the 9-component layout."""
+    return 3 * i + j
+
+
+# ----------------------------------------------------------------------------------------------
+# k-space tables: Plasticity/GridArray/FourierSpaceTools.py L5-59
+# ----------------------------------------------------------------------------------------------
+def _identity(a):
+    """FourierSpaceTools.py L5-7: wrap angles above pi to (-pi, pi]; +pi is kept."""
+    greater = (a > np.pi).astype(float)
+    return a - 2 * np.pi * greater
+
+
+def k_axis(n_scale, n_axis, count):
+    """``n_scale * identity(2 pi i / n_axis)`` for i in [0, count) (FourierSpaceTools.py L29-49)."""
+    i = np.arange(count, dtype=np.float64)
+    return n_scale * _identity(2. * np.pi * i / float(n_axis))
+
+
+def k_tables(shape):
+    """Return (k, kSq, kSqSq, kmask) on the rfft half grid, as in FourierSpaceTools.py L26-55.
+
+    ``k`` is a list of three broadcastable arrays (kx, ky, kz). In 2-D both wave vectors are
+    scaled by ``gridShape[1]`` (L29-30) and kz is zero; in 3-D each axis uses its own size (L47-49).
+    """
+    if len(shape) == 3:
+        n0, n1, n2 = shape
+        kx = k_axis(n0, n0, n0).reshape(n0, 1, 1)
+        ky = k_axis(n1, n1, n1).reshape(1, n1, 1)
+        kz = k_axis(n2, n2, n2 // 2 + 1).reshape(1, 1, n2 // 2 + 1)
+        full = (n0, n1, n2 // 2 + 1)
+        kx, ky, kz = (np.broadcast_to(v, full) for v in (kx, ky, kz))
+        kSq = kx * kx + ky * ky + kz * kz
+        kmask = np.ones(full)
+        kmask[0, 0, 0] = 0.
+    elif len(shape) == 2:
+        n0, n1 = shape
+        kx = k_axis(n1, n0, n0).reshape(n0, 1)
+        ky = k_axis(n1, n1, n1 // 2 + 1).reshape(1, n1 // 2 + 1)
+        full = (n0, n1 // 2 + 1)
+        kx, ky = (np.broadcast_to(v, full) for v in (kx, ky))
+        kz = np.zeros(full)
+        kSq = kx * kx + ky * ky
+        kmask = np.ones(full)
+        kmask[0, 0] = 0.
+    else:
+        raise ValueError("only 2-D and 3-D grids are supported")
+    kSqSq = kSq * kSq
+    return [kx, ky, kz], kSq, kSqSq, kmask
+
+
+# ----------------------------------------------------------------------------------------------
+# Stress: PlasticityState.CalculateSigma(type='k', source='betaE') L85-127 and
+#         PlasticityState.CalculateBetaElastic L357-390
+# ----------------------------------------------------------------------------------------------
+def beta_elastic(beta, mu, nu):
+    shape = beta.shape[1:]
+    axes = tuple(range(-len(shape), 0))
+    KbetaP = np.fft.rfftn(beta, axes=axes)
+    lamb = 2. * mu * nu / (1. - 2 * nu)
+    k, kSq0, kSqSq0, kmask = k_tables(shape)
+    kSq = kSq0 + ME
+    kSqSq = kSqSq0 + ME
+    KbetaE = np.zeros_like(KbetaP)
+    for i in range(3):
+        for j in range(3):
+            acc = np.zeros(KbetaP.shape[1:], dtype=complex)
+            for m in range(3):
+                for n in range(3):
+                    T = lamb / (lamb + 2. * mu) * k[i] * k[j] / kSq * (m == n) + \
+                        k[i] / kSq * ((k[m] * (j == n)) + (k[n] * (j == m))) - \
+                        2. * (lamb + mu) / (lamb + 2. * mu) * (k[i] * k[j] * k[m] * k[n]) / kSqSq
+                    acc += KbetaP[ci(m, n)] * T
+            acc *= kmask
+            KbetaE[ci(i, j)] = acc
+    betaE = np.fft.irfftn(KbetaE, s=shape, axes=axes)
+    return betaE - beta
+
+
+def stress(beta, mu, nu):
+    """Internal stress sigma (9 components, symmetric) of plastic distortion ``beta``."""
+    betaE = beta_elastic(beta, mu, nu)
+    lamb = 2. * mu * nu / (1. - 2. * nu)
+    tr = betaE[0] + betaE[4] + betaE[8]
+    sigma = np.zeros_like(beta)
+    for i in range(3):
+        for j in range(3):
+            sigma[ci(i, j)] += lamb * tr * (i == j) + mu * (betaE[ci(i, j)] + betaE[ci(j, i)])
+    return sigma
+
+
+def applied_stress(t, rate, mu, nu, initial=(0., 0., 0.), t0=0.):
+    """Uniform diagonal stress of an applied strain (RunPython.py L21-26, L44-47).
+
+    ``eps = initial + rate * (t - t0)``; ``sigma_ii += lamb tr(eps) + 2 mu eps_i``. The caller
+    chooses mu, nu (RunPython.py uses module-level 0.5, 0.3; the workloads use the state's).
+    """
+    eps = np.asarray(initial, float) + np.asarray(rate, float) * (t - t0)
+    lamb = 2. * mu * nu / (1. - 2. * nu)
+    tr = eps[0] + eps[1] + eps[2]
+    return np.array([lamb * tr + 2. * mu * eps[i] for i in range(3)])
+
+
+def elastic_energy_density(sigma, mu, nu):
+    """PlasticityState.CalculateElasticEnergy L317-330 (all 81 terms, reference order)."""
+    e = 0.
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                for m in range(3):
+                    S = (2. * (i == k) * (j == m) - (i == m) * (j == k)
+                         - nu * (i == j) * (k == m) / (1. + nu)) / (2. * mu)
+                    e += 0.5 * S * sigma[ci(i, j)] * sigma[ci(k, m)]
+    return e
+
+
+def elastic_energy(beta, mu, nu):
+    """Total elastic energy, summed over cells as Observers/Observer.py L99 does."""
+    return float(np.sum(elastic_energy_density(stress(beta, mu, nu), mu, nu)))
+
+
+def mean_strain_zz(beta):
+    """``numpy.average(betaP[z,z])`` (MattTools/Run/RunLoadingMPI.py L32)."""
+    return float(np.mean(beta[8]))
+
+
+# ----------------------------------------------------------------------------------------------
+# Limited one-sided derivatives: CentralUpwindHJ3D.py L11-34 with NumericalMethods.py L352-473
+# ----------------------------------------------------------------------------------------------
+def minmod3(a, b, c):
+    """NumericalMethods.MinMod3 L367-378 (0/1-mask form)."""
+    cond_a = (a > 0)
+    cond_b = (b > 0)
+    cond_c = (c > 0)
+    cond_ab = (a < b)
+    cond_bc = (b < c)
+    cond_ac = (a < c)
+    cond_abc = cond_a * cond_b * cond_c
+    cond_not_abc = (1 - cond_a) * (1 - cond_b) * (1 - cond_c)
+    return cond_abc * (cond_ab * cond_ac * a + (1 - cond_ab) * cond_bc * b
+                       + (1 - cond_bc) * (1 - cond_ac) * c) + \
+        cond_not_abc * ((1 - cond_ab) * (1 - cond_ac) * a + cond_ab * (1 - cond_bc) * b
+                        + cond_bc * cond_ac * c)
+
+
+THETA = 1.0   # CentralUpwindHJ3D.py L9
+
+
+def find_derivatives(field, axis, Dx):
+    """Return (deriv_p, deriv_m) of every component along grid ``axis`` (L11-34).
+
+    ``field`` has the component axis first; ``axis`` counts grid axes from 0.
+    """
+    ax = axis + 1
+    roll = np.roll
+    diff = roll(field, -1, ax) - field
+    diff2_1 = THETA * (roll(diff, -1, ax) - diff) / Dx / Dx
+    diff2_2 = (roll(diff, -1, ax) - roll(diff, 1, ax)) / Dx / Dx * 0.5
+    diff2_3 = roll(diff2_1, 1, ax)
+    diff2 = minmod3(diff2_1, diff2_2, diff2_3)
+    deriv_p = diff / Dx - 0.5 * Dx * diff2
+    deriv_m = roll(diff, 1, ax) / Dx + 0.5 * Dx * roll(diff2, 1, ax)
+    return deriv_p, deriv_m
+
+
+# ----------------------------------------------------------------------------------------------
+# Beta^P Hamiltonian: CentralUpwindHJBetaPDynamics3D.py L34-212 (2-D twin:
+# CentralUpwindHJBetaPDynamics.py L34-134, identical arithmetic)
+# ----------------------------------------------------------------------------------------------
+def rho_mod(us):
+    """|rho| at a corner from its derivative tensors ``us`` (2 or 3 of them), L34-58."""
+    rho2 = ME
+    for c in range(9):
+        for u in us:
+            rho2 = rho2 + u[c] * u[c]
+    for j in range(3):
+        for d, u in enumerate(us):
+            rho2 = rho2 - u[ci(d, j)] * u[ci(d, j)]
+        if len(us) == 2:
+            rho2 = rho2 - 2 * us[0][ci(1, j)] * us[1][ci(0, j)]
+        else:
+            ux, uy, uz = us
+            rho2 = rho2 - 2 * ux[ci(1, j)] * uy[ci(0, j)]
+            rho2 = rho2 - 2 * uy[ci(2, j)] * uz[ci(1, j)]
+            rho2 = rho2 - 2 * uz[ci(0, j)] * ux[ci(2, j)]
+    return np.sqrt(rho2)
+
+
+def velocity(us, sigma, Lambda):
+    """Dislocation velocity V (3 components) at a corner, L77-142."""
+    shape = us[0].shape[1:]
+    V = [np.zeros(shape), np.zeros(shape), np.zeros(shape)]
+    nd = len(us)
+    for n in range(3):
+        for l in range(3):
+            for d in range(nd):
+                V[l] = V[l] + us[d][ci(l, n)] * sigma[ci(d, n)]
+            for d in range(nd):
+                V[d] = V[d] - us[d][ci(l, n)] * sigma[ci(l, n)]
+    if Lambda != 0:
+        sigma_tr = (sigma[0] + sigma[4] + sigma[8]) / 3. * Lambda
+        for d in range(nd):
+            V[d] = V[d] + sigma_tr * (us[d][0] + us[d][4] + us[d][8])
+        for l in range(3):
+            acc = us[0][ci(l, 0)]
+            for d in range(1, nd):
+                acc = acc + us[d][ci(l, d)]
+            V[l] = V[l] - sigma_tr * acc
+    rho = rho_mod(us)
+    return [v / rho for v in V]
+
+
+def hamiltonian(us, V, Lambda):
+    """H_ij at a corner (L161-201)."""
+    nd = len(us)
+    H = us[0] * V[0]
+    for d in range(1, nd):
+        H = H + us[d] * V[d]
+    for j in range(3):
+        for l in range(3):
+            for i in range(nd):
+                H[ci(i, j)] = H[ci(i, j)] - V[l] * us[i][ci(l, j)]
+    if Lambda != 0:
+        if nd == 3:
+            ux, uy, uz = us
+            J = -Lambda / 3. * (V[0] * (ux[4] + ux[8] - uy[1] - uz[2])
+                                + V[1] * (uy[0] + uy[8] - ux[3] - uz[5])
+                                + V[2] * (uz[0] + uz[4] - ux[6] - uy[7]))
+        else:
+            ux, uy = us
+            J = -Lambda / 3. * (V[0] * (ux[4] + ux[8] - uy[1])
+                                + V[1] * (uy[0] + uy[8] - ux[3])
+                                - V[2] * (ux[6] + uy[7]))
+        for i in range(3):
+            H[ci(i, i)] = H[ci(i, i)] + J
+    return H
+
+
+# ----------------------------------------------------------------------------------------------
+# Central-upwind flux: CentralUpwindHJ3D.CalculateFlux L99-271
+# ----------------------------------------------------------------------------------------------
+def flux(beta, sigma, Lambda=0, Dx=None):
+    """Return (rhs, speed) for plastic distortion ``beta`` under total stress ``sigma``."""
+    shape = beta.shape[1:]
+    nd = len(shape)
+    if Dx is None:
+        Dx = 1. / shape[-1]                       # CentralUpwindHJ3D.py L15-16
+    der = [find_derivatives(beta, a, Dx) for a in range(nd)]   # [(p, m)] per axis
+    if nd == 3:
+        corners = [(sx, sy, sz) for sx in (1, 0) for sy in (1, 0) for sz in (1, 0)]
+    else:
+        corners = [(sx, sy) for sx in (1, 0) for sy in (1, 0)]
+
+    def us_of(c):
+        return [der[a][0] if c[a] else der[a][1] for a in range(nd)]
+
+    Vs = {c: velocity(us_of(c), sigma, Lambda) for c in corners}
+    sp, sm, tot = [], [], []
+    for a in range(nd):
+        vals = [Vs[c][a] for c in corners]
+        p = np.maximum.reduce(vals + [np.zeros(shape)])          # Max9 / Max5 with 0
+        m = np.fabs(np.minimum.reduce(vals + [np.zeros(shape)]))  # Min9 / Min5 with 0
+        sp.append(p)
+        sm.append(m)
+        tot.append(p + m + ME)
+    deriv = None
+    for c in corners:
+        H = hamiltonian(us_of(c), Vs[c], Lambda)
+        w = H
+        for a in range(nd):
+            w = w * (sm[a] if c[a] else sp[a])
+        deriv = -w if deriv is None else deriv - w
+    for a in range(nd):
+        deriv = deriv / tot[a]
+    for a in range(nd):
+        deriv = deriv + (der[a][0] - der[a][1]) * sm[a] * sp[a] / tot[a]
+    speed = tot[0] + tot[1]
+    if nd == 3:
+        speed = speed + tot[2]
+    return deriv, speed
+
+
+class Params:
+    """Material, loading and integrator parameters of one instance."""
+
+    def __init__(self, mu=1.0, nu=0.3, Lambda=0, cfl=0.25, load_rate=None,
+                 load_initial=(0., 0., 0.), load_t0=0., load_mu=None, load_nu=None):
+        self.mu, self.nu, self.Lambda, self.cfl = mu, nu, Lambda, cfl
+        self.load_rate = None if load_rate is None else np.asarray(load_rate, float)
+        self.load_initial = np.asarray(load_initial, float)
+        self.load_t0 = load_t0
+        self.load_mu = mu if load_mu is None else load_mu
+        self.load_nu = nu if load_nu is None else load_nu
+
+
+def total_stress(beta, t, p):
+    """Dynamics' GetSigma: internal stress plus the applied load at time t."""
+    sigma = stress(beta, p.mu, p.nu)
+    if p.load_rate is not None:
+        add = applied_stress(t, p.load_rate, p.load_mu, p.load_nu, p.load_initial, p.load_t0)
+        for i in range(3):
+            sigma[ci(i, i)] += add[i]
+    return sigma
+
+
+def full_flux(beta, t, p):
+    """BetaPDynamics.CalculateFlux (CentralUpwindHJBetaPDynamics3D.py L218-221)."""
+    return flux(beta, total_stress(beta, t, p), p.Lambda)
+
+
+# ----------------------------------------------------------------------------------------------
+# TVD Runge-Kutta 3: FieldMover.py L38-141
+# ----------------------------------------------------------------------------------------------
+def rk3_step(beta, t, t_end, p, fixed_dt=None):
+    """One TVD-RK3 step; returns (beta_new, dt).
+
+    Adaptive (L61-141): dt = CFL / (max(gridShape) * max(speed)), clamped so t + dt <= t_end.
+    Fixed (L38-58): dt = fixed_dt, clamped the same way. All three stages use the same ``t``.
+    """
+    rhs, speed = full_flux(beta, t, p)
+    if fixed_dt is None:
+        s = max(beta.shape[1:]) * speed.max()
+        dt = float(p.cfl / s)
+    else:
+        dt = float(fixed_dt)
+    if t + dt > t_end:
+        dt = t_end - t
+    F0 = 1.0 * beta + 1.0 * (dt * rhs)
+    rhs, _ = full_flux(F0, t, p)
+    F1 = 0.75 * beta + 0.25 * F0 + 0.25 * (dt * rhs)
+    rhs, _ = full_flux(F1, t, p)
+    F2 = (1. / 3.) * beta + (2. / 3.) * F1 + (2. / 3.) * (dt * rhs)
+    return F2, dt
+
+
+def run(beta, t0, t_end, p, max_steps=None, observer=None):
+    """TVDRungeKutta_FieldMover.Run (L20-36): step until t >= t_end."""
+    t = t0
+    n = 0
+    while True:
+        beta, dt = rk3_step(beta, t, t_end, p)
+        t += dt
+        n += 1
+        if observer is not None:
+            observer(t, beta)
+        if t >= t_end or (max_steps is not None and n >= max_steps):
+            return beta, t

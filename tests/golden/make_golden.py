@@ -1,0 +1,210 @@
+"""Generate the golden vectors in this folder by running the reference's own Python FP64 path.
+
+The reference (mattbierbaum/cuda-plasticity, ``Plasticity/``) is Python 2 code. This script copies
+the modules of the time-step path into ``oracle/_refpy/Plasticity`` (git-ignored and not shipped to
+GPU machines) and applies six mechanical Python-3 patches, none of which touches arithmetic:
+
+  (i)   ``raise E, "msg"`` -> ``raise E("msg")`` and ``print "..."`` -> ``print(...)``;
+  (ii)  ``/2+1`` -> ``//2+1`` (integer half-spectrum sizes, GridArray/FourierSpaceTools.py L17-45);
+  (iii) ``__div__``/``__rdiv__`` -> ``__truediv__``/``__rtruediv__`` (Fields.py, PlasticityState.py);
+  (iv)  ``from scipy import fromfunction, sin, pi`` -> ``from numpy import ...`` (PlasticityState.py L4);
+  (v)   ``copy=False`` -> ``copy=None`` (numpy-2 semantics, GridArray.py L8-9);
+  (vi)  tabs expanded.
+
+It then drives the reference through its public API -- ``PlasticityState``, the
+``BetaPDynamics.CalculateFlux`` of CentralUpwindHJBetaPDynamics3D.py (3-D) or of
+CentralUpwindHJBetaPDynamics.py (2-D, the module RunPython.py imports), and
+``TVDRungeKutta_FieldMover.CalculateOneAdaptiveTimeStep`` -- on seeded inputs from
+``cdd.initial.gaussian_random_field`` and writes ``*.npz`` fixtures next to this file.
+
+Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only NAME]``.
+Only this script reads the reference tree; tests read the committed ``.npz`` files.
+"""
+import argparse
+import os
+import re
+import shutil
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+PATCHED = os.path.join(REPO, "oracle", "_refpy")
+
+MODULES = [
+    "__init__.py", "Constants.py", "NumericalMethods.py", "PlasticitySystem.py",
+    "GridArray/__init__.py", "GridArray/GridArray.py", "GridArray/FourierSpaceTools.py",
+    "Fields/__init__.py", "Fields/Fields.py",
+    "PlasticityStates/__init__.py", "PlasticityStates/PlasticityState.py",
+    "PlasticityStates/BurgersState.py",
+    "FieldDynamics/__init__.py", "FieldDynamics/FieldDynamics.py",
+    "FieldDynamics/CentralUpwindHJ.py", "FieldDynamics/CentralUpwindHJ3D.py",
+    "FieldDynamics/CentralUpwindHJBetaPDynamics.py",
+    "FieldDynamics/CentralUpwindHJBetaPDynamics3D.py",
+    "FieldMovers/__init__.py", "FieldMovers/FieldMover.py",
+]
+
+
+def _patch(text):
+    text = text.expandtabs(8)                                               # (vi)
+    text = re.sub(r'raise (\w+), (".*?")', r"raise \1(\2)", text)           # (i)
+    text = re.sub(r'^(\s*)print (".*)$', r"\1print(\2)", text, flags=re.M)  # (i)
+    text = text.replace("/2+1", "//2+1")                                    # (ii)
+    text = text.replace("__rdiv__", "__rtruediv__").replace("__div__", "__truediv__")  # (iii)
+    text = text.replace("from scipy import fromfunction, sin, pi",
+                        "from numpy import fromfunction, sin, pi")         # (iv)
+    text = text.replace("copy=False", "copy=None")                          # (v)
+    return text
+
+
+def build_patched_copy(reference):
+    src_root = os.path.join(reference, "Plasticity")
+    dst_root = os.path.join(PATCHED, "Plasticity")
+    if os.path.isdir(PATCHED):
+        shutil.rmtree(PATCHED)
+    for rel in MODULES:
+        dst = os.path.join(dst_root, rel)
+        os.makedirs(os.path.dirname(dst), exist_ok=True)
+        with open(os.path.join(src_root, rel)) as f:
+            text = f.read()
+        with open(dst, "w") as f:
+            f.write(_patch(text))
+    return PATCHED
+
+
+COMPONENTS = [(a, b) for a in "xyz" for b in "xyz"]
+
+
+def _import_reference():
+    sys.path.insert(0, PATCHED)
+    from Plasticity.PlasticityStates import PlasticityState
+    from Plasticity.GridArray import GridArray
+    from Plasticity.FieldMovers import FieldMover
+    from Plasticity.FieldDynamics import CentralUpwindHJBetaPDynamics3D as Dyn3
+    from Plasticity.FieldDynamics import CentralUpwindHJBetaPDynamics as Dyn2
+    return PlasticityState, GridArray, FieldMover, Dyn3, Dyn2
+
+
+def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.25,
+             load_rate=None, store_fields=True, t_end=1e30):
+    PlasticityState, GridArray, FieldMover, Dyn3, Dyn2 = _import_reference()
+    sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
+    from cdd.initial import gaussian_random_field
+
+    beta0 = gaussian_random_field(shape, sigma_f, 0.05, seed)
+    shape = tuple(shape)
+    mod = Dyn3 if len(shape) == 3 else Dyn2
+
+    if load_rate is None:
+        dynamics = mod.BetaPDynamics(Lambda=Lambda)
+    else:
+        rate = np.asarray(load_rate, dtype=np.float64)
+
+        class LoadedDynamics(mod.BetaPDynamics):
+            """RunPython.py L21-26/L35-50 loading, with the state's own mu and nu."""
+            def GetSigma(self, state, time):
+                sigma = state.CalculateSigma()
+                lamb = 2. * state.mu * state.nu / (1. - 2. * state.nu)
+                eps = rate * time
+                tr = eps[0] + eps[1] + eps[2]
+                for i, a in enumerate("xyz"):
+                    sigma[a, a] += lamb * tr + 2. * state.mu * eps[i]
+                return sigma
+        dynamics = LoadedDynamics(Lambda=Lambda)
+
+    def make_state(arr):
+        st = PlasticityState.PlasticityState(shape, mu=mu, nu=nu)
+        for c, comp in enumerate(COMPONENTS):
+            st.betaP[comp] = GridArray.GridArray(arr[c].copy())
+        return st
+
+    def to_array(st):
+        return np.stack([np.asarray(st.betaP[comp]) for comp in COMPONENTS])
+
+    def observables(st):
+        e = float(np.sum(st.CalculateElasticEnergy()))
+        m = float(np.asarray(st.betaP["z", "z"]).mean())
+        return e, m
+
+    out = {"shape": np.array(shape), "sigma_f": sigma_f, "seed": seed, "mu": mu, "nu": nu,
+           "Lambda": Lambda, "cfl": cfl,
+           "load_rate": np.zeros(3) if load_rate is None else np.asarray(load_rate, float)}
+    state = make_state(beta0)
+    t0 = time.time()
+    sig = state.CalculateSigma()
+    rhs, speed = dynamics.CalculateFlux(0.0, state, CFLCondition=True)
+    if store_fields:
+        out["beta0"] = beta0
+        out["sigma"] = np.stack([np.asarray(sig[comp]) for comp in COMPONENTS])
+        out["rhs"] = np.stack([np.asarray(rhs[comp]) for comp in COMPONENTS])
+        out["speed"] = np.asarray(speed)
+    mover = FieldMover.TVDRungeKutta_FieldMover(CFLsafeFactor=cfl)
+    t = 0.0
+    energies, means, dts = [], [], []
+    e, m = observables(state)
+    energies.append(e)
+    means.append(m)
+    for n in range(steps):
+        state, dt = mover.CalculateOneAdaptiveTimeStep(t, state, dynamics, t_end)
+        t += dt
+        dts.append(dt)
+        e, m = observables(state)
+        energies.append(e)
+        means.append(m)
+        if store_fields and n == 0:
+            out["beta1"] = to_array(state)
+    final = to_array(state)
+    if store_fields:
+        out["beta_final"] = final
+    out["steps"] = steps
+    out["dts"] = np.array(dts)
+    out["t_final"] = t
+    out["energy"] = np.array(energies)
+    out["mean_zz"] = np.array(means)
+    out["final_sum"] = final.reshape(9, -1).sum(axis=1)
+    out["final_sumsq"] = (final.reshape(9, -1) ** 2).sum(axis=1)
+    out["wall_s"] = time.time() - t0
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-16s shape=%-14s steps=%-4d wall=%.1fs -> %s"
+          % (name, shape, steps, out["wall_s"], os.path.relpath(path, REPO)))
+
+
+CASES = {
+    # one flux, one step and 10 steps of 3-D glide+climb dynamics
+    "g3d_16": dict(shape=(16, 16, 16), sigma_f=0.05, seed=1, steps=10),
+    # 2-D twin modules, 20 steps
+    "g2d_32": dict(shape=(32, 32), sigma_f=0.05, seed=2, steps=20),
+    # non-cubic 3-D grid: the k tables use each axis' own size, Dx uses the last axis
+    "g3d_aniso": dict(shape=(8, 12, 16), sigma_f=0.06, seed=3, steps=3),
+    # glide-projected dynamics (Lambda = 1)
+    "g3d_lambda": dict(shape=(12, 12, 12), sigma_f=0.06, seed=4, steps=3, Lambda=1),
+    # applied strain rate diag(-0.025, -0.025, 0.05), mu = 1
+    "g3d_load": dict(shape=(12, 12, 12), sigma_f=0.06, seed=5, steps=3,
+                     load_rate=(-0.025, -0.025, 0.05)),
+    # 2-D run at mixed-radix size (48 = 16 * 3) and a clamped end time
+    "g2d_48_tend": dict(shape=(48, 48), sigma_f=0.05, seed=6, steps=6, t_end=0.004),
+    # config-1 style curves: 2-D 128^2, sigma 0.05, no load, 100 steps (observables only)
+    "c1_2d_128": dict(shape=(128, 128), sigma_f=0.05, seed=11, steps=100, store_fields=False),
+    # config-2 style curves at reduced size: 3-D 32^3, sigma 0.04, applied strain rate, 40 steps
+    "c2_3d_32": dict(shape=(32, 32, 32), sigma_f=0.04, seed=12, steps=40, store_fields=False,
+                     load_rate=(-0.025, -0.025, 0.05)),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    build_patched_copy(args.reference)
+    for name, kw in CASES.items():
+        if args.only and name != args.only:
+            continue
+        run_case(name, **kw)
+
+
+if __name__ == "__main__":
+    main()
