@@ -1,0 +1,209 @@
+"""Torch-facing wrapper of the libcdd C ABI: a plan over a batch of CDD instances.
+
+Device memory and streams come from PyTorch; every computation runs in libcdd.so. A packed field
+is a 1-D tensor of ``plan.field_elems`` elements (FP64 or FP32 by plan precision); instance ``i``
+occupies ``field_view(t, i)``, shaped ``(9,) + shape`` with the last grid axis contiguous.
+"""
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import CDDError, check
+
+
+@dataclass
+class Instance:
+    """One simulation: grid, material, dynamics and loading (see cdd_instance in include/cdd.h)."""
+    shape: Sequence[int]
+    mu: float = 1.0
+    nu: float = 0.3
+    Lambda: float = 0.0
+    cfl: float = 0.25
+    load_rate: Optional[Sequence[float]] = None
+    load_initial: Sequence[float] = (0.0, 0.0, 0.0)
+    load_t0: float = 0.0
+    load_mu: Optional[float] = None
+    load_nu: Optional[float] = None
+
+    def to_c(self):
+        c = _lib.cdd_instance()
+        shp = tuple(int(v) for v in self.shape)
+        c.ndim = len(shp)
+        for a in range(3):
+            c.shape[a] = shp[a] if a < len(shp) else 1
+        c.mu, c.nu, c.Lambda, c.cfl = float(self.mu), float(self.nu), float(self.Lambda), float(self.cfl)
+        c.has_load = 0 if self.load_rate is None else 1
+        rate = (0., 0., 0.) if self.load_rate is None else self.load_rate
+        for a in range(3):
+            c.load_rate[a] = float(rate[a])
+            c.load_initial[a] = float(self.load_initial[a])
+        c.load_t0 = float(self.load_t0)
+        c.load_mu = float(self.mu if self.load_mu is None else self.load_mu)
+        c.load_nu = float(self.nu if self.load_nu is None else self.load_nu)
+        return c
+
+    @property
+    def cells(self):
+        return int(np.prod(self.shape))
+
+
+def _stream(stream=None):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Plan:
+    """A batch of instances at one precision ("f64" or "f32") on the current CUDA device."""
+
+    def __init__(self, instances, precision="f64", device=None):
+        if isinstance(instances, Instance):
+            instances = [instances]
+        self.instances = list(instances)
+        if precision not in ("f64", "f32"):
+            raise ValueError("precision must be 'f64' or 'f32'")
+        self.precision = precision
+        self.dtype = torch.float64 if precision == "f64" else torch.float32
+        if not torch.cuda.is_available():
+            raise RuntimeError("cdd.Plan needs a CUDA device (sm_100a)")
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.lib = _lib.load()
+        arr = (_lib.cdd_instance * len(self.instances))(*[i.to_c() for i in self.instances])
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(self.lib.cdd_plan_create(arr, len(self.instances),
+                                           _lib.CDD_F64 if precision == "f64" else _lib.CDD_F32,
+                                           ctypes.byref(h)))
+        self.handle = h
+        n = len(self.instances)
+        self.field_elems = int(self.lib.cdd_plan_field_elems(h))
+        self.stress_elems = int(self.lib.cdd_plan_stress_elems(h))
+        self.field_offsets = [int(self.lib.cdd_plan_field_offset(h, i)) for i in range(n)]
+        self.stress_offsets = [int(self.lib.cdd_plan_stress_offset(h, i)) for i in range(n)]
+        self.cells = [int(self.lib.cdd_plan_cells(h, i)) for i in range(n)]
+        self.total_cells = int(self.lib.cdd_plan_cells(h, -1))
+        self.scratch_bytes = int(self.lib.cdd_plan_scratch_bytes(h))
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.cdd_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ buffers
+    def empty_field(self):
+        return torch.empty(self.field_elems, dtype=self.dtype, device=self.device)
+
+    def empty_stress(self):
+        return torch.empty(self.stress_elems, dtype=self.dtype, device=self.device)
+
+    def field_view(self, buf, i):
+        inst = self.instances[i]
+        o = self.field_offsets[i]
+        return buf[o:o + 9 * self.cells[i]].view((9,) + tuple(inst.shape))
+
+    def stress_view(self, buf, i):
+        inst = self.instances[i]
+        o = self.stress_offsets[i]
+        return buf[o:o + 6 * self.cells[i]].view((6,) + tuple(inst.shape))
+
+    def pack(self, arrays):
+        """Copy a list of (9,)+shape arrays (numpy or torch) into a new packed device field."""
+        buf = self.empty_field()
+        for i, a in enumerate(arrays):
+            t = torch.as_tensor(np.ascontiguousarray(a) if isinstance(a, np.ndarray) else a)
+            self.field_view(buf, i).copy_(t.to(self.dtype))
+        return buf
+
+    def unpack(self, buf):
+        return [self.field_view(buf, i).detach().cpu().numpy() for i in range(len(self.instances))]
+
+    def _check_field(self, buf, name="beta"):
+        if not isinstance(buf, torch.Tensor) or buf.dtype != self.dtype or not buf.is_cuda \
+                or not buf.is_contiguous() or buf.numel() != self.field_elems:
+            raise ValueError("%s must be a contiguous %s CUDA tensor of %d elements"
+                             % (name, self.dtype, self.field_elems))
+
+    # ------------------------------------------------------------------ operators
+    def stress(self, beta, out=None, stream=None):
+        """Internal stress (6 symmetric components per instance) of a packed field."""
+        self._check_field(beta)
+        out = self.empty_stress() if out is None else out
+        check(self.lib.cdd_stress(self.handle, ctypes.c_void_p(beta.data_ptr()),
+                                  ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+        return out
+
+    def flux(self, beta, t=0.0, want_speed=True, stream=None):
+        """(rhs, speed) of the central-upwind flux at time t; speed is one value per cell."""
+        self._check_field(beta)
+        rhs = self.empty_field()
+        speed = torch.empty(self.total_cells, dtype=self.dtype, device=self.device) if want_speed else None
+        check(self.lib.cdd_flux(self.handle, ctypes.c_void_p(beta.data_ptr()), float(t),
+                                ctypes.c_void_p(rhs.data_ptr()),
+                                ctypes.c_void_p(speed.data_ptr() if speed is not None else 0),
+                                _stream(stream)))
+        return rhs, speed
+
+    def set_time(self, t=None, t_end=None):
+        n = len(self.instances)
+        def arr(v):
+            if v is None:
+                return None
+            v = np.broadcast_to(np.asarray(v, dtype=np.float64), (n,)).copy()
+            return (ctypes.c_double * n)(*v)
+        torch.cuda.current_stream().synchronize()
+        check(self.lib.cdd_set_time(self.handle, arr(t), arr(t_end)))
+
+    def get_time(self):
+        """(t, dt_last, active) arrays; synchronises."""
+        n = len(self.instances)
+        t = (ctypes.c_double * n)()
+        dt = (ctypes.c_double * n)()
+        act = (ctypes.c_int * n)()
+        torch.cuda.current_stream().synchronize()
+        check(self.lib.cdd_get_time(self.handle, t, dt, act))
+        return np.array(t[:]), np.array(dt[:]), np.array(act[:], dtype=bool)
+
+    def step(self, beta, stream=None):
+        self._check_field(beta)
+        check(self.lib.cdd_step(self.handle, ctypes.c_void_p(beta.data_ptr()), _stream(stream)))
+
+    def step_fixed(self, beta, dt, stream=None):
+        self._check_field(beta)
+        check(self.lib.cdd_step_fixed(self.handle, ctypes.c_void_p(beta.data_ptr()), float(dt),
+                                      _stream(stream)))
+
+    def run(self, beta, n_steps, graph=True, stream=None):
+        self._check_field(beta)
+        check(self.lib.cdd_run(self.handle, ctypes.c_void_p(beta.data_ptr()), int(n_steps),
+                               1 if graph else 0, _stream(stream)))
+
+    def observables(self, beta, stream=None):
+        """(energy, mean_zz) arrays over instances, FP64; synchronises."""
+        self._check_field(beta)
+        n = len(self.instances)
+        e = (ctypes.c_double * n)()
+        m = (ctypes.c_double * n)()
+        check(self.lib.cdd_observables(self.handle, ctypes.c_void_p(beta.data_ptr()), e, m,
+                                       _stream(stream)))
+        return np.array(e[:]), np.array(m[:])
+
+    def check_status(self):
+        torch.cuda.current_stream().synchronize()
+        check(self.lib.cdd_check_status(self.handle))
+
+
+def stress_to_tensor9(s6):
+    """Expand (6,)+grid symmetric storage xx, xy, xz, yy, yz, zz to (9,)+grid."""
+    idx = [0, 1, 2, 1, 3, 4, 2, 4, 5]
+    return s6[idx]

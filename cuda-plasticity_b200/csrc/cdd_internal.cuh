@@ -1,0 +1,348 @@
+// Internal declarations shared by the libcdd translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cdd.h"
+
+namespace cdd {
+
+constexpr int MAX_STAGES = 12;
+constexpr double ME = 2.220446049250313080847263336181640625e-16;   // DBL_EPSILON
+
+// One-dimensional FFT of length n as a sequence of Stockham stages of radix 2, 3, 4, 5, 8, 16.
+struct LinePlan {
+    int n;
+    int nst;
+    int radix[MAX_STAGES];
+    int tw;   // offset (complex elements) of this length's twiddle table w_n^k, k < n
+};
+
+// Per-pass tiling of one instance (host-chosen, read by the kernels).
+struct PassTile {
+    int blocks;    // blocks this instance contributes to the launch
+    int lines;     // rows kernel: line pairs per block; strided kernels: columns per block (W)
+    int threads;   // threads this instance needs (<= launch blockDim)
+    int tiles_a;   // strided kernels: number of column tiles along the row
+};
+
+enum Pass { PASS_R2C = 0, PASS_MID_F, PASS_GREEN, PASS_MID_I, PASS_C2R, NUM_PASSES };
+
+// Device-side description of one instance.
+struct InstDev {
+    int nd;                 // 2 or 3
+    int n0, n1, n2;         // grid; n2 = 1 in 2-D
+    int nl;                 // length of the contiguous (last) axis
+    int nh;                 // nl / 2 + 1
+    int nhp;                // padded spectrum row length (complex elements)
+    int rows;               // real rows per component (cells / nl)
+    long long cells;
+    long long foff;         // offset of the packed 9-component field
+    long long soff;         // offset of the packed 6-component stress
+    long long coff;         // offset in per-cell arrays (speed)
+    long long spoff;        // offset (complex elements) of the 9-component spectrum
+    long long rsoff;        // offset of the per-row FP64 sums (FP32 mean path)
+    LinePlan lp_last;       // complex FFT of length nl (two real rows packed)
+    LinePlan lp_mid;        // axis 1 (3-D only)
+    LinePlan lp_first;      // axis 0
+    int koff0, koff1, koffh;    // k tables: axis 0, axis 1 (3-D), half axis (last)
+    PassTile tile[NUM_PASSES];
+    int stencil_blocks;
+    double mu, nu, lamb, Lambda, cfl, nmax;
+    double h, inv_h;        // Dx = 1 / shape[-1] (CentralUpwindHJ3D.py L15-16)
+    double inv_cells;
+    int has_load;
+    double load_rate[3], load_init[3], load_t0, load_lamb, load_mu;
+};
+
+// Per-instance clock and reduction results kept on the device.
+struct InstClock {
+    double t;          // current time
+    double t_end;      // end of the current Run interval
+    double t_stage;    // step-start time (used for the load in all three stages)
+    double dt;         // dt of the current/last step
+    double vmax;       // last wave-speed maximum
+    int active;        // this step is applied
+    int steps;
+};
+
+// Device status bits.
+enum StatusBits { ST_NONFINITE = 1, ST_TIMEOUT = 2 };
+
+template <typename T> struct VecOf;
+template <> struct VecOf<float> { typedef float2 type; };
+template <> struct VecOf<double> { typedef double2 type; };
+
+template <typename V> __device__ __forceinline__ V vadd(V a, V b) { V r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename V> __device__ __forceinline__ V vsub(V a, V b) { V r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename V> __device__ __forceinline__ V vmul(V a, V b) {
+    V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename V> __device__ __forceinline__ V vconj(V a) { a.y = -a.y; return a; }
+template <typename V, typename T> __device__ __forceinline__ V vscale(V a, T s) { a.x *= s; a.y *= s; return a; }
+template <typename V> __device__ __forceinline__ V vmake(double x, double y) {
+    V r; r.x = (decltype(r.x))x; r.y = (decltype(r.y))y; return r;
+}
+// multiply by -i (forward transform) or +i (inverse transform)
+template <typename V, bool INV> __device__ __forceinline__ V vrot(V a) {
+    V r;
+    if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// Small DFT codelets, out[k] = sum_n in[n] exp(-+ 2 pi i n k / R), in place.
+// Constants are the exact mathematical values rounded to the working precision.
+// ------------------------------------------------------------------------------------------
+#define CDD_SQRT1_2 0.707106781186547524400844362104849039
+#define CDD_COS_PI8 0.923879532511286756128183189396788933
+#define CDD_SIN_PI8 0.382683432365089771728459984030398866
+#define CDD_SQRT3_2 0.866025403784438646763723170752936183
+#define CDD_COS_2PI5 0.309016994374947424102293417182819059
+#define CDD_COS_4PI5 (-0.809016994374947424102293417182819059)
+#define CDD_SIN_2PI5 0.951056516295153572116439333379382143
+#define CDD_SIN_4PI5 0.587785252292473129168705954639072769
+
+template <typename V, bool INV> __device__ __forceinline__ void dft2(V* x) {
+    V a = x[0];
+    x[0] = vadd(a, x[1]);
+    x[1] = vsub(a, x[1]);
+}
+
+template <typename V, bool INV> __device__ __forceinline__ void dft3(V* x) {
+    typedef decltype(x[0].x) T;
+    V t1 = vadd(x[1], x[2]);
+    V t2 = vsub(x[1], x[2]);
+    V m = x[0];
+    m.x -= (T)0.5 * t1.x;
+    m.y -= (T)0.5 * t1.y;
+    x[0] = vadd(x[0], t1);
+    V r = vrot<V, INV>(vscale(t2, (T)CDD_SQRT3_2));
+    x[1] = vadd(m, r);
+    x[2] = vsub(m, r);
+}
+
+template <typename V, bool INV> __device__ __forceinline__ void dft4(V* x) {
+    V t0 = vadd(x[0], x[2]);
+    V t1 = vsub(x[0], x[2]);
+    V t2 = vadd(x[1], x[3]);
+    V t3 = vrot<V, INV>(vsub(x[1], x[3]));
+    x[0] = vadd(t0, t2);
+    x[2] = vsub(t0, t2);
+    x[1] = vadd(t1, t3);
+    x[3] = vsub(t1, t3);
+}
+
+template <typename V, bool INV> __device__ __forceinline__ void dft5(V* x) {
+    typedef decltype(x[0].x) T;
+    const T c1 = (T)CDD_COS_2PI5, c2 = (T)CDD_COS_4PI5, s1 = (T)CDD_SIN_2PI5, s2 = (T)CDD_SIN_4PI5;
+    V a1 = vadd(x[1], x[4]), b1 = vsub(x[1], x[4]);
+    V a2 = vadd(x[2], x[3]), b2 = vsub(x[2], x[3]);
+    V x0 = x[0];
+    V m1, m2, n1, n2;
+    m1.x = x0.x + c1 * a1.x + c2 * a2.x; m1.y = x0.y + c1 * a1.y + c2 * a2.y;
+    m2.x = x0.x + c2 * a1.x + c1 * a2.x; m2.y = x0.y + c2 * a1.y + c1 * a2.y;
+    n1.x = s1 * b1.x + s2 * b2.x; n1.y = s1 * b1.y + s2 * b2.y;
+    n2.x = s2 * b1.x - s1 * b2.x; n2.y = s2 * b1.y - s1 * b2.y;
+    V r1 = vrot<V, INV>(n1), r2 = vrot<V, INV>(n2);
+    x[0] = vadd(vadd(x0, a1), a2);
+    x[1] = vadd(m1, r1);
+    x[4] = vsub(m1, r1);
+    x[2] = vadd(m2, r2);
+    x[3] = vsub(m2, r2);
+}
+
+template <typename V, bool INV> __device__ __forceinline__ void dft8(V* x) {
+    typedef decltype(x[0].x) T;
+    V e[4] = {x[0], x[2], x[4], x[6]};
+    V o[4] = {x[1], x[3], x[5], x[7]};
+    dft4<V, INV>(e);
+    dft4<V, INV>(o);
+    const T s = (T)CDD_SQRT1_2;
+    const T sg = INV ? (T)1 : (T)-1;
+    o[1] = vmul(o[1], vmake<V>(s, sg * s));
+    o[2] = vrot<V, INV>(o[2]);
+    o[3] = vmul(o[3], vmake<V>(-s, sg * s));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        x[k] = vadd(e[k], o[k]);
+        x[k + 4] = vsub(e[k], o[k]);
+    }
+}
+
+template <typename V, bool INV> __device__ __forceinline__ void dft16(V* x) {
+    typedef decltype(x[0].x) T;
+    V e[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { e[k] = x[2 * k]; o[k] = x[2 * k + 1]; }
+    dft8<V, INV>(e);
+    dft8<V, INV>(o);
+    const T c = (T)CDD_COS_PI8, s = (T)CDD_SIN_PI8, r = (T)CDD_SQRT1_2;
+    const T sg = INV ? (T)1 : (T)-1;
+    o[1] = vmul(o[1], vmake<V>(c, sg * s));
+    o[2] = vmul(o[2], vmake<V>(r, sg * r));
+    o[3] = vmul(o[3], vmake<V>(s, sg * c));
+    o[4] = vrot<V, INV>(o[4]);
+    o[5] = vmul(o[5], vmake<V>(-s, sg * c));
+    o[6] = vmul(o[6], vmake<V>(-r, sg * r));
+    o[7] = vmul(o[7], vmake<V>(-c, sg * s));
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        x[k] = vadd(e[k], o[k]);
+        x[k + 8] = vsub(e[k], o[k]);
+    }
+}
+
+template <int R, typename V, bool INV> __device__ __forceinline__ void dft(V* x) {
+    if (R == 2) dft2<V, INV>(x);
+    else if (R == 3) dft3<V, INV>(x);
+    else if (R == 4) dft4<V, INV>(x);
+    else if (R == 5) dft5<V, INV>(x);
+    else if (R == 8) dft8<V, INV>(x);
+    else if (R == 16) dft16<V, INV>(x);
+}
+
+// ------------------------------------------------------------------------------------------
+// Shared-memory line FFT engine: out-of-place Stockham autosort, mixed radix, natural order in
+// and out. Each stage reads one buffer and writes the other; a thread holds one butterfly
+// (R values) at a time.
+//
+// Lines live in shared memory through a layout functor L:
+//   L.addr(line, idx)  -> element offset of element idx of line `line`
+//   L.lines            -> number of lines
+//   L.line_fast        -> true when consecutive butterflies should walk lines (column tiles)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int row_pad(int a) { return a + (a >> 4); }
+
+struct RowLayout {   // lines are rows of length n, padded every 16 elements
+    int lines, ld;
+    __device__ __forceinline__ int addr(int l, int i) const { return l * ld + row_pad(i); }
+    static constexpr bool line_fast = false;
+};
+
+struct ColLayout {   // element i of line l = (c, w) at (c * cs) + i * w_count + w
+    int lines, wcount, cs;
+    __device__ __forceinline__ int addr(int l, int i) const {
+        int c = l / wcount;
+        int w = l - c * wcount;
+        return c * cs + i * wcount + w;
+    }
+    static constexpr bool line_fast = true;
+};
+
+template <int R, typename V, bool INV, typename Lay>
+__device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restrict__ dst,
+                                          const Lay& lay, int n, int ns,
+                                          const V* __restrict__ tw, int tid, int nt) {
+    const int nr = n / R;
+    const int twstep = n / (ns * R);
+    const int total = lay.lines * nr;
+#pragma unroll 1
+    for (int g = tid; g < total; g += nt) {
+        int l, j;
+        if (Lay::line_fast) { l = g % lay.lines; j = g / lay.lines; }
+        else { j = g % nr; l = g / nr; }
+        const int jm = j % ns;
+        V v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            V a = src[lay.addr(l, j + r * nr)];
+            if (r > 0 && jm != 0) {
+                V w = __ldg(&tw[r * jm * twstep]);
+                if (INV) w.y = -w.y;
+                a = vmul(a, w);
+            }
+            v[r] = a;
+        }
+        dft<R, V, INV>(v);
+        const int jd = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[lay.addr(l, jd + r * ns)] = v[r];
+    }
+    __syncthreads();
+}
+
+// Run all stages of `lp` on the lines of `lay`, starting in buffer a (b is scratch of the same
+// layout). Returns the buffer that holds the result. Every thread of the block must call this.
+template <typename V, bool INV, typename Lay>
+__device__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
+                        int tid, int nt) {
+    const int n = lp.n;
+    const V* tw = twbase + lp.tw;
+    int ns = 1;
+    V* src = a;
+    V* dst = b;
+    for (int st = 0; st < lp.nst; ++st) {
+        const int R = lp.radix[st];
+        switch (R) {
+            case 2: fft_stage<2, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            case 3: fft_stage<3, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            case 4: fft_stage<4, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            case 5: fft_stage<5, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            case 8: fft_stage<8, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            default: fft_stage<16, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+        }
+        ns *= R;
+        V* t = src; src = dst; dst = t;
+    }
+    return src;
+}
+
+// Find the instance that owns global block b, given prefix sums pre[0..n] of blocks.
+__device__ __forceinline__ int find_instance(const int* __restrict__ pre, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&pre[mid]) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------------------------------
+// Host-side plan core shared by the translation units (device pointers + launch shapes).
+// ------------------------------------------------------------------------------------------
+struct LaunchShape {
+    int blocks = 0;       // total blocks over all instances
+    int threads = 0;      // blockDim.x
+    size_t smem = 0;      // dynamic shared memory bytes
+    int* d_pre = nullptr; // prefix sums of blocks per instance (n_inst + 1)
+};
+
+struct PlanCore {
+    int n_inst = 0;
+    int precision = CDD_F64;
+    int max_nd = 3;
+    bool any3d = false;
+    long long field_elems = 0, stress_elems = 0, cells = 0, spec_elems = 0, rows_total = 0;
+    InstDev* d_inst = nullptr;       // device copy of the instance table
+    InstClock* d_clock = nullptr;
+    void* d_tw = nullptr;            // twiddles (double2 or float2)
+    void* d_k = nullptr;             // k tables (double or float)
+    void* d_spec = nullptr;          // 9-component half spectra
+    void* d_sigma = nullptr;         // 6-component internal stress
+    void* d_f0 = nullptr;            // stage-1 rhs / F0
+    void* d_f1 = nullptr;            // F1
+    double* d_rowsum = nullptr;      // FP32 path: FP64 per-row sums
+    double* d_sbar = nullptr;        // FP32 path: FP64 mean stress per instance (6)
+    double* d_bmax = nullptr;        // per-block wave-speed maxima
+    double* d_bsum = nullptr;        // per-block energy and mean-zz partial sums (2 per block)
+    double* d_obs = nullptr;         // per-instance energy, mean zz (2 per instance)
+    int* d_status = nullptr;
+    LaunchShape pass[NUM_PASSES];
+    LaunchShape stencil;
+    LaunchShape cellwise;            // elementwise kernels over cells
+};
+
+// stress.cu
+cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st);
+// stencil.cu
+enum StencilMode { M_FLUX = 0, M_STAGE1 = 1, M_STAGE2 = 2, M_STAGE3 = 3 };
+cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,
+                           void* speed, double t_flux, cudaStream_t st);
+cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
+cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaStream_t st);
+cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st);
+cudaError_t stencil_set_attributes(int precision);
+cudaError_t stress_set_attributes(int precision, size_t max_smem);
+
+}  // namespace cdd

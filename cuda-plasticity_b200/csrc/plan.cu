@@ -1,0 +1,563 @@
+// Plan construction and the C ABI of libcdd (see include/cdd.h).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "cdd_internal.cuh"
+
+using namespace cdd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CDD_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(CDD_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// FFT length plans
+// ------------------------------------------------------------------------------------------
+bool factor(int n, int& a, int& b, int& c) {
+    a = b = c = 0;
+    while (n % 2 == 0) { n /= 2; ++a; }
+    while (n % 3 == 0) { n /= 3; ++b; }
+    while (n % 5 == 0) { n /= 5; ++c; }
+    return n == 1;
+}
+
+// Radix sequence for length n = 2^a 3^b 5^c: radix-16 stages for the power of two (an 8 x 4
+// pair instead of 16 x 2 when a = 1 mod 4), then radix 3 and radix 5 stages.
+bool make_line_plan(int n, LinePlan& lp) {
+    int a, b, c;
+    if (!factor(n, a, b, c) || a < 1) return false;
+    std::memset(&lp, 0, sizeof lp);
+    lp.n = n;
+    std::vector<int> r;
+    int q = a / 4, m = a % 4;
+    if (m == 1 && q > 0) { q -= 1; m = 5; }
+    for (int i = 0; i < q; ++i) r.push_back(16);
+    if (m == 1) r.push_back(2);
+    else if (m == 2) r.push_back(4);
+    else if (m == 3) r.push_back(8);
+    else if (m == 5) { r.push_back(8); r.push_back(4); }
+    for (int i = 0; i < b; ++i) r.push_back(3);
+    for (int i = 0; i < c; ++i) r.push_back(5);
+    if ((int)r.size() > MAX_STAGES) return false;
+    lp.nst = (int)r.size();
+    for (int i = 0; i < lp.nst; ++i) lp.radix[i] = r[i];
+    return true;
+}
+
+// w_n^k = exp(-2 pi i k / n): cosl/sinl of the exact angle in long double, reduced to the first
+// octant by the symmetries of the unit circle so that the table is exactly symmetric.
+void twiddle(int n, int k, long double& re, long double& im) {
+    const long double PI = 3.141592653589793238462643383279502884L;
+    k %= n;
+    // angle = 2 pi k / n; use the octant index of 8k/n
+    long long k8 = 8LL * k;
+    long long q = k8 / n;              // octant 0..7
+    long long rem8 = k8 - q * n;       // 8k mod n, in [0, n)
+    // angle = (q + rem8/n) * pi/4 ; t = rem8 / n * pi/4 in [0, pi/4)
+    long double t = (long double)rem8 / (long double)n * (PI / 4.0L);
+    long double ct = cosl(t), st = sinl(t);
+    long double cr, ci;   // cos and sin of the full angle
+    const long double r2 = 0.707106781186547524400844362104849039L;
+    switch (q) {
+        case 0: cr = ct; ci = st; break;
+        case 1: cr = r2 * (ct - st); ci = r2 * (ct + st); break;   // pi/4 + t
+        case 2: cr = -st; ci = ct; break;
+        case 3: cr = -r2 * (ct + st); ci = r2 * (ct - st); break;  // 3pi/4 + t
+        case 4: cr = -ct; ci = -st; break;
+        case 5: cr = -r2 * (ct - st); ci = -r2 * (ct + st); break;
+        case 6: cr = st; ci = -ct; break;
+        default: cr = r2 * (ct + st); ci = -r2 * (ct - st); break;
+    }
+    re = cr;
+    im = -ci;
+}
+
+// k_d = n_scale * identity(2 pi i / n_axis), identity wrapping angles above pi by -2 pi
+// (FourierSpaceTools.py L5-7, L29-49), evaluated with the same double operations as the reference.
+double k_value(int n_scale, int n_axis, int i) {
+    double a = 2.0 * M_PI * (double)i / (double)n_axis;
+    if (a > M_PI) a = a - 2 * M_PI;
+    return (double)n_scale * a;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {}
+};
+
+}  // namespace
+
+struct cdd_plan {
+    PlanCore core;
+    std::vector<InstDev> inst;
+    std::vector<cdd_instance> desc;
+    long long scratch_bytes = 0;
+    std::vector<void*> allocs;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    const void* graph_beta = nullptr;
+    int device = 0;
+};
+
+namespace {
+
+cudaError_t dalloc(cdd_plan* p, void** ptr, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaSuccess) {
+        p->allocs.push_back(*ptr);
+        p->scratch_bytes += (long long)bytes;
+    }
+    return e;
+}
+
+void free_plan(cdd_plan* p) {
+    if (!p) return;
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+    for (void* a : p->allocs) cudaFree(a);
+    delete p;
+}
+
+int build_shapes(cdd_plan* p, size_t elt) {
+    PlanCore& C = p->core;
+    const int n = C.n_inst;
+    const size_t velt = 2 * elt;
+    std::vector<int> pre[NUM_PASSES];
+    std::vector<int> pre_st, pre_cw;
+    for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(0);
+    pre_st.push_back(0);
+    pre_cw.push_back(0);
+    size_t smem_max[NUM_PASSES] = {0, 0, 0, 0, 0};
+    int thr_max[NUM_PASSES] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        InstDev& I = p->inst[i];
+        // rows kernels (R2C: 9 components, C2R: 6); ping-pong buffers of P padded rows
+        for (int k : {PASS_R2C, PASS_C2R}) {
+            const int comps = (k == PASS_R2C) ? 9 : 6;
+            long long npairs = ((long long)comps * I.rows + 1) / 2;
+            const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
+            int P = (int)((40 * 1024) / line_bytes);
+            if (P < 1) P = 1;
+            if (P > npairs) P = (int)npairs;
+            PassTile& t = I.tile[k];
+            t.lines = P;
+            t.threads = 256;
+            t.blocks = (int)((npairs + P - 1) / P);
+            t.tiles_a = 1;
+            size_t sm = 2 * (size_t)P * line_bytes;
+            if (sm > smem_max[k]) smem_max[k] = sm;
+            if (t.threads > thr_max[k]) thr_max[k] = t.threads;
+        }
+        // axis-1 FFT (3-D only): W columns of 128 bytes
+        for (int k : {PASS_MID_F, PASS_MID_I}) {
+            PassTile& t = I.tile[k];
+            if (I.nd != 3) { t.blocks = 0; t.lines = t.threads = t.tiles_a = 0; continue; }
+            const int comps = (k == PASS_MID_F) ? 9 : 6;
+            int W = (int)(128 / velt);
+            while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
+            t.lines = W;
+            t.threads = 256;
+            t.tiles_a = (I.nh + W - 1) / W;
+            t.blocks = comps * I.n0 * t.tiles_a;
+            size_t sm = 2 * (size_t)W * I.n1 * velt;
+            if (sm > smem_max[k]) smem_max[k] = sm;
+            if (t.threads > thr_max[k]) thr_max[k] = t.threads;
+        }
+        // fused Green pass along axis 0: 9 components x W columns, ping-pong
+        {
+            PassTile& t = I.tile[PASS_GREEN];
+            int W = 16;
+            while (W > 1 && 2 * (size_t)9 * (I.n0 * W + W) * velt > 200 * 1024) W >>= 1;
+            if (2 * (size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
+                return fail(CDD_ERR_SHAPE, "axis-0 length %d too large for the fused k-space pass", I.n0);
+            t.lines = W;
+            t.threads = 512;
+            t.tiles_a = (I.nh + W - 1) / W;
+            t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
+            size_t sm = 2 * (size_t)9 * (I.n0 * W + W) * velt;
+            if (sm > smem_max[PASS_GREEN]) smem_max[PASS_GREEN] = sm;
+            if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
+        }
+        for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(pre[k].back() + I.tile[k].blocks);
+        I.stencil_blocks = (int)((I.cells + 127) / 128);
+        pre_st.push_back(pre_st.back() + I.stencil_blocks);
+        pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));
+    }
+    size_t smem_all = 0;
+    for (int k = 0; k < NUM_PASSES; ++k) {
+        LaunchShape& L = C.pass[k];
+        L.blocks = pre[k].back();
+        L.threads = (k == PASS_GREEN) ? 512 : 256;
+        L.smem = smem_max[k];
+        if (L.smem > smem_all) smem_all = L.smem;
+        CDD_CUDA(dalloc(p, (void**)&L.d_pre, sizeof(int) * (n + 1)));
+        CDD_CUDA(cudaMemcpy(L.d_pre, pre[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
+    C.stencil.blocks = pre_st.back();
+    C.stencil.threads = 128;
+    CDD_CUDA(dalloc(p, (void**)&C.stencil.d_pre, sizeof(int) * (n + 1)));
+    CDD_CUDA(cudaMemcpy(C.stencil.d_pre, pre_st.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    C.cellwise.blocks = pre_cw.back();
+    C.cellwise.threads = 256;
+    CDD_CUDA(dalloc(p, (void**)&C.cellwise.d_pre, sizeof(int) * (n + 1)));
+    CDD_CUDA(cudaMemcpy(C.cellwise.d_pre, pre_cw.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CDD_CUDA(stress_set_attributes(C.precision, smem_all < 48 * 1024 ? 48 * 1024 : smem_all));
+    return CDD_OK;
+}
+
+int check_plan(const cdd_plan* p) {
+    if (!p) return fail(CDD_ERR_ARG, "null plan");
+    return CDD_OK;
+}
+
+int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_fixed) {
+    PlanCore& C = p->core;
+    CDD_CUDA(launch_stress(C, beta, C.d_sigma, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE1, beta, beta, C.d_f0, nullptr, 0.0, st));
+    CDD_CUDA(launch_dt(C, fixed, dt_fixed, st));
+    CDD_CUDA(launch_axpy_f0(C, beta, C.d_f0, st));
+    CDD_CUDA(launch_stress(C, C.d_f0, C.d_sigma, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE2, C.d_f0, beta, C.d_f1, nullptr, 0.0, st));
+    CDD_CUDA(launch_stress(C, C.d_f1, C.d_sigma, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE3, C.d_f1, beta, beta, nullptr, 0.0, st));
+    return CDD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cdd_last_error(void) { return g_last_error.c_str(); }
+const char* cdd_version(void) { return "cdd-b200 0.1 (sm_100a)"; }
+
+int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_plan** out) {
+    g_last_error.clear();
+    if (!inst || n_inst <= 0 || !out) return fail(CDD_ERR_ARG, "bad arguments to cdd_plan_create");
+    if (precision != CDD_F64 && precision != CDD_F32) return fail(CDD_ERR_ARG, "bad precision %d", precision);
+    *out = nullptr;
+    cdd_plan* p = new cdd_plan();
+    cudaGetDevice(&p->device);
+    PlanCore& C = p->core;
+    C.n_inst = n_inst;
+    C.precision = precision;
+    const size_t elt = precision == CDD_F64 ? sizeof(double) : sizeof(float);
+    p->desc.assign(inst, inst + n_inst);
+    p->inst.resize(n_inst);
+    std::map<int, int> tw_off;
+    std::vector<double> twre, twim;
+    std::vector<double> ktab;
+    long long foff = 0, soff = 0, coff = 0, spoff = 0, rsoff = 0;
+    C.any3d = false;
+    for (int i = 0; i < n_inst; ++i) {
+        const cdd_instance& d = inst[i];
+        InstDev& I = p->inst[i];
+        std::memset(&I, 0, sizeof I);
+        if (d.ndim != 2 && d.ndim != 3) {
+            free_plan(p);
+            return fail(CDD_ERR_SHAPE, "instance %d: ndim must be 2 or 3 (got %d)", i, d.ndim);
+        }
+        int sh[3] = {d.shape[0], d.shape[1], d.ndim == 3 ? d.shape[2] : 1};
+        for (int a = 0; a < d.ndim; ++a) {
+            int A, B, Cc;
+            if (sh[a] < 4 || sh[a] > 1024 || sh[a] % 2 || !factor(sh[a], A, B, Cc) || (B > 0 && Cc > 0)) {
+                free_plan(p);
+                return fail(CDD_ERR_SHAPE,
+                            "instance %d: axis %d size %d unsupported (even, 4..1024, 2^a 3^b or 2^a 5^c)",
+                            i, a, sh[a]);
+            }
+        }
+        if (!(d.mu > 0) || !(d.nu < 0.5) || !(d.nu > -1.0) || !(d.cfl > 0)) {
+            free_plan(p);
+            return fail(CDD_ERR_ARG, "instance %d: need mu > 0, -1 < nu < 0.5, cfl > 0", i);
+        }
+        I.nd = d.ndim;
+        I.n0 = sh[0]; I.n1 = sh[1]; I.n2 = sh[2];
+        if (I.nd == 3) C.any3d = true;
+        I.nl = (I.nd == 3) ? I.n2 : I.n1;
+        I.nh = I.nl / 2 + 1;
+        I.nhp = (I.nh + 7) & ~7;
+        I.cells = (long long)I.n0 * I.n1 * I.n2;
+        I.rows = (int)(I.cells / I.nl);
+        I.foff = foff; foff += 9 * I.cells;
+        I.soff = soff; soff += 6 * I.cells;
+        I.coff = coff; coff += I.cells;
+        I.spoff = spoff; spoff += 9LL * I.rows * I.nhp;
+        I.rsoff = rsoff; rsoff += 9LL * I.rows;
+        LinePlan* lps[3] = {&I.lp_last, &I.lp_mid, &I.lp_first};
+        int lens[3] = {I.nl, I.nd == 3 ? I.n1 : I.n0, I.n0};
+        for (int k = 0; k < 3; ++k) {
+            if (!make_line_plan(lens[k], *lps[k])) {
+                free_plan(p);
+                return fail(CDD_ERR_SHAPE, "instance %d: no FFT plan for length %d", i, lens[k]);
+            }
+            auto it = tw_off.find(lens[k]);
+            if (it == tw_off.end()) {
+                int off = (int)twre.size();
+                for (int kk = 0; kk < lens[k]; ++kk) {
+                    long double re, im;
+                    twiddle(lens[k], kk, re, im);
+                    twre.push_back((double)re);
+                    twim.push_back((double)im);
+                }
+                it = tw_off.emplace(lens[k], off).first;
+            }
+            lps[k]->tw = it->second;
+        }
+        // k tables (FourierSpaceTools.py L26-55)
+        if (I.nd == 3) {
+            I.koff0 = (int)ktab.size();
+            for (int a = 0; a < I.n0; ++a) ktab.push_back(k_value(I.n0, I.n0, a));
+            I.koff1 = (int)ktab.size();
+            for (int a = 0; a < I.n1; ++a) ktab.push_back(k_value(I.n1, I.n1, a));
+            I.koffh = (int)ktab.size();
+            for (int a = 0; a < I.nh; ++a) ktab.push_back(k_value(I.n2, I.n2, a));
+        } else {
+            I.koff0 = (int)ktab.size();
+            for (int a = 0; a < I.n0; ++a) ktab.push_back(k_value(I.n1, I.n0, a));
+            I.koff1 = I.koff0;
+            I.koffh = (int)ktab.size();
+            for (int a = 0; a < I.nh; ++a) ktab.push_back(k_value(I.n1, I.n1, a));
+        }
+        I.mu = d.mu;
+        I.nu = d.nu;
+        I.lamb = 2. * d.mu * d.nu / (1. - 2. * d.nu);
+        I.Lambda = d.Lambda;
+        I.cfl = d.cfl;
+        I.nmax = (double)(I.n0 > I.n1 ? (I.n0 > I.n2 ? I.n0 : I.n2) : (I.n1 > I.n2 ? I.n1 : I.n2));
+        I.h = 1.0 / (double)I.nl;
+        I.inv_h = (double)I.nl;
+        I.inv_cells = 1.0 / (double)I.cells;
+        I.has_load = d.has_load ? 1 : 0;
+        for (int a = 0; a < 3; ++a) { I.load_rate[a] = d.load_rate[a]; I.load_init[a] = d.load_initial[a]; }
+        I.load_t0 = d.load_t0;
+        I.load_mu = d.load_mu;
+        I.load_lamb = 2. * d.load_mu * d.load_nu / (1. - 2. * d.load_nu);
+    }
+    C.field_elems = foff;
+    C.stress_elems = soff;
+    C.cells = coff;
+    C.spec_elems = spoff;
+    C.rows_total = rsoff;
+
+    int rc = build_shapes(p, elt);
+    if (rc != CDD_OK) { free_plan(p); return rc; }
+
+#define ALLOC_OR_FAIL(ptr, bytes)                                                               \
+    do {                                                                                        \
+        cudaError_t e_ = dalloc(p, (void**)&(ptr), (bytes));                                    \
+        if (e_ != cudaSuccess) {                                                                \
+            free_plan(p);                                                                       \
+            return fail(CDD_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", (size_t)(bytes),   \
+                        cudaGetErrorString(e_));                                                \
+        }                                                                                       \
+    } while (0)
+#define COPY_OR_FAIL(dst, src, bytes)                                                           \
+    do {                                                                                        \
+        cudaError_t e_ = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice);             \
+        if (e_ != cudaSuccess) {                                                                \
+            free_plan(p);                                                                       \
+            return fail(CDD_ERR_CUDA, "cudaMemcpy failed: %s", cudaGetErrorString(e_));         \
+        }                                                                                       \
+    } while (0)
+
+    ALLOC_OR_FAIL(C.d_inst, sizeof(InstDev) * n_inst);
+    COPY_OR_FAIL(C.d_inst, p->inst.data(), sizeof(InstDev) * n_inst);
+    ALLOC_OR_FAIL(C.d_clock, sizeof(InstClock) * n_inst);
+    {
+        std::vector<InstClock> clk(n_inst);
+        for (auto& c : clk) { std::memset(&c, 0, sizeof c); c.t_end = 1e300; }
+        COPY_OR_FAIL(C.d_clock, clk.data(), sizeof(InstClock) * n_inst);
+    }
+    const size_t ntw = twre.size();
+    if (precision == CDD_F64) {
+        std::vector<double2> tw(ntw);
+        for (size_t k = 0; k < ntw; ++k) tw[k] = make_double2(twre[k], twim[k]);
+        ALLOC_OR_FAIL(C.d_tw, sizeof(double2) * ntw);
+        COPY_OR_FAIL(C.d_tw, tw.data(), sizeof(double2) * ntw);
+        ALLOC_OR_FAIL(C.d_k, sizeof(double) * ktab.size());
+        COPY_OR_FAIL(C.d_k, ktab.data(), sizeof(double) * ktab.size());
+    } else {
+        std::vector<float2> tw(ntw);
+        for (size_t k = 0; k < ntw; ++k) tw[k] = make_float2((float)twre[k], (float)twim[k]);
+        ALLOC_OR_FAIL(C.d_tw, sizeof(float2) * ntw);
+        COPY_OR_FAIL(C.d_tw, tw.data(), sizeof(float2) * ntw);
+        std::vector<float> kf(ktab.begin(), ktab.end());
+        ALLOC_OR_FAIL(C.d_k, sizeof(float) * kf.size());
+        COPY_OR_FAIL(C.d_k, kf.data(), sizeof(float) * kf.size());
+    }
+    ALLOC_OR_FAIL(C.d_spec, 2 * elt * (size_t)C.spec_elems);
+    cudaMemset(C.d_spec, 0, 2 * elt * (size_t)C.spec_elems);
+    ALLOC_OR_FAIL(C.d_sigma, elt * (size_t)C.stress_elems);
+    ALLOC_OR_FAIL(C.d_f0, elt * (size_t)C.field_elems);
+    ALLOC_OR_FAIL(C.d_f1, elt * (size_t)C.field_elems);
+    if (precision == CDD_F32) ALLOC_OR_FAIL(C.d_rowsum, sizeof(double) * (size_t)C.rows_total);
+    ALLOC_OR_FAIL(C.d_sbar, sizeof(double) * 6 * n_inst);
+    ALLOC_OR_FAIL(C.d_bmax, sizeof(double) * (size_t)C.stencil.blocks);
+    ALLOC_OR_FAIL(C.d_bsum, sizeof(double) * 2 * (size_t)C.stencil.blocks);
+    ALLOC_OR_FAIL(C.d_obs, sizeof(double) * 2 * n_inst);
+    ALLOC_OR_FAIL(C.d_status, sizeof(int));
+    cudaMemset(C.d_status, 0, sizeof(int));
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { free_plan(p); return fail(CDD_ERR_CUDA, "plan setup: %s", cudaGetErrorString(e)); }
+    *out = p;
+    return CDD_OK;
+#undef ALLOC_OR_FAIL
+#undef COPY_OR_FAIL
+}
+
+int cdd_plan_destroy(cdd_plan* plan) {
+    if (!plan) return CDD_OK;
+    free_plan(plan);
+    return CDD_OK;
+}
+
+int cdd_plan_num_instances(const cdd_plan* p) { return p ? p->core.n_inst : 0; }
+int cdd_plan_precision(const cdd_plan* p) { return p ? p->core.precision : -1; }
+long long cdd_plan_field_elems(const cdd_plan* p) { return p ? p->core.field_elems : -1; }
+long long cdd_plan_field_offset(const cdd_plan* p, int i) {
+    return (p && i >= 0 && i < p->core.n_inst) ? p->inst[i].foff : -1;
+}
+long long cdd_plan_stress_elems(const cdd_plan* p) { return p ? p->core.stress_elems : -1; }
+long long cdd_plan_stress_offset(const cdd_plan* p, int i) {
+    return (p && i >= 0 && i < p->core.n_inst) ? p->inst[i].soff : -1;
+}
+long long cdd_plan_cells(const cdd_plan* p, int i) {
+    if (!p) return -1;
+    if (i < 0) return p->core.cells;
+    return i < p->core.n_inst ? p->inst[i].cells : -1;
+}
+long long cdd_plan_scratch_bytes(const cdd_plan* p) { return p ? p->scratch_bytes : -1; }
+
+int cdd_stress(cdd_plan* p, const void* beta, void* sigma6, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !sigma6) return fail(CDD_ERR_ARG, "null buffer");
+    CDD_CUDA(launch_stress(p->core, beta, sigma6, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_flux(cdd_plan* p, const void* beta, double t, void* rhs, void* speed, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !rhs) return fail(CDD_ERR_ARG, "null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    CDD_CUDA(launch_stress(p->core, beta, p->core.d_sigma, st));
+    CDD_CUDA(launch_stencil(p->core, M_FLUX, beta, beta, rhs, speed, t, st));
+    return CDD_OK;
+}
+
+int cdd_set_time(cdd_plan* p, const double* t, const double* t_end) {
+    if (int rc = check_plan(p)) return rc;
+    const int n = p->core.n_inst;
+    std::vector<InstClock> clk(n);
+    CDD_CUDA(cudaMemcpy(clk.data(), p->core.d_clock, sizeof(InstClock) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+        if (t) clk[i].t = t[i];
+        if (t_end) clk[i].t_end = t_end[i];
+    }
+    CDD_CUDA(cudaMemcpy(p->core.d_clock, clk.data(), sizeof(InstClock) * n, cudaMemcpyHostToDevice));
+    return CDD_OK;
+}
+
+int cdd_get_time(cdd_plan* p, double* t, double* dt_last, int* active) {
+    if (int rc = check_plan(p)) return rc;
+    const int n = p->core.n_inst;
+    std::vector<InstClock> clk(n);
+    CDD_CUDA(cudaMemcpy(clk.data(), p->core.d_clock, sizeof(InstClock) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+        if (t) t[i] = clk[i].t;
+        if (dt_last) dt_last[i] = clk[i].dt;
+        if (active) active[i] = clk[i].active;
+    }
+    return CDD_OK;
+}
+
+int cdd_step(cdd_plan* p, void* beta, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta) return fail(CDD_ERR_ARG, "null buffer");
+    return record_step(p, beta, (cudaStream_t)stream, 0, 0.0);
+}
+
+int cdd_step_fixed(cdd_plan* p, void* beta, double dt, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta) return fail(CDD_ERR_ARG, "null buffer");
+    if (!(dt >= 0)) return fail(CDD_ERR_ARG, "dt must be >= 0");
+    return record_step(p, beta, (cudaStream_t)stream, 1, dt);
+}
+
+int cdd_run(cdd_plan* p, void* beta, int n_steps, int use_graph, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || n_steps < 0) return fail(CDD_ERR_ARG, "bad arguments to cdd_run");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!use_graph) {
+        for (int k = 0; k < n_steps; ++k)
+            if (int rc = record_step(p, beta, st, 0, 0.0)) return rc;
+        return CDD_OK;
+    }
+    if (!p->graph || p->graph_beta != beta) {
+        if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+        if (!p->cap_stream) CDD_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        CDD_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int rc = record_step(p, beta, p->cap_stream, 0, 0.0);
+        cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(CDD_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&p->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(CDD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        p->graph_beta = beta;
+    }
+    for (int k = 0; k < n_steps; ++k) CDD_CUDA(cudaGraphLaunch(p->graph, st));
+    return CDD_OK;
+}
+
+int cdd_observables(cdd_plan* p, const void* beta, double* energy, double* mean_zz, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta) return fail(CDD_ERR_ARG, "null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    CDD_CUDA(launch_stress(p->core, beta, p->core.d_sigma, st));
+    CDD_CUDA(launch_observe(p->core, beta, st));
+    const int n = p->core.n_inst;
+    std::vector<double> obs(2 * n);
+    CDD_CUDA(cudaMemcpyAsync(obs.data(), p->core.d_obs, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, st));
+    CDD_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) {
+        if (energy) energy[i] = obs[2 * i];
+        if (mean_zz) mean_zz[i] = obs[2 * i + 1];
+    }
+    return CDD_OK;
+}
+
+int cdd_check_status(cdd_plan* p) {
+    if (int rc = check_plan(p)) return rc;
+    int s = 0;
+    CDD_CUDA(cudaMemcpy(&s, p->core.d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    CDD_CUDA(cudaMemset(p->core.d_status, 0, sizeof(int)));
+    if (s & ST_NONFINITE) return fail(CDD_ERR_NONFINITE, "non-finite wave speed: step not applied");
+    if (s & ST_TIMEOUT) return fail(CDD_ERR_TIMEOUT, "device wait timed out");
+    return CDD_OK;
+}
+
+}  // extern "C"

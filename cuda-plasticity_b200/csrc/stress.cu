@@ -1,0 +1,444 @@
+// Internal stress sigma(beta^P) on the device: a batched real-to-complex / complex-to-real FFT
+// pipeline with the isotropic Green's-function contraction fused into the k-space pass.
+//
+// Mathematics (PlasticityState.CalculateSigma(source='betaE') + CalculateBetaElastic,
+// Plasticity/PlasticityStates/PlasticityState.py L85-127, L357-390):
+//   betaE^(k)_ij = kmask * sum_mn T_ijmn(k) betaP^(k)_mn - betaP^(k)_ij,
+//   T_ijmn = A k_i k_j d_mn / kSq + k_i (k_m d_jn + k_n d_jm) / kSq - B k_i k_j k_m k_n / kSqSq,
+//   A = lam / (lam + 2 mu), B = 2 (lam + mu) / (lam + 2 mu), kSq += ME, kSqSq += ME,
+//   sigma_ij = lam tr(betaE) d_ij + mu (betaE_ij + betaE_ji).
+// Contracting T with betaP gives, per k point,
+//   sum_mn T_ijmn b_mn = k_i g_j,  g_j = k_j (A s / kSq - B r / kSqSq) + (p_j + q_j) / kSq,
+//   s = tr b, p_j = sum_m k_m b_mj, q_j = sum_n b_jn k_n, r = sum_m k_m q_m,
+// so the six stress components are formed directly in k space and only six inverse transforms
+// are needed. The k tables are the reference's (FourierSpaceTools.py L5-59), built on the host.
+//
+// 3-D pipeline (grid n0 x n1 x n2, last axis contiguous, spectrum rows of nhp complex):
+//   R2C rows (axis 2, two real rows per complex FFT)  -> forward FFT along axis 1
+//   -> [forward FFT along axis 0, Green contraction, inverse FFT along axis 0] in one kernel
+//   -> inverse FFT along axis 1 -> C2R rows (axis 2).
+// 2-D: R2C rows (axis 1) -> fused Green pass along axis 0 -> C2R rows.
+//
+// FP32 plans keep the k = 0 mode in FP64: the R2C pass records FP64 row sums of beta, a small
+// kernel turns their means into the mean stress -lam tr<b> d - mu (<b> + <b>^T), and the C2R pass
+// adds it after the FP32 transforms (which carry a zero k = 0 mode).
+#include "cdd_internal.cuh"
+
+namespace cdd {
+
+constexpr int ROW_THREADS = 256;
+constexpr int GREEN_THREADS = 512;
+
+__host__ __device__ inline int rows_ld(int n) { return n + (n >> 4) + 1; }
+
+// ------------------------------------------------------------------------------------------
+// R2C along the contiguous axis: pairs of real rows (a + i b) per complex FFT.
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MEAN64>
+__global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restrict__ insts, int n_inst,
+                                                  const int* __restrict__ pre,
+                                                  const T* __restrict__ beta,
+                                                  typename VecOf<T>::type* __restrict__ spec,
+                                                  const typename VecOf<T>::type* __restrict__ tw,
+                                                  double* __restrict__ rowsum) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    const int lb = blockIdx.x - pre[ii];
+    const int N = I.nl, P = I.tile[PASS_R2C].lines, ld = rows_ld(N);
+    const long long nrows = 9LL * I.rows;
+    const long long npairs = (nrows + 1) / 2;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const T* src = beta + I.foff;
+
+    for (int i = tid; i < P * N; i += nt) {
+        int pl = i / N, idx = i - pl * N;
+        long long p = (long long)lb * P + pl;
+        V z; z.x = 0; z.y = 0;
+        if (p < npairs) {
+            long long ra = 2 * p;
+            z.x = src[ra * N + idx];
+            if (ra + 1 < nrows) z.y = src[(ra + 1) * N + idx];
+        }
+        s[pl * ld + row_pad(idx)] = z;
+    }
+    __syncthreads();
+    if (MEAN64) {
+        const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+        for (int r = warp; r < 2 * P; r += nw) {
+            int pl = r >> 1;
+            long long row = ((long long)lb * P + pl) * 2 + (r & 1);
+            double acc = 0.0;
+            for (int idx = lane; idx < N; idx += 32) {
+                V z = s[pl * ld + row_pad(idx)];
+                acc += (double)((r & 1) ? z.y : z.x);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0 && row < nrows) rowsum[I.rsoff + row] = acc;
+        }
+    }
+    RowLayout lay{P, ld};
+    s = fft_lines<V, false>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
+    const int nh = I.nh;
+    V* dst = spec + I.spoff;
+    for (int i = tid; i < P * nh; i += nt) {
+        int pl = i / nh, k = i - pl * nh;
+        long long p = (long long)lb * P + pl;
+        if (p >= npairs) continue;
+        V zk = s[pl * ld + row_pad(k)];
+        int km = (k == 0) ? 0 : N - k;
+        V zm = s[pl * ld + row_pad(km)];
+        V a, b;
+        a.x = (T)0.5 * (zk.x + zm.x);
+        a.y = (T)0.5 * (zk.y - zm.y);
+        b.x = (T)0.5 * (zk.y + zm.y);
+        b.y = (T)-0.5 * (zk.x - zm.x);
+        long long ra = 2 * p;
+        dst[ra * I.nhp + k] = a;
+        if (ra + 1 < nrows) dst[(ra + 1) * I.nhp + k] = b;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// C2R along the contiguous axis for the 6 stress components (pairs of half spectra).
+// The imaginary parts of the k = 0 and Nyquist bins are dropped (numpy irfft semantics).
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MEAN64>
+__global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restrict__ insts, int n_inst,
+                                                  const int* __restrict__ pre,
+                                                  const typename VecOf<T>::type* __restrict__ spec,
+                                                  T* __restrict__ sigma,
+                                                  const typename VecOf<T>::type* __restrict__ tw,
+                                                  const double* __restrict__ sbar) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    const int lb = blockIdx.x - pre[ii];
+    const int N = I.nl, P = I.tile[PASS_C2R].lines, ld = rows_ld(N), nh = I.nh;
+    const long long nrows = 6LL * I.rows;
+    const long long npairs = (nrows + 1) / 2;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const V* src = spec + I.spoff;
+
+    for (int i = tid; i < P * nh; i += nt) {
+        int pl = i / nh, k = i - pl * nh;
+        long long p = (long long)lb * P + pl;
+        V A, B;
+        A.x = A.y = B.x = B.y = 0;
+        if (p < npairs) {
+            long long ra = 2 * p;
+            A = src[ra * I.nhp + k];
+            if (ra + 1 < nrows) B = src[(ra + 1) * I.nhp + k];
+        }
+        V z;
+        if (k == 0 || 2 * k == N) {
+            z.x = A.x; z.y = B.x;
+            s[pl * ld + row_pad(k)] = z;
+        } else {
+            z.x = A.x - B.y; z.y = A.y + B.x;
+            s[pl * ld + row_pad(k)] = z;
+            z.x = A.x + B.y; z.y = B.x - A.y;
+            s[pl * ld + row_pad(N - k)] = z;
+        }
+    }
+    __syncthreads();
+    RowLayout lay{P, ld};
+    s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
+    T* dst = sigma + I.soff;
+    for (int i = tid; i < P * N; i += nt) {
+        int pl = i / N, idx = i - pl * N;
+        long long p = (long long)lb * P + pl;
+        if (p >= npairs) continue;
+        V z = s[pl * ld + row_pad(idx)];
+        long long ra = 2 * p;
+        T va = z.x, vb = z.y;
+        if (MEAN64) {
+            va += (T)sbar[6 * ii + (int)(ra / I.rows)];
+            if (ra + 1 < nrows) vb += (T)sbar[6 * ii + (int)((ra + 1) / I.rows)];
+        }
+        dst[ra * N + idx] = va;
+        if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Complex FFT along axis 1 of a 3-D spectrum, in place, for `ncomp` components.
+// Block = (component, i0, column tile of W).
+// ------------------------------------------------------------------------------------------
+template <typename T, bool INV>
+__global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restrict__ insts, int n_inst,
+                                                 const int* __restrict__ pre,
+                                                 typename VecOf<T>::type* __restrict__ spec,
+                                                 const typename VecOf<T>::type* __restrict__ tw,
+                                                 int pass) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    int lb = blockIdx.x - pre[ii];
+    const PassTile& tl = I.tile[pass];
+    const int W = tl.lines, ta_n = tl.tiles_a;
+    const int ta = lb % ta_n; lb /= ta_n;
+    const int i0 = lb % I.n0;
+    const int c = lb / I.n0;
+    const int N = I.n1, nhp = I.nhp, nh = I.nh;
+    const int col0 = ta * W;
+    const int wv = min(W, nh - col0);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+    for (int i = tid; i < N * W; i += nt) {
+        int e = i / W, w = i - e * W;
+        V z; z.x = 0; z.y = 0;
+        if (w < wv) z = base[(long long)e * nhp + w];
+        s[i] = z;
+    }
+    __syncthreads();
+    ColLayout lay{W, W, 0};
+    s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tw, tid, nt);
+    for (int i = tid; i < N * W; i += nt) {
+        int e = i / W, w = i - e * W;
+        if (w < wv) base[(long long)e * nhp + w] = s[i];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Fused k-space pass along axis 0: forward FFT of the 9 components, Green contraction to the 6
+// stress components (scaled by 1 / cells), inverse FFT of the 6. In place on the spectrum.
+// ------------------------------------------------------------------------------------------
+template <typename T, typename V>
+__device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz, bool kzero,
+                                            T lam, T mu, T A, T B, T scale, bool drop_k0) {
+    const T k[3] = {kx, ky, kz};
+    const T ksq = kx * kx + ky * ky + kz * kz;
+    const T ikse = (T)1 / (ksq + (T)ME);
+    const T ikqe = (T)1 / (ksq * ksq + (T)ME);
+    V s1 = vadd(vadd(b[0], b[4]), b[8]);
+    V p[3], q[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        p[j].x = k[0] * b[j].x + k[1] * b[3 + j].x + k[2] * b[6 + j].x;
+        p[j].y = k[0] * b[j].y + k[1] * b[3 + j].y + k[2] * b[6 + j].y;
+        q[j].x = b[3 * j].x * k[0] + b[3 * j + 1].x * k[1] + b[3 * j + 2].x * k[2];
+        q[j].y = b[3 * j].y * k[0] + b[3 * j + 1].y * k[1] + b[3 * j + 2].y * k[2];
+    }
+    V r;
+    r.x = k[0] * q[0].x + k[1] * q[1].x + k[2] * q[2].x;
+    r.y = k[0] * q[0].y + k[1] * q[1].y + k[2] * q[2].y;
+    V cc;
+    cc.x = A * s1.x * ikse - B * r.x * ikqe;
+    cc.y = A * s1.y * ikse - B * r.y * ikqe;
+    const T mask = kzero ? (T)0 : (T)1;
+    V g[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        g[j].x = mask * (k[j] * cc.x + (p[j].x + q[j].x) * ikse);
+        g[j].y = mask * (k[j] * cc.y + (p[j].y + q[j].y) * ikse);
+    }
+    V tr;
+    tr.x = k[0] * g[0].x + k[1] * g[1].x + k[2] * g[2].x - s1.x;
+    tr.y = k[0] * g[0].y + k[1] * g[1].y + k[2] * g[2].y - s1.y;
+    const int ia[6] = {0, 0, 0, 1, 1, 2};
+    const int ja[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const int i = ia[o], j = ja[o];
+        V v;
+        v.x = mu * (k[i] * g[j].x + k[j] * g[i].x - b[3 * i + j].x - b[3 * j + i].x);
+        v.y = mu * (k[i] * g[j].y + k[j] * g[i].y - b[3 * i + j].y - b[3 * j + i].y);
+        if (i == j) { v.x += lam * tr.x; v.y += lam * tr.y; }
+        v.x *= scale;
+        v.y *= scale;
+        if (drop_k0 && kzero) { v.x = 0; v.y = 0; }
+        out[o] = v;
+    }
+}
+
+template <typename T, bool MEAN64>
+__global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restrict__ insts, int n_inst,
+                                                const int* __restrict__ pre,
+                                                typename VecOf<T>::type* __restrict__ spec,
+                                                const typename VecOf<T>::type* __restrict__ tw,
+                                                const T* __restrict__ ktab) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    int lb = blockIdx.x - pre[ii];
+    const PassTile& tl = I.tile[PASS_GREEN];
+    const int W = tl.lines, ta_n = tl.tiles_a;
+    const int ta = lb % ta_n;
+    const int i1 = lb / ta_n;          // 0 in 2-D
+    const int N = I.n0, nhp = I.nhp, nh = I.nh;
+    const int col0 = ta * W;
+    const int wv = min(W, nh - col0);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int cs = N * W + W;          // padded component stride in shared memory
+    const long long estride = (I.nd == 3) ? (long long)I.n1 * nhp : (long long)nhp;
+    const long long cstride = (long long)N * estride;
+    V* base = spec + I.spoff + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0;
+
+    for (int i = tid; i < 9 * N * W; i += nt) {
+        int c = i / (N * W);
+        int rem = i - c * N * W;
+        int e = rem / W, w = rem - e * W;
+        V z; z.x = 0; z.y = 0;
+        if (w < wv) z = base[c * cstride + e * estride + w];
+        s[c * cs + rem] = z;
+    }
+    __syncthreads();
+    V* s2 = s + 9 * cs;
+    {
+        ColLayout lay{9 * W, W, cs};
+        V* r = fft_lines<V, false>(s, s2, lay, I.lp_first, tw, tid, nt);
+        if (r != s) { V* t = s; s = s2; s2 = t; }
+    }
+    // Green contraction, one k point per thread iteration
+    const T lam = (T)I.lamb, mu = (T)I.mu;
+    const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
+    const T B = (T)(2.0 * (I.lamb + I.mu) / (I.lamb + 2.0 * I.mu));
+    const T scale = (T)I.inv_cells;
+    for (int i = tid; i < N * W; i += nt) {
+        int e = i / W, w = i - e * W;
+        int kh = col0 + w;
+        if (w >= wv) continue;
+        T kx, ky, kz;
+        bool kzero;
+        if (I.nd == 3) {
+            kx = ktab[I.koff0 + e];
+            ky = ktab[I.koff1 + i1];
+            kz = ktab[I.koffh + kh];
+            kzero = (e == 0 && i1 == 0 && kh == 0);
+        } else {
+            kx = ktab[I.koff0 + e];
+            ky = ktab[I.koffh + kh];
+            kz = (T)0;
+            kzero = (e == 0 && kh == 0);
+        }
+        V b[9], o[6];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) b[c] = s[c * cs + i];
+        green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) s[c * cs + i] = o[c];
+    }
+    __syncthreads();
+    {
+        ColLayout lay{6 * W, W, cs};
+        s = fft_lines<V, true>(s, s2, lay, I.lp_first, tw, tid, nt);
+    }
+    for (int i = tid; i < 6 * N * W; i += nt) {
+        int c = i / (N * W);
+        int rem = i - c * N * W;
+        int e = rem / W, w = rem - e * W;
+        if (w < wv) base[c * cstride + e * estride + w] = s[c * cs + rem];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP32 plans: FP64 mean of each beta component from the row sums, and the mean stress
+// sigma_bar = -lam tr<b> d - mu (<b> + <b>^T), one block per instance (fixed summation order).
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mean_stress(const InstDev* __restrict__ insts,
+                                                     const double* __restrict__ rowsum,
+                                                     double* __restrict__ sbar) {
+    const InstDev& I = insts[blockIdx.x];
+    __shared__ double red[9][8];
+    __shared__ double mean[9];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = 0; c < 9; ++c) {
+        double acc = 0.0;
+        for (long long r = tid; r < I.rows; r += blockDim.x) acc += rowsum[I.rsoff + c * (long long)I.rows + r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) red[c][warp] = acc;
+    }
+    __syncthreads();
+    if (tid < 9) {
+        double acc = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += red[tid][w];
+        mean[tid] = acc * I.inv_cells;
+    }
+    __syncthreads();
+    if (tid < 6) {
+        const int ia[6] = {0, 0, 0, 1, 1, 2};
+        const int ja[6] = {0, 1, 2, 1, 2, 2};
+        int i = ia[tid], j = ja[tid];
+        double tr = mean[0] + mean[4] + mean[8];
+        double v = -I.mu * (mean[3 * i + j] + mean[3 * j + i]);
+        if (i == j) v -= I.lamb * tr;
+        sbar[6 * blockIdx.x + tid] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Host launch sequence
+// ------------------------------------------------------------------------------------------
+template <typename T>
+static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st) {
+    typedef typename VecOf<T>::type V;
+    const bool f32 = (P.precision == CDD_F32);
+    V* spec = (V*)P.d_spec;
+    const V* tw = (const V*)P.d_tw;
+    const LaunchShape* L = P.pass;
+    if (f32) {
+        k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum);
+        k_mean_stress<<<P.n_inst, 256, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
+    } else {
+        k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr);
+    }
+    if (L[PASS_MID_F].blocks > 0)
+        k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
+    if (f32)
+        k_green<T, true><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+    else
+        k_green<T, false><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+    if (L[PASS_MID_I].blocks > 0)
+        k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
+    if (f32)
+        k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar);
+    else
+        k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st) {
+    if (P.precision == CDD_F32) return run_stress<float>(P, beta, sigma, st);
+    return run_stress<double>(P, beta, sigma, st);
+}
+
+template <typename T>
+static cudaError_t set_attr_t(size_t smem) {
+    cudaError_t e;
+    int v = (int)smem;
+    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_fft_mid<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_fft_mid<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    return cudaSuccess;
+}
+
+cudaError_t stress_set_attributes(int precision, size_t max_smem) {
+    if (precision == CDD_F32) return set_attr_t<float>(max_smem);
+    return set_attr_t<double>(max_smem);
+}
+
+}  // namespace cdd

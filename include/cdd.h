@@ -1,0 +1,144 @@
+/*
+ * cdd.h -- C ABI of the B200 continuum-dislocation-dynamics (CDD) time step.
+ *
+ * One library, libcdd.so (sm_100a), built from cuda-plasticity_b200/csrc. Every entry point takes
+ * plain pointers and sizes; device buffers are raw device pointers, streams are cudaStream_t
+ * passed as void*. No entry point allocates memory except cdd_plan_create, which allocates the
+ * plan's scratch (k-space spectra, stage buffers, reduction partials) once.
+ *
+ * Field layout ("packed field"): instances are concatenated; instance i starts at element
+ * cdd_plan_field_offset(plan, i) and holds 9 components in the order xx, xy, xz, yx, yy, yz,
+ * zx, zy, zz, each a C-order array over the grid (axis 0 = the reference's x, last axis
+ * contiguous). That is the numpy C order of the reference's per-component GridArray
+ * (Plasticity/Fields/Fields.py L247-249, Plasticity/GridArray/GridArray.py L7-13).
+ * Stress outputs use 6 symmetric components xx, xy, xz, yy, yz, zz (same per-instance base,
+ * cdd_plan_stress_offset).
+ *
+ * Element type: double for CDD_F64 plans, float for CDD_F32 plans. Time, dt, speed maxima,
+ * energies and mean strains are always double.
+ *
+ * Errors: every int-returning call returns a CDD_* status; cdd_last_error() gives a message for
+ * the calling thread's last failure. Nothing here exits the process.
+ *
+ * Concurrency: calls on one plan are stream-ordered on the stream they are given and share the
+ * plan's scratch, so two calls on the same plan must not overlap on the GPU. Different plans are
+ * independent.
+ */
+#ifndef CDD_H
+#define CDD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cdd_status {
+    CDD_OK = 0,
+    CDD_ERR_ARG = 1,          /* bad argument (null pointer, negative count, ...) */
+    CDD_ERR_SHAPE = 2,        /* unsupported grid shape */
+    CDD_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+    CDD_ERR_NONFINITE = 4,    /* a wave-speed maximum was NaN/Inf: the step was not applied */
+    CDD_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+    CDD_ERR_UNSUPPORTED = 6,  /* option not supported by this build */
+    CDD_ERR_ALLOC = 7         /* device allocation failed */
+};
+
+enum cdd_precision { CDD_F64 = 0, CDD_F32 = 1 };
+
+/* One simulation instance: grid, material, dynamics, loading and integrator parameters.
+ * Mirrors PlasticityState(gridShape, nu, mu) (Plasticity/PlasticityStates/PlasticityState.py
+ * L23-39), BetaPDynamics(Lambda) (Plasticity/FieldDynamics/CentralUpwindHJBetaPDynamics3D.py
+ * L10-23), TVDRungeKutta_FieldMover(CFLsafeFactor) (Plasticity/FieldMovers/FieldMover.py
+ * L14-18) and the applied-strain loading of UpwindLoadingBetaPDynamics (Plasticity/RunPython.py
+ * L21-26, L35-50): sigma_ii += lamb_L tr(eps) + 2 mu_L eps_i, eps = load_initial +
+ * load_rate (t - load_t0), lamb_L = 2 mu_L nu_L / (1 - 2 nu_L). */
+typedef struct cdd_instance {
+    int ndim;              /* 2 or 3 */
+    int shape[3];          /* grid; shape[2] ignored for ndim == 2. Each size even, >= 4,
+                              of the form 2^a 3^b or 2^a 5^c, <= 1024 */
+    double mu, nu;         /* shear modulus and Poisson ratio of the internal stress */
+    double Lambda;         /* 0: glide and climb; != 0: glide-projected (H_3D L195-200) */
+    double cfl;            /* CFLsafeFactor of the adaptive time step */
+    int has_load;          /* nonzero: add the applied-strain stress */
+    double load_rate[3], load_initial[3], load_t0;
+    double load_mu, load_nu;   /* stiffness the load is converted with */
+} cdd_instance;
+
+typedef struct cdd_plan cdd_plan;
+
+/* Create a plan for n_inst instances at the given precision on the current CUDA device.
+ * Allocates all scratch. Replaces the per-run header generation + make of the reference's CUDA
+ * path (Plasticity/RunCUDA.py L26-29, L194-214) and setupSystem (plasticity_kernel.cu L931-949). */
+int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_plan** out);
+int cdd_plan_destroy(cdd_plan* plan);
+
+int cdd_plan_num_instances(const cdd_plan* plan);
+int cdd_plan_precision(const cdd_plan* plan);
+/* Total elements of a packed 9-component field, and the start of instance i in it. */
+long long cdd_plan_field_elems(const cdd_plan* plan);
+long long cdd_plan_field_offset(const cdd_plan* plan, int i);
+/* Total elements of a packed 6-component stress field, and the start of instance i. */
+long long cdd_plan_stress_elems(const cdd_plan* plan);
+long long cdd_plan_stress_offset(const cdd_plan* plan, int i);
+/* Total cells over all instances, and the cells of instance i. */
+long long cdd_plan_cells(const cdd_plan* plan, int i);
+/* Bytes of device scratch the plan holds. */
+long long cdd_plan_scratch_bytes(const cdd_plan* plan);
+
+/* Internal stress sigma(beta^P) through the Fourier-space Green's function, FP64 k=0 mode.
+ * Replaces PlasticityState.CalculateSigma(type='k', source='betaE') +
+ * CalculateBetaElastic (PlasticityState.py L85-127, L357-390); reference CUDA twin
+ * calculateSigma/calculateKSigma (plasticity_kernel.cu L778-1041).
+ * beta: packed 9-component field; sigma6: packed 6-component output. */
+int cdd_stress(cdd_plan* plan, const void* beta, void* sigma6, void* stream);
+
+/* Central-upwind Hamilton-Jacobi flux with the wave speed used by the CFL condition, at time t
+ * (t sets the applied load). Replaces BetaPDynamics.CalculateFlux(time, state,
+ * CFLCondition=True) (CentralUpwindHJBetaPDynamics3D.py L218-221 ->
+ * CentralUpwindHJ3D.py L99-271); reference CUDA twin calculateFlux/centralHJ
+ * (plasticity_kernel.cu L1068-1094, L118-697).
+ * rhs: packed 9-component output; speed: one value per cell (packed, instance i at
+ * sum of previous cells), may be NULL. */
+int cdd_flux(cdd_plan* plan, const void* beta, double t, void* rhs, void* speed, void* stream);
+
+/* Per-instance clocks: t (current time) and t_end (end of the current Run interval).
+ * Host arrays of length n_inst. */
+int cdd_set_time(cdd_plan* plan, const double* t, const double* t_end);
+/* Read t, the last dt and the active flags back (synchronises the plan's last stream).
+ * Any pointer may be NULL. */
+int cdd_get_time(cdd_plan* plan, double* t, double* dt_last, int* active);
+
+/* One adaptive TVD-RK3 step of every active instance, in place on beta (device).
+ * dt = cfl / (max(shape) * max_cells(speed)), clamped so t + dt <= t_end; the three stages use
+ * the step-start time; t += dt on the device. An instance with t >= t_end is left untouched.
+ * Replaces TVDRungeKutta_FieldMover.CalculateOneAdaptiveTimeStep (FieldMover.py L61-141);
+ * reference CUDA twin TVD3rd (plasticity_kernel.cu L1139-1206). No host synchronisation. */
+int cdd_step(cdd_plan* plan, void* beta, void* stream);
+
+/* One TVD-RK3 step with a fixed dt (clamped to t_end).
+ * Replaces CalculateOneFixedTimeStep (FieldMover.py L38-58). */
+int cdd_step_fixed(cdd_plan* plan, void* beta, double dt, void* stream);
+
+/* n_steps adaptive steps; with use_graph != 0 the step is captured once into a CUDA graph
+ * (per plan, beta pointer and stream) and replayed. */
+int cdd_run(cdd_plan* plan, void* beta, int n_steps, int use_graph, void* stream);
+
+/* Elastic energy (sum over cells of 1/2 S:sigma sigma, PlasticityState.CalculateElasticEnergy
+ * L317-330 as summed in Observers/Observer.py L99) and mean beta^P_zz of every instance,
+ * accumulated in FP64. energy, mean_zz: host arrays of length n_inst (either may be NULL).
+ * Synchronises the stream. */
+int cdd_observables(cdd_plan* plan, const void* beta, double* energy, double* mean_zz,
+                    void* stream);
+
+/* Device status flags accumulated by kernels (CDD_ERR_NONFINITE, ...); clears them. */
+int cdd_check_status(cdd_plan* plan);
+
+/* Message for the calling thread's last failing call ("" if none). */
+const char* cdd_last_error(void);
+
+/* Library version string. */
+const char* cdd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CDD_H */

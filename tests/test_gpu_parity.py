@@ -1,0 +1,237 @@
+"""GPU parity of the CUDA path (libcdd.so through its C ABI) against the reference's golden vectors
+and the CPU oracle.
+
+Tolerances (FP64 form): stress and flux fields rel-L2 <= 1e-12, one step <= 1e-11, ten steps
+<= 1e-10 (the drop-in bar), energy / mean-strain curves relative 1e-8 over full runs.
+FP32 form: per-field rel-L2 <= 1e-5 after 10 steps against the FP64 form.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import cdd
+import cdd_oracle as O
+from conftest import golden_path
+
+FIELD_CASES = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_lambda", "g3d_load", "g2d_48_tend"]
+T_END = {"g2d_48_tend": 0.004}
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def inst_of(g):
+    lr = g["load_rate"]
+    return cdd.Instance(shape=tuple(int(v) for v in g["shape"]), mu=float(g["mu"]), nu=float(g["nu"]),
+                        Lambda=float(g["Lambda"]), cfl=float(g["cfl"]),
+                        load_rate=tuple(lr) if np.any(lr) else None)
+
+
+def params_of(g):
+    lr = g["load_rate"]
+    return O.Params(mu=float(g["mu"]), nu=float(g["nu"]), Lambda=float(g["Lambda"]),
+                    cfl=float(g["cfl"]), load_rate=lr if np.any(lr) else None)
+
+
+SYM = [0, 1, 2, 4, 5, 8]   # xx xy xz yy yz zz in the 9-component order
+
+
+@pytest.mark.parametrize("name", FIELD_CASES)
+def test_stress_matches_reference(name):
+    g = np.load(golden_path(name))
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([g["beta0"]])
+    s6 = plan.stress(beta)
+    torch.cuda.synchronize()
+    got = plan.stress_view(s6, 0).cpu().numpy()
+    assert rel(got, g["sigma"][SYM]) < 1e-12
+
+
+@pytest.mark.parametrize("name", FIELD_CASES)
+def test_flux_matches_reference(name):
+    g = np.load(golden_path(name))
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([g["beta0"]])
+    rhs, speed = plan.flux(beta, 0.0)
+    torch.cuda.synchronize()
+    assert rel(plan.field_view(rhs, 0).cpu().numpy(), g["rhs"]) < 1e-12
+    assert rel(speed.cpu().numpy().reshape(g["speed"].shape), g["speed"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", FIELD_CASES)
+def test_steps_match_reference(name):
+    g = np.load(golden_path(name))
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([g["beta0"]])
+    plan.set_time(0.0, T_END.get(name, 1e30))
+    plan.step(beta)
+    t, dt, act = plan.get_time()
+    assert abs(dt[0] - g["dts"][0]) <= 1e-12 * g["dts"][0]
+    assert rel(plan.field_view(beta, 0).cpu().numpy(), g["beta1"]) < 1e-11
+    for _ in range(int(g["steps"]) - 1):
+        plan.step(beta)
+    t, dt, act = plan.get_time()
+    assert rel(plan.field_view(beta, 0).cpu().numpy(), g["beta_final"]) < 1e-10
+    assert abs(t[0] - float(g["t_final"])) <= 1e-12 * float(g["t_final"])
+    plan.check_status()
+
+
+@pytest.mark.parametrize("name", ["c1_2d_128", "c2_3d_32"])
+def test_observable_curves_full_run(name):
+    """Energy and mean-strain curves over the whole run agree with the reference to 1e-8."""
+    g = np.load(golden_path(name))
+    shape = tuple(int(v) for v in g["shape"])
+    b0 = cdd.gaussian_random_field(shape, float(g["sigma_f"]), 0.05, int(g["seed"]))
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([b0])
+    plan.set_time(0.0, 1e30)
+    e, m = plan.observables(beta)
+    energies, means = [e[0]], [m[0]]
+    for _ in range(int(g["steps"])):
+        plan.step(beta)
+        e, m = plan.observables(beta)
+        energies.append(e[0])
+        means.append(m[0])
+    t, _, _ = plan.get_time()
+    np.testing.assert_allclose(energies, g["energy"], rtol=1e-8)
+    np.testing.assert_allclose(means, g["mean_zz"], rtol=1e-8, atol=1e-14)
+    assert abs(t[0] - float(g["t_final"])) <= 1e-10 * float(g["t_final"])
+    fin = plan.field_view(beta, 0).cpu().numpy().reshape(9, -1)
+    np.testing.assert_allclose((fin ** 2).sum(axis=1), g["final_sumsq"], rtol=1e-8)
+
+
+def test_batched_plan_matches_single_plans_bitwise():
+    names = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_load"]
+    gs = [np.load(golden_path(n)) for n in names]
+    batch = cdd.Plan([inst_of(g) for g in gs], "f64")
+    bb = batch.pack([g["beta0"] for g in gs])
+    batch.set_time(0.0, 1e30)
+    for _ in range(2):
+        batch.step(bb)
+    for i, g in enumerate(gs):
+        single = cdd.Plan([inst_of(g)], "f64")
+        bs = single.pack([g["beta0"]])
+        single.set_time(0.0, 1e30)
+        for _ in range(2):
+            single.step(bs)
+        assert torch.equal(batch.field_view(bb, i), single.field_view(bs, 0))
+
+
+def test_graph_run_equals_eager_steps():
+    g = np.load(golden_path("g3d_16"))
+    p1 = cdd.Plan([inst_of(g)], "f64")
+    p2 = cdd.Plan([inst_of(g)], "f64")
+    b1 = p1.pack([g["beta0"]])
+    b2 = p2.pack([g["beta0"]])
+    p1.set_time(0.0, 1e30)
+    p2.set_time(0.0, 1e30)
+    p1.run(b1, 4, graph=True)
+    for _ in range(4):
+        p2.step(b2)
+    torch.cuda.synchronize()
+    assert torch.equal(b1, b2)
+    assert np.array_equal(p1.get_time()[0], p2.get_time()[0])
+
+
+@pytest.mark.parametrize("shape", [(24, 48, 20), (40, 12), (12, 10, 16), (96, 8)])
+def test_mixed_radix_shapes_against_oracle(shape):
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 21)
+    p = O.Params(mu=1.0, nu=0.3)
+    plan = cdd.Plan([cdd.Instance(shape)], "f64")
+    beta = plan.pack([b0])
+    s6 = plan.stress(beta)
+    torch.cuda.synchronize()
+    assert rel(plan.stress_view(s6, 0).cpu().numpy(), O.stress(b0, 1.0, 0.3)[SYM]) < 1e-12
+    plan.set_time(0.0, 1e30)
+    plan.step(beta)
+    ref, dt = O.rk3_step(b0, 0.0, 1e30, p)
+    assert rel(plan.field_view(beta, 0).cpu().numpy(), ref) < 1e-11
+
+
+def test_fixed_dt_step_against_oracle():
+    g = np.load(golden_path("g3d_load"))
+    p = params_of(g)
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([g["beta0"]])
+    plan.set_time(0.1, 1e30)
+    plan.step_fixed(beta, 1.5e-3)
+    ref, _ = O.rk3_step(g["beta0"], 0.1, 1e30, p, fixed_dt=1.5e-3)
+    assert rel(plan.field_view(beta, 0).cpu().numpy(), ref) < 1e-11
+
+
+def test_uniform_state_known_answer():
+    shape = (8, 8, 8)
+    m = np.arange(1, 10, dtype=float) * 0.01
+    b0 = m.reshape(9, 1, 1, 1) * np.ones((9,) + shape)
+    plan = cdd.Plan([cdd.Instance(shape)], "f64")
+    beta = plan.pack([b0])
+    rhs, speed = plan.flux(beta)
+    s6 = plan.stress(beta)
+    torch.cuda.synchronize()
+    lamb = 2 * 0.3 / (1 - 0.6)
+    M = m.reshape(3, 3)
+    expect = (-lamb * np.trace(M) * np.eye(3) - (M + M.T)).reshape(9)[SYM]
+    got = plan.stress_view(s6, 0).cpu().numpy().reshape(6, -1)
+    np.testing.assert_allclose(got, np.repeat(expect[:, None], got.shape[1], axis=1), atol=1e-14)
+    assert float(rhs.abs().max()) == 0.0
+    np.testing.assert_allclose(speed.cpu().numpy(), 3 * O.ME)
+
+
+def test_end_time_reached_then_inactive():
+    g = np.load(golden_path("g2d_48_tend"))
+    plan = cdd.Plan([inst_of(g)], "f64")
+    beta = plan.pack([g["beta0"]])
+    plan.set_time(0.0, 0.004)
+    for _ in range(int(g["steps"])):
+        plan.step(beta)
+    t, dt, act = plan.get_time()
+    assert t[0] == 0.004
+    before = beta.clone()
+    plan.step(beta)
+    t2, dt2, act2 = plan.get_time()
+    assert not act2[0] and dt2[0] == 0.0 and t2[0] == 0.004
+    assert torch.equal(before, beta)
+
+
+def test_nonfinite_state_is_reported_and_not_applied():
+    shape = (12, 12, 12)
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 3)
+    b0[4, 3, 3, 3] = np.nan
+    plan = cdd.Plan([cdd.Instance(shape)], "f64")
+    beta = plan.pack([b0])
+    before = beta.clone()
+    plan.set_time(0.0, 1e30)
+    plan.step(beta)
+    with pytest.raises(cdd.CDDError) as ei:
+        plan.check_status()
+    assert ei.value.code == 4
+    assert torch.equal(torch.nan_to_num(before, nan=7.0), torch.nan_to_num(beta, nan=7.0))
+    plan.check_status()   # cleared
+
+
+def test_fp32_form_error_against_fp64():
+    shape = (32, 32, 32)
+    b0 = cdd.gaussian_random_field(shape, 0.04, 0.05, 5)
+    inst = cdd.Instance(shape, load_rate=(-0.025, -0.025, 0.05))
+    p64 = cdd.Plan([inst], "f64")
+    p32 = cdd.Plan([inst], "f32")
+    b64 = p64.pack([b0])
+    b32 = p32.pack([b0])
+    for p in (p64, p32):
+        p.set_time(0.0, 1e30)
+    for _ in range(10):
+        p64.step(b64)
+        p32.step(b32)
+    x64 = p64.field_view(b64, 0).cpu().numpy()
+    x32 = p32.field_view(b32, 0).cpu().numpy().astype(np.float64)
+    for c in range(9):
+        assert rel(x32[c], x64[c]) < 1e-5, c
+    e64, m64 = p64.observables(b64)
+    e32, m32 = p32.observables(b32)
+    assert abs(e32[0] - e64[0]) <= 1e-5 * abs(e64[0])
+    assert abs(m32[0] - m64[0]) <= 1e-6 * max(abs(m64[0]), 1e-3)
