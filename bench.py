@@ -1,0 +1,367 @@
+"""Benchmark of the CDD time step on B200: cell-stage updates per second.
+
+Workload (per GPU): one 3-D 256^3 periodic grid, seeded Gaussian random field (sigma 0.03 L,
+rms 0.05), mu = 1, nu = 0.3, applied strain rate diag(-0.025, -0.025, 0.05), glide and climb,
+adaptive TVD-RK3 at CFL 0.25. The headline value is the FP32 form (FP64 CFL maximum, energy /
+mean-strain sums and k = 0 mode); the plain FP64 form is measured beside it on the same input,
+together with the FP32-vs-FP64 field error after 10 steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cdd|reference]
+
+One cell-stage update = one cell through one RK3 stage (stress solve + flux + stage update);
+value = cells x 3 x steps / time. Under torchrun each rank advances its own independent grid
+(replicas; no data-path collective) and the time is the maximum over ranks.
+``--impl reference`` times the CPU oracle (a numpy restatement of the reference's Python path)
+on the host cores instead.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
+
+METRIC = "cell-stage updates/s at 256³: FP32 batched vs FP64 plain (≤1e-5 rel-L2); adj/fwd"
+UNIT = "cell-stage updates/s"
+WORDS_PER_CELL_STAGE = 48      # stress operator: read 9 + write 6; stencil + stage: read 24, write 9
+STRESS_WORDS = 15
+STENCIL_WORDS = 33
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cdd", choices=["cdd", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=64, help="grid of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def workload(size, seed):
+    import cdd
+    shape = (size, size, size)
+    inst = cdd.Instance(shape, mu=1.0, nu=0.3, Lambda=0.0, cfl=0.25,
+                        load_rate=(-0.025, -0.025, 0.05))
+    return shape, inst
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling while the GPU works."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", "clocks_bench.csv") if os.path.isdir(
+            os.path.join(REPO, "gpurun_out")) else "/dev/null"
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = open(self.path + ".tmp" if self.path != "/dev/null" else os.devnull, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            text, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            text = ""
+        rows = []
+        for line in text.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        if self.path != "/dev/null":
+            with open(self.path, "w") as fo:
+                fo.write(text)
+        if not rows:
+            return None
+        load = [r for r in rows if r[2] > 0.35 * max(x[2] for x in rows)] or rows
+        sm = sorted(r[0] for r in load)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows), "samples_under_load": len(load),
+                "power_w_max": max(r[2] for r in rows)}
+
+
+def cpu_baseline(sample):
+    """The oracle (numpy FP64 restatement of the reference path), one step on one host thread."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import cdd_oracle as O
+    from cdd.initial import gaussian_random_field
+    shape = (sample,) * 3
+    b = gaussian_random_field(shape, 0.03, 0.05, 7)
+    p = O.Params(mu=1.0, nu=0.3, cfl=0.25, load_rate=(-0.025, -0.025, 0.05))
+    t0 = time.perf_counter()
+    O.rk3_step(b, 0.0, 1e30, p)
+    dt = time.perf_counter() - t0
+    return {"value": sample ** 3 * 3 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "1 TVD-RK3 step of the numpy FP64 oracle at %d^3 (same physics and load), "
+                      "1 thread of %d host cores, %.1f s" % (sample, os.cpu_count() or 1, dt)}
+
+
+def _oracle_sample_step(args):
+    sample, seed = args
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
+    import cdd_oracle as O
+    from cdd.initial import gaussian_random_field
+    b = gaussian_random_field((sample,) * 3, 0.03, 0.05, seed)
+    p = O.Params(mu=1.0, nu=0.3, cfl=0.25, load_rate=(-0.025, -0.025, 0.05))
+    O.rk3_step(b, 0.0, 1e30, p)
+    return sample ** 3 * 3
+
+
+def run_reference(args):
+    """CPU arm: the oracle on all usable host cores, one sample grid per worker process."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        mem_gb = psutil.virtual_memory().available / 2 ** 30
+    except Exception:
+        mem_gb = 16.0
+    sample = 48
+    workers = max(1, min(cores, int(mem_gb // 1.0), 64))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        for w in range(args.warmup):
+            pool.map(_oracle_sample_step, [(sample, 100 + i) for i in range(workers)])
+        t0 = time.perf_counter()
+        units = 0
+        for s in range(args.steps):
+            units += sum(pool.map(_oracle_sample_step, [(sample, 1000 * s + i) for i in range(workers)]))
+        el = time.perf_counter() - t0
+    val = units / el
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded Gaussian random fields, sigma 0.03 L, rms 0.05",
+            "config": {"workload": "3-D CDD step, numpy FP64 oracle of the reference Python path, "
+                                   "%d worker processes x one %d^3 sample grid per step" % (workers, sample),
+                       "grid": [sample] * 3, "workers": workers},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": "%d processes x 1 step of a %d^3 grid per timed step" % (workers, sample)},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import cdd
+    from cdd.initial import gaussian_random_field_torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    K, W = args.steps, max(3, args.warmup)
+    shape, inst = workload(args.size, 100 + rank)
+    cells = int(np.prod(shape))
+    clocks = ClockSampler(local)
+
+    b0 = gaussian_random_field_torch(shape, 0.03, 0.05, 100 + rank, device=dev)   # FP64 on device
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_run(plan, beta, steps):
+        st = torch.cuda.current_stream()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(st)
+        plan.run(beta, steps, graph=True)
+        ev1.record(st)
+        barrier()
+        return ev0.elapsed_time(ev1) / 1e3
+
+    clocks.start()
+    # ---------------- FP32 form (headline) ----------------
+    p32 = cdd.Plan([inst], "f32")
+    beta32 = p32.empty_field()
+    beta32.copy_(b0.reshape(-1).to(torch.float32))
+    p32.set_time(0.0, 1e30)
+    p32.run(beta32, W, graph=True)
+    el32 = max_over_ranks(timed_run(p32, beta32, K))
+    p32.check_status()
+    rate32 = world * cells * 3 * K / el32
+    ms32 = 1e3 * el32 / K
+
+    # per-operator times (eager launches, CUDA events on the launching stream)
+    st = torch.cuda.current_stream()
+    M = 5
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    s6 = p32.empty_stress()
+    p32.stress(beta32, out=s6)
+    p32.flux(beta32)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(M):
+        p32.stress(beta32, out=s6)
+    e1.record(st)
+    for _ in range(M):
+        p32.flux(beta32, want_speed=False)
+    e2.record(st)
+    torch.cuda.synchronize()
+    t_stress = e0.elapsed_time(e1) / 1e3 / M
+    t_flux = e1.elapsed_time(e2) / 1e3 / M
+    t_stencil = max(t_flux - t_stress, 1e-9)
+
+    # ---------------- FP64 plain form and FP32 error ----------------
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        p64 = cdd.Plan([inst], "f64")
+        beta64 = p64.empty_field()
+        beta64.copy_(b0.reshape(-1))
+        p64.set_time(0.0, 1e30)
+        p64.run(beta64, W, graph=True)
+        K64 = max(3, min(K, 10))
+        el64 = max_over_ranks(timed_run(p64, beta64, K64))
+        rate64 = world * cells * 3 * K64 / el64
+        fp64 = {"value": rate64, "unit": UNIT, "ms_per_step": 1e3 * el64 / K64, "steps": K64}
+        # error of the FP32 form after 10 steps from the same state
+        beta64.copy_(b0.reshape(-1))
+        beta32.copy_(b0.reshape(-1).to(torch.float32))
+        p64.set_time(0.0, 1e30)
+        p32.set_time(0.0, 1e30)
+        p64.run(beta64, 10, graph=True)
+        p32.run(beta32, 10, graph=True)
+        torch.cuda.synchronize()
+        a = beta64.view(9, -1)
+        b = beta32.view(9, -1).to(torch.float64)
+        rels = ((a - b).norm(dim=1) / a.norm(dim=1)).cpu().numpy()
+        e64, m64 = p64.observables(beta64)
+        e32, m32 = p32.observables(beta32)
+        err = {"per_field_rel_l2_max": float(rels.max()), "per_field_rel_l2": [float(x) for x in rels],
+               "energy_rel": float(abs(e32[0] - e64[0]) / abs(e64[0])),
+               "mean_zz_abs": float(abs(m32[0] - m64[0]))}
+        del p64, beta64
+
+    # ---------------- end to end: host buffers through the public API ----------------
+    host_in = torch.empty(p32.field_elems, dtype=torch.float32, pin_memory=True)
+    host_in.copy_(b0.reshape(-1).to(torch.float32).cpu())
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    p32.set_time(0.0, 1e30)
+    Ke = max(3, min(K, 10))
+    for _ in range(2):
+        beta32.copy_(host_in, non_blocking=True)
+        p32.step(beta32)
+        host_out.copy_(beta32, non_blocking=True)
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    for _ in range(Ke):
+        beta32.copy_(host_in, non_blocking=True)
+        p32.step(beta32)
+        host_out.copy_(beta32, non_blocking=True)
+    ev1.record(st)
+    barrier()
+    ele = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    e2e = {"value": world * cells * 3 * Ke / ele, "unit": UNIT,
+           "h2d_bytes_per_step": host_in.numel() * 4, "d2h_bytes_per_step": host_out.numel() * 4,
+           "path": "cdd.Plan.step on a field copied in from pinned host memory and copied back every step"}
+    clk = clocks.stop()
+
+    if world > 1:
+        dist.barrier()
+        del p32
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peak, peak_kind = peaks()
+    stage_s = el32 / K / 3
+    achieved = WORDS_PER_CELL_STAGE * 4 * cells / stage_s / 1e9
+    launches_per_step = 3 * 6 + 3 + 2
+    line = {
+        "metric": METRIC, "value": rate32, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded Gaussian random field per rank (sigma 0.03 L, rms 0.05), generated on device",
+        "config": {"workload": "3-D %d^3 CDD step, FP32 form, 1 instance per GPU" % args.size,
+                   "grid": list(shape), "mu": 1.0, "nu": 0.3, "cfl": 0.25, "Lambda": 0.0,
+                   "strain_rate": [-0.025, -0.025, 0.05], "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (FP32 field %.0f MB)" % (9 * cells * 4 / 1e6),
+                   "timing": "CUDA graph of whole steps, CUDA events, max over ranks"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "kernel": "one RK3 stage (stress FFT passes + stencil/stage kernel)",
+                     "algorithmic_bytes_per_cell_stage": WORDS_PER_CELL_STAGE * 4,
+                     "traffic": None,
+                     "per_operator": {
+                         "stress_fft": {"ms": 1e3 * t_stress, "GBps": STRESS_WORDS * 4 * cells / t_stress / 1e9},
+                         "stencil_stage": {"ms": 1e3 * t_stencil,
+                                           "GBps": STENCIL_WORDS * 4 * cells / t_stencil / 1e9}}},
+        "gpu_launches": launches_per_step * K,
+        "e2e": e2e,
+        "clocks": clk,
+        "fp64_plain": fp64,
+        "fp32_over_fp64": (rate32 / fp64["value"]) if fp64 else None,
+        "fp32_error_10_steps": err,
+        "adj_over_fwd": None,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()
