@@ -74,6 +74,8 @@ _PROTOS = {
     "cdd_observables": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "cdd_check_status": (ctypes.c_int, [ctypes.c_void_p]),
+    "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_last_error": (ctypes.c_char_p, []),
     "cdd_version": (ctypes.c_char_p, []),
 }

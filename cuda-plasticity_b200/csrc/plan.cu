@@ -248,6 +248,11 @@ int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_f
 
 }  // namespace
 
+namespace cdd {
+// Lets other translation units report through cdd_last_error().
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace cdd
+
 extern "C" {
 
 const char* cdd_last_error(void) { return g_last_error.c_str(); }
