@@ -1,5 +1,6 @@
 // Internal declarations shared by the libcdd translation units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -8,6 +9,7 @@
 namespace cdd {
 
 constexpr int MAX_STAGES = 12;
+#define CDD_MAX_TMA_INSTANCES 16
 constexpr double ME = 2.220446049250313080847263336181640625e-16;   // DBL_EPSILON
 
 // One-dimensional FFT of length n as a sequence of Stockham stages of radix 2, 3, 4, 5, 8, 16.
@@ -48,6 +50,8 @@ struct InstDev {
     int koff0, koff1, koffh;    // k tables: axis 0, axis 1 (3-D), half axis (last)
     PassTile tile[NUM_PASSES];
     int stencil_blocks;
+    int st_zc;              // planes per stencil block along axis 0 (3-D)
+    int tma_slot;           // index of this instance's tensor map, -1: threads stage the planes
     double mu, nu, lamb, Lambda, cfl, nmax;
     double h, inv_h;        // Dx = 1 / shape[-1] (CentralUpwindHJ3D.py L15-16)
     double inv_cells;
@@ -323,7 +327,7 @@ struct PlanCore {
     void* d_f0 = nullptr;            // stage-1 rhs / F0
     void* d_f1 = nullptr;            // F1
     double* d_rowsum = nullptr;      // FP32 path: FP64 per-row sums
-    double* d_sbar = nullptr;        // FP32 path: FP64 mean stress per instance (6)
+    double* d_sbar = nullptr;        // FP32 path: FP64 mean of each beta component (9 per instance)
     double* d_bmax = nullptr;        // per-block wave-speed maxima
     double* d_bsum = nullptr;        // per-block energy and mean-zz partial sums (2 per block)
     double* d_obs = nullptr;         // per-instance energy, mean zz (2 per instance)
@@ -331,6 +335,13 @@ struct PlanCore {
     LaunchShape pass[NUM_PASSES];
     LaunchShape stencil;
     LaunchShape cellwise;            // elementwise kernels over cells
+    LaunchShape obs;                 // observables: one thread per cell
+};
+
+// Tensor maps of one stage-input buffer for the TMA-staged instances (see stencil.cu).
+struct StencilMapSet {
+    int enabled = 0;
+    CUtensorMap m[CDD_MAX_TMA_INSTANCES];
 };
 
 // stress.cu
@@ -338,11 +349,17 @@ cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cuda
 // stencil.cu
 enum StencilMode { M_FLUX = 0, M_STAGE1 = 1, M_STAGE2 = 2, M_STAGE3 = 3 };
 cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,
-                           void* speed, double t_flux, cudaStream_t st);
+                           void* speed, double t_flux, const StencilMapSet& maps, cudaStream_t st);
+// Encode the tensor maps of buffer `base` for every instance with tma_slot >= 0; returns false
+// (and leaves maps disabled) if the driver entry point is missing or an address is misaligned.
+bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* base, StencilMapSet& maps);
+bool stencil_tma_eligible(const InstDev& I, int precision);
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
 cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaStream_t st);
 cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st);
-cudaError_t stencil_set_attributes(int precision);
+cudaError_t stencil_set_attributes(int precision, size_t smem);
+size_t stencil_smem_bytes(int precision, bool any3d);
+void stencil_geometry(InstDev& I);
 cudaError_t stress_set_attributes(int precision, size_t max_smem);
 
 }  // namespace cdd

@@ -233,7 +233,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     const size_t off_k = align256(off_tw + velt * twre.size());
     const size_t off_rs = align256(off_k + elt * ktab.size());
     const size_t off_sbar = align256(off_rs + (f64 ? 0 : sizeof(double) * 9 * (size_t)I.rows));
-    const size_t off_spec = align256(off_sbar + sizeof(double) * 6);
+    const size_t off_spec = align256(off_sbar + sizeof(double) * 9);
     const size_t total = off_spec + velt * 9 * (size_t)I.rows * I.nhp;
     if (total > (size_t)CDD_STRESS_NOALLOC_MAX_BYTES)
         return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: grid needs " + std::to_string(total) +

@@ -119,6 +119,8 @@ struct cdd_plan {
     cudaGraphExec_t graph = nullptr;
     const void* graph_beta = nullptr;
     int device = 0;
+    StencilMapSet maps_f0, maps_f1, maps_user;   // tensor maps of the stage inputs
+    const void* maps_user_ptr = nullptr;
 };
 
 namespace {
@@ -146,11 +148,13 @@ int build_shapes(cdd_plan* p, size_t elt) {
     const int n = C.n_inst;
     const size_t velt = 2 * elt;
     std::vector<int> pre[NUM_PASSES];
-    std::vector<int> pre_st, pre_cw;
+    std::vector<int> pre_st, pre_cw, pre_ob;
     for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(0);
     pre_st.push_back(0);
     pre_cw.push_back(0);
+    pre_ob.push_back(0);
     size_t smem_max[NUM_PASSES] = {0, 0, 0, 0, 0};
+    int n_tma = 0;
     int thr_max[NUM_PASSES] = {0, 0, 0, 0, 0};
     for (int i = 0; i < n; ++i) {
         InstDev& I = p->inst[i];
@@ -202,8 +206,11 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }
         for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(pre[k].back() + I.tile[k].blocks);
-        I.stencil_blocks = (int)((I.cells + 127) / 128);
+        stencil_geometry(I);
+        I.tma_slot = -1;
+        if (stencil_tma_eligible(I, C.precision) && n_tma < CDD_MAX_TMA_INSTANCES) I.tma_slot = n_tma++;
         pre_st.push_back(pre_st.back() + I.stencil_blocks);
+        pre_ob.push_back(pre_ob.back() + (int)((I.cells + 255) / 256));
         pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));
     }
     size_t smem_all = 0;
@@ -217,7 +224,13 @@ int build_shapes(cdd_plan* p, size_t elt) {
         CDD_CUDA(cudaMemcpy(L.d_pre, pre[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     }
     C.stencil.blocks = pre_st.back();
-    C.stencil.threads = 128;
+    C.stencil.threads = 256;
+    C.stencil.smem = stencil_smem_bytes(C.precision, C.any3d);
+    CDD_CUDA(stencil_set_attributes(C.precision, C.stencil.smem < 48 * 1024 ? 48 * 1024 : C.stencil.smem));
+    C.obs.blocks = pre_ob.back();
+    C.obs.threads = 256;
+    CDD_CUDA(dalloc(p, (void**)&C.obs.d_pre, sizeof(int) * (n + 1)));
+    CDD_CUDA(cudaMemcpy(C.obs.d_pre, pre_ob.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     CDD_CUDA(dalloc(p, (void**)&C.stencil.d_pre, sizeof(int) * (n + 1)));
     CDD_CUDA(cudaMemcpy(C.stencil.d_pre, pre_st.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     C.cellwise.blocks = pre_cw.back();
@@ -233,16 +246,25 @@ int check_plan(const cdd_plan* p) {
     return CDD_OK;
 }
 
+const StencilMapSet& user_maps(cdd_plan* p, const void* beta) {
+    if (p->maps_user_ptr != beta) {
+        encode_stencil_maps(p->core, p->inst.data(), beta, p->maps_user);
+        p->maps_user_ptr = beta;
+    }
+    return p->maps_user;
+}
+
 int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_fixed) {
     PlanCore& C = p->core;
+    const StencilMapSet& mu = user_maps(p, beta);
     CDD_CUDA(launch_stress(C, beta, C.d_sigma, st));
-    CDD_CUDA(launch_stencil(C, M_STAGE1, beta, beta, C.d_f0, nullptr, 0.0, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE1, beta, beta, C.d_f0, nullptr, 0.0, mu, st));
     CDD_CUDA(launch_dt(C, fixed, dt_fixed, st));
     CDD_CUDA(launch_axpy_f0(C, beta, C.d_f0, st));
     CDD_CUDA(launch_stress(C, C.d_f0, C.d_sigma, st));
-    CDD_CUDA(launch_stencil(C, M_STAGE2, C.d_f0, beta, C.d_f1, nullptr, 0.0, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE2, C.d_f0, beta, C.d_f1, nullptr, 0.0, p->maps_f0, st));
     CDD_CUDA(launch_stress(C, C.d_f1, C.d_sigma, st));
-    CDD_CUDA(launch_stencil(C, M_STAGE3, C.d_f1, beta, beta, nullptr, 0.0, st));
+    CDD_CUDA(launch_stencil(C, M_STAGE3, C.d_f1, beta, beta, nullptr, 0.0, p->maps_f1, st));
     return CDD_OK;
 }
 
@@ -419,12 +441,14 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
     ALLOC_OR_FAIL(C.d_f0, elt * (size_t)C.field_elems);
     ALLOC_OR_FAIL(C.d_f1, elt * (size_t)C.field_elems);
     if (precision == CDD_F32) ALLOC_OR_FAIL(C.d_rowsum, sizeof(double) * (size_t)C.rows_total);
-    ALLOC_OR_FAIL(C.d_sbar, sizeof(double) * 6 * n_inst);
+    ALLOC_OR_FAIL(C.d_sbar, sizeof(double) * 9 * n_inst);
     ALLOC_OR_FAIL(C.d_bmax, sizeof(double) * (size_t)C.stencil.blocks);
-    ALLOC_OR_FAIL(C.d_bsum, sizeof(double) * 2 * (size_t)C.stencil.blocks);
+    ALLOC_OR_FAIL(C.d_bsum, sizeof(double) * 2 * (size_t)(C.stencil.blocks > C.obs.blocks ? C.stencil.blocks : C.obs.blocks));
     ALLOC_OR_FAIL(C.d_obs, sizeof(double) * 2 * n_inst);
     ALLOC_OR_FAIL(C.d_status, sizeof(int));
     cudaMemset(C.d_status, 0, sizeof(int));
+    encode_stencil_maps(C, p->inst.data(), C.d_f0, p->maps_f0);
+    encode_stencil_maps(C, p->inst.data(), C.d_f1, p->maps_f1);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { free_plan(p); return fail(CDD_ERR_CUDA, "plan setup: %s", cudaGetErrorString(e)); }
     *out = p;
@@ -468,7 +492,7 @@ int cdd_flux(cdd_plan* p, const void* beta, double t, void* rhs, void* speed, vo
     if (!beta || !rhs) return fail(CDD_ERR_ARG, "null buffer");
     cudaStream_t st = (cudaStream_t)stream;
     CDD_CUDA(launch_stress(p->core, beta, p->core.d_sigma, st));
-    CDD_CUDA(launch_stencil(p->core, M_FLUX, beta, beta, rhs, speed, t, st));
+    CDD_CUDA(launch_stencil(p->core, M_FLUX, beta, beta, rhs, speed, t, user_maps(p, beta), st));
     return CDD_OK;
 }
 

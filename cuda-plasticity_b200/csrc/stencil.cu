@@ -22,50 +22,115 @@
 // contracts to 6 scalars G[d][s] and 18 scalars Q[i][s][l] (sums of w V over the corners with a
 // given sign on one axis). No per-corner H or derivative tensor is formed. The derivatives are
 // computed one tensor column (j) at a time, twice: pass 1 accumulates A, P, C; pass 2 forms rhs.
+#include <cudaTypedefs.h>
+
 #include "cdd_internal.cuh"
 
 namespace cdd {
 
-template <typename T> __device__ __forceinline__ T mm3(T a, T b, T c) {
-    // NumericalMethods.MinMod3 (L367-378) for finite inputs: the smallest if all are positive,
-    // the largest if none is positive, else 0.
-    if (a > (T)0 && b > (T)0 && c > (T)0) return fmin(a, fmin(b, c));
-    if (!(a > (T)0) && !(b > (T)0) && !(c > (T)0)) return fmax(a, fmax(b, c));
-    return (T)0;
+// The limiter of FindDerivatives is MinMod3(D1_i, D2_i, D1_{i-1}) (NumericalMethods.py L367-378)
+// with D2_i = (D1_i + D1_{i-1}) / 2: the middle argument is the mean of the outer two. It has the
+// sign of both when they agree and its magnitude is never below the smaller of theirs (also after
+// rounding: fl(a + c) / 2 >= min(a, c) for a, c > 0), so the 3-way minmod equals the 2-way one:
+// min(|a|, |c|) with their common sign, 0 when the signs differ or one is zero.
+template <typename T> __device__ __forceinline__ T minmod2(T a, T c) {
+    const T m = fmin(fabs(a), fabs(c));
+    const bool pos = (a > (T)0) & (c > (T)0);
+    const bool neg = (a < (T)0) & (c < (T)0);
+    return pos ? m : (neg ? -m : (T)0);
 }
 
-struct Nbr {     // offsets of the +-1, +-2 neighbours along one axis (periodic)
-    long long p1, p2, m1, m2;
+// 1/sqrt and division: FP32 uses the hardware approximations (<= 2 ulp), FP64 exact ones.
+__device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double inv_sqrt(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+
+// Shared-memory tiles of the 2.5-D march: a block owns TXS x TYS cells of a plane (last axis x
+// contiguous) and walks along axis 0 (3-D). Each staged plane holds all 9 components of a box of
+// RY rows (2-row halo in y) by RX columns starting OX cells left of the tile: RX/OX keep the box's
+// x origin on a 16-byte boundary (TMA), i.e. 40/4 for FP32 and 36/2 for FP64.
+constexpr int TXS = 32, TYS = 4, RY = TYS + 4;
+constexpr int ST_THREADS = TXS * TYS;
+template <typename T> struct TileGeom;
+template <> struct TileGeom<float> { static constexpr int RX = 40, OX = 4, NS = 6; };
+template <> struct TileGeom<double> { static constexpr int RX = 36, OX = 2, NS = 5; };
+template <typename T> __host__ __device__ constexpr int tile_pp() { return RY * TileGeom<T>::RX; }   // per component
+
+template <typename T, int ND>
+struct TileView {
+    static constexpr int RX = TileGeom<T>::RX, PP = tile_pp<T>();
+    const T* sm;       // shared memory base
+    int so[5];         // element offsets of the ring planes z-2 .. z+2 (3-D); so[2] = current plane
+    int idx;           // in-plane offset of this thread's cell (halo included)
+    __device__ __forceinline__ T center(int c) const { return sm[so[2] + c * PP + idx]; }
+    __device__ __forceinline__ void load5(int c, int d, T* v) const {
+        if (ND == 3 && d == 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) v[q] = sm[so[q] + c * PP + idx];
+        } else {
+            const int st = (d == ND - 1) ? 1 : RX;
+            const T* p = sm + so[2] + c * PP + idx;
+            v[0] = p[-2 * st]; v[1] = p[-st]; v[2] = p[0]; v[3] = p[st]; v[4] = p[2 * st];
+        }
+    }
 };
 
-__device__ __forceinline__ Nbr make_nbr(int i, int n, long long stride) {
-    int ip1 = (i + 1 == n) ? 0 : i + 1;
-    int ip2 = (ip1 + 1 == n) ? 0 : ip1 + 1;
-    int im1 = (i == 0) ? n - 1 : i - 1;
-    int im2 = (im1 == 0) ? n - 1 : im1 - 1;
-    Nbr r;
-    r.p1 = (long long)(ip1 - i) * stride;
-    r.p2 = (long long)(ip2 - i) * stride;
-    r.m1 = (long long)(im1 - i) * stride;
-    r.m2 = (long long)(im2 - i) * stride;
-    return r;
+// ---- TMA and mbarrier primitives (inline PTX, sm_100a) ----
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^22 polls (well above any TMA latency) and reports false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); ++i) {
+        if (mbar_test(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                            int z, int c) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(smem_addr(bar))
+        : "memory");
 }
 
-// u+ and u- of one component along one axis.
+// u+ and u- from the five values u_{-2} .. u_{+2} along one axis. The limiter arguments D1, D2
+// of FindDerivatives all carry 1/h^2; minmod is positively homogeneous, so the kernel limits the
+// undivided second differences and applies 1/h once: u+ = (d_0 - mm/2) / h, u- = (d_-1 + mm_-1/2) / h.
 template <typename T>
-__device__ __forceinline__ void derivs(const T* __restrict__ p, T u0, const Nbr& nb, T ih, T ih2,
-                                       T hh, T& up, T& um) {
-    T um2 = __ldg(p + nb.m2), um1 = __ldg(p + nb.m1), up1 = __ldg(p + nb.p1), up2 = __ldg(p + nb.p2);
-    T dm2 = um1 - um2, dm1 = u0 - um1, d0 = up1 - u0, d1 = up2 - up1;
-    T D1_0 = (d1 - d0) * ih2;
-    T D2_0 = (d1 - dm1) * ih2 * (T)0.5;
-    T D1_m1 = (d0 - dm1) * ih2;
-    T D2_m1 = (d0 - dm2) * ih2 * (T)0.5;
-    T D1_m2 = (dm1 - dm2) * ih2;
-    T dd0 = mm3(D1_0, D2_0, D1_m1);
-    T ddm = mm3(D1_m1, D2_m1, D1_m2);
-    up = d0 * ih - hh * dd0;
-    um = dm1 * ih + hh * ddm;
+__device__ __forceinline__ void derivs5(const T* v, T ih, T& up, T& um) {
+    const T dm2 = v[1] - v[0], dm1 = v[2] - v[1], d0 = v[3] - v[2], d1 = v[4] - v[3];
+    const T e0 = d1 - d0, em1 = d0 - dm1, em2 = dm1 - dm2;
+    const T dd0 = minmod2(e0, em1);
+    const T ddm = minmod2(em1, em2);
+    up = (d0 - (T)0.5 * dd0) * ih;
+    um = (dm1 + (T)0.5 * ddm) * ih;
 }
 
 template <typename T>
@@ -101,37 +166,14 @@ __device__ __forceinline__ void applied_load(const InstDev& I, double t, double*
     for (int i = 0; i < 3; ++i) add[i] = I.load_lamb * tr + 2.0 * I.load_mu * eps[i];
 }
 
-constexpr int ST_THREADS = 128;
-
 template <typename T, int ND, int MODE>
-__device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long cell,
-                                             const T* __restrict__ bs, const T* bn, T* out,
+__device__ __forceinline__ void stencil_cell(const InstDev& I, int ii, long long cl, bool valid,
+                                             const TileView<T, ND>& tv, const T* bn, T* out,
                                              const T* __restrict__ sig, T* __restrict__ speed_out,
                                              const InstClock* __restrict__ clk, double t_flux,
-                                             double* __restrict__ bmax, double* __restrict__ bsum,
-                                             double* red) {
-    const bool valid = cell < I.cells;
-    const long long cl = valid ? cell : 0;
-
-    // neighbour offsets
-    Nbr nb[ND];
-    if (ND == 3) {
-        int i2 = (int)(cl % I.n2);
-        long long r = cl / I.n2;
-        int i1 = (int)(r % I.n1);
-        int i0 = (int)(r / I.n1);
-        nb[0] = make_nbr(i0, I.n0, (long long)I.n1 * I.n2);
-        nb[1] = make_nbr(i1, I.n1, I.n2);
-        if (ND == 3) nb[ND - 1] = make_nbr(i2, I.n2, 1);
-    } else {
-        int i1 = (int)(cl % I.n1);
-        int i0 = (int)(cl / I.n1);
-        nb[0] = make_nbr(i0, I.n0, I.n1);
-        nb[ND - 1] = make_nbr(i1, I.n1, 1);
-    }
+                                             double& vmax, double& esum, double& zsum) {
     const T ih = (T)I.inv_h, ih2 = (T)(I.inv_h * I.inv_h), hh = (T)(0.5 * I.h);
     const long long cells = I.cells;
-    const T* u = bs + I.foff + cl;
 
     // total stress at the cell: internal + applied load (FP64), symmetric
     // load time: the step-start time in all three stages (FieldMover.py L62, L123, L133); stage 1
@@ -175,15 +217,29 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
 #pragma unroll
             for (int b = 0; b < 2; ++b) Cp[p][a][b] = 0;
 
-#pragma unroll 1
+    // FP32 keeps all 54 one-sided derivatives in registers for pass 2; FP64 recomputes them
+    // from shared memory (register budget).
+    constexpr bool KEEPU = (sizeof(T) == 4);
+    T Ukeep[KEEPU ? ND : 1][2][9];
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
         T U[ND][2][3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-            const T* pc = u + (long long)(3 * l + j) * cells;
-            T u0 = __ldg(pc);
 #pragma unroll
-            for (int d = 0; d < ND; ++d) derivs(pc, u0, nb[d], ih, ih2, hh, U[d][0][l], U[d][1][l]);
+            for (int d = 0; d < ND; ++d) {
+                T v5[5];
+                tv.load5(3 * l + j, d, v5);
+                derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+            }
+        }
+        if constexpr (KEEPU) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) Ukeep[d][s][3 * l + j] = U[d][s][l];
         }
         T Sj[3], Sdj[3];
 #pragma unroll
@@ -246,7 +302,7 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
                    - (T)2 * (Cp[0][sx][sy] + Cp[1 % NP][sy][sz] + Cp[2 % NP][sz][sx]);
         else
             rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] - (T)2 * Cp[0][sx][sy];
-        T inv = (T)1 / sqrt(rho2);
+        T inv = inv_sqrt(rho2);
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
             T a = A[0][sx][l] + A[1][sy][l];
@@ -288,10 +344,10 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
             for (int d = 0; d < ND; ++d) Q[d][sg[d]][l] += wv;
         }
     }
-    T inv_abc = (T)1 / (ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
+    T inv_abc = fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
     T coef[ND];
 #pragma unroll
-    for (int d = 0; d < ND; ++d) coef[d] = pm[d] * pp[d] / tot[d];
+    for (int d = 0; d < ND; ++d) coef[d] = fdiv(pm[d] * pp[d], tot[d]);
     T spd = tot[0] + tot[1];
     if (ND == 3) spd += tot[2 % ND];
     if (vsum != vsum) spd = vsum;
@@ -308,15 +364,26 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
                 Jp += qdd * trU[d][s];
             }
     }
-#pragma unroll 1
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
         T U[ND][2][3];
+        if constexpr (KEEPU) {
 #pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            const T* pc = u + (long long)(3 * l + j) * cells;
-            T u0 = __ldg(pc);
+            for (int d = 0; d < ND; ++d)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) derivs(pc, u0, nb[d], ih, ih2, hh, U[d][0][l], U[d][1][l]);
+                for (int s = 0; s < 2; ++s)
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
+        } else {
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T v5[5];
+                    tv.load5(3 * l + j, d, v5);
+                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                }
+            }
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
@@ -371,27 +438,16 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
             T* o = out + I.foff + cl;
 #pragma unroll
             for (int c = 0; c < 9; ++c) o[c * cells] = rhs[c];
-        }
-        double v = (double)spd;
-        if (!(v <= 1.0e300)) v = __longlong_as_double(0x7ff0000000000000LL);   // NaN/Inf -> +Inf
-        if (!valid) v = 0.0;
-        double m = block_reduce_max(v, red);
-        // observables of the step-start state: elastic energy of the internal stress, mean b_zz
-        double e = 0.0, z = 0.0;
-        if (valid) {
+            double v = (double)spd;
+            if (!(v <= 1.0e300)) v = __longlong_as_double(0x7ff0000000000000LL);   // NaN/Inf -> +Inf
+            vmax = fmax(vmax, v);
+            // observables of the step-start state: elastic energy of the internal stress, mean b_zz
             double s0 = (double)sp[0], s1 = (double)sp[cells], s2 = (double)sp[2 * cells];
             double s3 = (double)sp[3 * cells], s4 = (double)sp[4 * cells], s5 = (double)sp[5 * cells];
             double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
             double tr = s0 + s3 + s5;
-            e = (sq - I.nu / (1.0 + I.nu) * tr * tr) / (4.0 * I.mu);
-            z = (double)u[8 * cells];
-        }
-        double es = block_reduce_sum(e, red);
-        double zs = block_reduce_sum(z, red);
-        if (threadIdx.x == 0) {
-            bmax[blockIdx.x] = m;
-            bsum[2 * blockIdx.x] = es;
-            bsum[2 * blockIdx.x + 1] = zs;
+            esum += (sq - I.nu / (1.0 + I.nu) * tr * tr) / (4.0 * I.mu);
+            zsum += (double)tv.center(8);
         }
     } else {
         if (valid && clk[ii].active) {
@@ -401,10 +457,9 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
             T vn[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
-            const T* us = bs + I.foff + cl;
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
-                T vs = us[c * cells];
+                T vs = tv.center(c);
                 T L = dt * rhs[c];
                 T r;
                 if (MODE == M_STAGE2) r = (T)0.75 * vn[c] + (T)0.25 * vs + (T)0.25 * L;
@@ -415,20 +470,177 @@ __device__ __forceinline__ void stencil_body(const InstDev& I, int ii, long long
     }
 }
 
+// One block: a TXS x TYS tile of planes [z0, z0 + zc) (3-D) or of the single plane (2-D).
+// The 3-D ring holds planes z-2 .. z+2 of all 9 components of beta_s (NS slots). With TMA
+// (I.tma_slot >= 0) one 4-D bulk-tensor copy stages a whole plane box; coordinates outside the
+// grid read zeros, and tiles whose box crosses the periodic boundary patch those cells with
+// wrapped loads after the copy lands. FP32 (6 slots) prefetches plane z+3 while computing z;
+// FP64 (5 slots) refills the slot of z-2 after computing z. Otherwise threads load the box.
+template <typename T, int ND, int MODE>
+__device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, double* red, uint64_t* bars,
+                                      const StencilMapSet& maps,
+                                      const T* __restrict__ bs, const T* bn, T* out,
+                                      const T* __restrict__ sig, T* __restrict__ speed_out,
+                                      const InstClock* __restrict__ clk, double t_flux,
+                                      double* __restrict__ bmax, double* __restrict__ bsum,
+                                      int* __restrict__ status) {
+    constexpr int RX = TileGeom<T>::RX, OX = TileGeom<T>::OX, PP = tile_pp<T>();
+    constexpr int NS = (ND == 3) ? TileGeom<T>::NS : 1;
+    constexpr uint32_t PLANE_BYTES = 9u * PP * sizeof(T);
+    const int nZ = (ND == 3) ? I.n0 : 1;
+    const int nY = (ND == 3) ? I.n1 : I.n0;
+    const int nX = (ND == 3) ? I.n2 : I.n1;
+    const int tXn = (nX + TXS - 1) / TXS, tYn = (nY + TYS - 1) / TYS;
+    int b = lb;
+    const int bx = b % tXn; b /= tXn;
+    const int by = b % tYn; b /= tYn;
+    const int z0 = b * I.st_zc;
+    const int z1 = min(z0 + I.st_zc, nZ);
+    const int tid = threadIdx.x, tx = tid % TXS, ty = tid / TXS;
+    const int x0 = bx * TXS, y0 = by * TYS;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool vxy = (x < nX) && (y < nY);
+    const long long cells = I.cells;
+    const long long plane = (long long)nY * nX;
+    const T* src = bs + I.foff;
+    const bool use_tma = (ND == 3) && maps.enabled && (I.tma_slot >= 0);
+    const bool edge = (x0 - OX < 0) || (x0 - OX + RX > nX) || (y0 - 2 < 0) || (y0 - 2 + RY > nY);
+
+    auto wrapz = [&](int z) { while (z < 0) z += nZ; while (z >= nZ) z -= nZ; return z; };
+    // Fill (all = true) or patch the out-of-grid cells (all = false) of the box of plane zp.
+    auto load_box = [&](int slot, int zp, bool all) {
+        T* dst = sm + slot * 9 * PP;
+        const T* sp0 = src + (long long)zp * plane;
+        for (int e = tid; e < 9 * PP; e += ST_THREADS) {
+            const int c = e / PP;
+            const int r = e - c * PP;
+            const int iy = r / RX, ix = r - iy * RX;
+            int yy = y0 - 2 + iy, xx = x0 - OX + ix;
+            if (!all && yy >= 0 && yy < nY && xx >= 0 && xx < nX) continue;
+            while (yy < 0) yy += nY;
+            while (yy >= nY) yy -= nY;
+            while (xx < 0) xx += nX;
+            while (xx >= nX) xx -= nX;
+            dst[e] = __ldg(sp0 + c * cells + (long long)yy * nX + xx);
+        }
+    };
+    // plane with relative index pr (= z - (z0 - 2)) lives in slot pr % NS
+    auto issue = [&](int pr) {
+        const int slot = pr % NS;
+        mbar_expect_tx(&bars[slot], PLANE_BYTES);
+        tma_load_4d(sm + slot * 9 * PP, &maps.m[I.tma_slot], &bars[slot], x0 - OX, y0 - 2,
+                    wrapz(z0 - 2 + pr), 0);
+    };
+    int ok = 1;
+    auto arrive = [&](int pr) {   // wait for plane pr and patch it; block-uniform result in ok
+        if (!ok) return;
+        const int slot = pr % NS;
+        bool got = mbar_wait(&bars[slot], (uint32_t)((pr / NS) & 1));
+        if (__syncthreads_or(!got)) {
+            ok = 0;
+            if (tid == 0) atomicOr(status, (int)ST_TIMEOUT);
+            return;
+        }
+        if (edge) load_box(slot, wrapz(z0 - 2 + pr), false);
+    };
+
+    int issued = -1;   // highest plane index handed to TMA
+    if (use_tma) {
+        if (tid == 0) {
+#pragma unroll 1
+            for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int pr = 0; pr < 5; ++pr) issue(pr);
+        issued = 4;
+#pragma unroll 1
+        for (int pr = 0; pr < 5; ++pr) arrive(pr);
+    } else if (ND == 3) {
+#pragma unroll 1
+        for (int q = 0; q < 5; ++q) load_box(q, wrapz(z0 - 2 + q), true);
+    } else {
+        load_box(0, 0, true);
+    }
+    __syncthreads();
+    double vmax = 0.0, esum = 0.0, zsum = 0.0;
+    TileView<T, ND> tv;
+    tv.sm = sm;
+    tv.idx = (ty + 2) * RX + tx + OX;
+#pragma unroll 1
+    for (int z = z0, k = 0; ok && z < z1; ++z, ++k) {
+        const bool more = (z + 1 < z1);
+        if (use_tma && NS == 6 && more && tid == 0) {
+            fence_proxy_async();
+            issue(k + 5);
+        }
+        if (use_tma && NS == 6 && more) issued = k + 5;
+        if (ND == 3) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) tv.so[q] = ((k + q) % NS) * 9 * PP;
+        } else {
+            tv.so[2] = 0;
+        }
+        const long long cl = ((long long)z * nY + y) * nX + x;
+        stencil_cell<T, ND, MODE>(I, ii, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, clk, t_flux,
+                                  vmax, esum, zsum);
+        if (ND == 3 && more) {
+            if (use_tma) {
+                if (NS == 5) {
+                    __syncthreads();
+                    if (tid == 0) {
+                        fence_proxy_async();
+                        issue(k + 5);
+                    }
+                    issued = k + 5;
+                }
+                arrive(k + 5);
+            } else {
+                __syncthreads();
+                load_box(k % NS, wrapz(z + 3), true);
+            }
+            __syncthreads();
+        }
+    }
+    if (!ok) {
+        // a copy did not land in time: let every copy this block issued finish (bounded), then leave
+        for (int pr = max(0, issued - NS + 1); pr <= issued; ++pr)
+            mbar_wait(&bars[pr % NS], (uint32_t)((pr / NS) & 1));
+        return;
+    }
+    if (MODE == M_STAGE1) {
+        double m = block_reduce_max(vmax, red);
+        double es = block_reduce_sum(esum, red);
+        double zs = block_reduce_sum(zsum, red);
+        if (tid == 0) {
+            bmax[blockIdx.x] = m;
+            bsum[2 * blockIdx.x] = es;
+            bsum[2 * blockIdx.x + 1] = zs;
+        }
+    }
+}
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(ST_THREADS)
+__global__ void __launch_bounds__(ST_THREADS, (sizeof(T) == 4) ? 3 : 2)
 k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre,
           const T* __restrict__ bs, const T* bn, T* out, const T* __restrict__ sig,
           T* __restrict__ speed_out, const InstClock* __restrict__ clk, double t_flux,
-          double* __restrict__ bmax, double* __restrict__ bsum) {
+          double* __restrict__ bmax, double* __restrict__ bsum, int* __restrict__ status,
+          const __grid_constant__ StencilMapSet maps) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
     __shared__ double red[ST_THREADS / 32];
+    __shared__ __align__(8) uint64_t bars[6];
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
-    const long long cell = (long long)(blockIdx.x - pre[ii]) * ST_THREADS + threadIdx.x;
+    const int lb = blockIdx.x - pre[ii];
     if (I.nd == 3)
-        stencil_body<T, 3, MODE>(I, ii, cell, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum, red);
+        march<T, 3, MODE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+                          status);
     else
-        stencil_body<T, 2, MODE>(I, ii, cell, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum, red);
+        march<T, 2, MODE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+                          status);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -450,9 +662,11 @@ __global__ void __launch_bounds__(256) k_dt(const InstDev* __restrict__ insts,
         m = fmax(m, bmax[b]);
     }
     m = block_reduce_max(m, red);
-    // observable sums in a fixed order (thread 0 walks the partials)
+    // observable sums: fixed-order strided partial sums, then a fixed tree (deterministic)
+    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) { es += bsum[2 * b]; zs += bsum[2 * b + 1]; }
+    es = block_reduce_sum(es, red);
+    zs = block_reduce_sum(zs, red);
     if (threadIdx.x == 0) {
-        for (int b = b0; b < b1; ++b) { es += bsum[2 * b]; zs += bsum[2 * b + 1]; }
         obs[2 * ii] = es;
         obs[2 * ii + 1] = zs * I.inv_cells;
         InstClock c = clk[ii];
@@ -493,15 +707,15 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
 
 // Energy and mean b_zz partials of a state whose internal stress is in sig (observables).
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS) k_observe(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(256) k_observe(const InstDev* __restrict__ insts, int n_inst,
                                                         const int* __restrict__ pre,
                                                         const T* __restrict__ beta,
                                                         const T* __restrict__ sig,
                                                         double* __restrict__ bsum) {
-    __shared__ double red[ST_THREADS / 32];
+    __shared__ double red[8];
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
-    const long long cell = (long long)(blockIdx.x - pre[ii]) * ST_THREADS + threadIdx.x;
+    const long long cell = (long long)(blockIdx.x - pre[ii]) * blockDim.x + threadIdx.x;
     double e = 0.0, z = 0.0;
     if (cell < I.cells) {
         const T* sp = sig + I.soff + cell;
@@ -518,28 +732,37 @@ __global__ void __launch_bounds__(ST_THREADS) k_observe(const InstDev* __restric
     if (threadIdx.x == 0) { bsum[2 * blockIdx.x] = es; bsum[2 * blockIdx.x + 1] = zs; }
 }
 
-__global__ void k_obs_reduce(const InstDev* __restrict__ insts, const int* __restrict__ pre,
-                             const double* __restrict__ bsum, double* __restrict__ obs) {
+__global__ void __launch_bounds__(256) k_obs_reduce(const InstDev* __restrict__ insts,
+                                                    const int* __restrict__ pre,
+                                                    const double* __restrict__ bsum,
+                                                    double* __restrict__ obs) {
+    __shared__ double red[8];
     const int ii = blockIdx.x;
-    if (threadIdx.x != 0) return;
     double es = 0.0, zs = 0.0;
-    for (int b = pre[ii]; b < pre[ii + 1]; ++b) { es += bsum[2 * b]; zs += bsum[2 * b + 1]; }
-    obs[2 * ii] = es;
-    obs[2 * ii + 1] = zs * insts[ii].inv_cells;
+    for (int b = pre[ii] + threadIdx.x; b < pre[ii + 1]; b += blockDim.x) {
+        es += bsum[2 * b];
+        zs += bsum[2 * b + 1];
+    }
+    es = block_reduce_sum(es, red);
+    zs = block_reduce_sum(zs, red);
+    if (threadIdx.x == 0) {
+        obs[2 * ii] = es;
+        obs[2 * ii + 1] = zs * insts[ii].inv_cells;
+    }
 }
 
 // ------------------------------------------------------------------------------------------
 template <typename T>
 static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,
-                             void* speed, double t, cudaStream_t st) {
+                             void* speed, double t, const StencilMapSet& maps, cudaStream_t st) {
     const LaunchShape& L = P.stencil;
     const T* b = (const T*)bs;
     const T* n = (const T*)bn;
     T* o = (T*)out;
     const T* s = (const T*)P.d_sigma;
-#define CDD_LAUNCH_ST(M, SP)                                                                   \
-    k_stencil<T, M><<<L.blocks, ST_THREADS, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                     P.d_clock, t, P.d_bmax, P.d_bsum)
+#define CDD_LAUNCH_ST(M, SP)                                                                       \
+    k_stencil<T, M><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
+                                                         P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps)
     switch (mode) {
         case M_FLUX: CDD_LAUNCH_ST(M_FLUX, (T*)speed); break;
         case M_STAGE1: CDD_LAUNCH_ST(M_STAGE1, nullptr); break;
@@ -550,10 +773,63 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
 }
 
 cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,
-                           void* speed, double t_flux, cudaStream_t st) {
-    if (P.precision == CDD_F32) stencil_dispatch<float>(P, mode, bs, bn, out, speed, t_flux, st);
-    else stencil_dispatch<double>(P, mode, bs, bn, out, speed, t_flux, st);
+                           void* speed, double t_flux, const StencilMapSet& maps, cudaStream_t st) {
+    if (P.precision == CDD_F32) stencil_dispatch<float>(P, mode, bs, bn, out, speed, t_flux, maps, st);
+    else stencil_dispatch<double>(P, mode, bs, bn, out, speed, t_flux, maps, st);
     return cudaGetLastError();
+}
+
+bool stencil_tma_eligible(const InstDev& I, int precision) {
+    if (I.nd != 3) return false;
+    const int RX = precision == CDD_F32 ? TileGeom<float>::RX : TileGeom<double>::RX;
+    if (I.n2 < RX || I.n1 < RY) return false;
+    if (precision == CDD_F32 && I.n2 % 4) return false;
+    return true;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 4-D map per instance: (x = last axis, y, z = axis 0, component); box = one staged plane of all
+// 9 components, RX x RY cells; out-of-grid coordinates read zeros (patched by the kernel).
+bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* base, StencilMapSet& maps) {
+    maps.enabled = 0;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || !base) return false;
+    const bool f32 = (P.precision == CDD_F32);
+    const size_t elt = f32 ? sizeof(float) : sizeof(double);
+    const cuuint32_t RX = f32 ? TileGeom<float>::RX : TileGeom<double>::RX;
+    bool any = false;
+    for (int i = 0; i < P.n_inst; ++i) {
+        const InstDev& I = insts[i];
+        if (I.tma_slot < 0) continue;
+        const char* addr = (const char*)base + (size_t)I.foff * elt;
+        if (((uintptr_t)addr) % 16) return false;
+        cuuint64_t dims[4] = {(cuuint64_t)I.n2, (cuuint64_t)I.n1, (cuuint64_t)I.n0, 9};
+        cuuint64_t strides[3] = {(cuuint64_t)I.n2 * elt, (cuuint64_t)I.n2 * I.n1 * elt,
+                                 (cuuint64_t)I.cells * elt};
+        cuuint32_t box[4] = {RX, (cuuint32_t)RY, 1, 9};
+        cuuint32_t estr[4] = {1, 1, 1, 1};
+        CUresult r = enc(&maps.m[I.tma_slot], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         4, (void*)addr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+        any = true;
+    }
+    maps.enabled = any ? 1 : 0;
+    return any;
 }
 
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st) {
@@ -574,17 +850,51 @@ cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaS
 }
 
 cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st) {
-    const LaunchShape& L = P.stencil;
+    const LaunchShape& L = P.obs;
     if (P.precision == CDD_F32)
-        k_observe<float><<<L.blocks, ST_THREADS, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const float*)beta,
+        k_observe<float><<<L.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const float*)beta,
                                                          (const float*)P.d_sigma, P.d_bsum);
     else
-        k_observe<double><<<L.blocks, ST_THREADS, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const double*)beta,
+        k_observe<double><<<L.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const double*)beta,
                                                           (const double*)P.d_sigma, P.d_bsum);
-    k_obs_reduce<<<P.n_inst, 32, 0, st>>>(P.d_inst, L.d_pre, P.d_bsum, P.d_obs);
+    k_obs_reduce<<<P.n_inst, 256, 0, st>>>(P.d_inst, P.obs.d_pre, P.d_bsum, P.d_obs);
     return cudaGetLastError();
 }
 
-cudaError_t stencil_set_attributes(int) { return cudaSuccess; }
+template <typename T>
+static cudaError_t st_attr(size_t smem) {
+    cudaError_t e;
+    int v = (int)smem;
+    if ((e = cudaFuncSetAttribute(k_stencil<T, M_FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_stencil<T, M_STAGE1>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_stencil<T, M_STAGE2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    return cudaFuncSetAttribute(k_stencil<T, M_STAGE3>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+}
+
+cudaError_t stencil_set_attributes(int precision, size_t smem) {
+    return precision == CDD_F32 ? st_attr<float>(smem) : st_attr<double>(smem);
+}
+
+size_t stencil_smem_bytes(int precision, bool any3d) {
+    if (precision == CDD_F32)
+        return (size_t)(any3d ? TileGeom<float>::NS : 1) * 9 * tile_pp<float>() * sizeof(float);
+    return (size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() * sizeof(double);
+}
+
+void stencil_geometry(InstDev& I) {
+    const int nZ = (I.nd == 3) ? I.n0 : 1;
+    const int nY = (I.nd == 3) ? I.n1 : I.n0;
+    const int nX = (I.nd == 3) ? I.n2 : I.n1;
+    const int tiles = ((nX + TXS - 1) / TXS) * ((nY + TYS - 1) / TYS);
+    int chunks = 1;
+    if (I.nd == 3) {
+        chunks = (1776 + tiles - 1) / tiles;
+        if (chunks > nZ) chunks = nZ;
+        if (chunks < 1) chunks = 1;
+    }
+    I.st_zc = (nZ + chunks - 1) / chunks;
+    chunks = (nZ + I.st_zc - 1) / I.st_zc;
+    I.stencil_blocks = tiles * chunks;
+}
 
 }  // namespace cdd

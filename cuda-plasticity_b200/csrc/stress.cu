@@ -31,6 +31,16 @@ constexpr int GREEN_THREADS = 512;
 
 __host__ __device__ inline int rows_ld(int n) { return n + (n >> 4) + 1; }
 
+// Mean stress -lam tr<b> d_ij - mu (<b>_ij + <b>_ji) of symmetric component o (xx xy xz yy yz zz).
+__device__ __forceinline__ double mean_stress(const InstDev& I, const double* m, int o) {
+    const int ia[6] = {0, 0, 0, 1, 1, 2};
+    const int ja[6] = {0, 1, 2, 1, 2, 2};
+    const int i = ia[o], j = ja[o];
+    double v = -I.mu * (m[3 * i + j] + m[3 * j + i]);
+    if (i == j) v -= I.lamb * (m[0] + m[4] + m[8]);
+    return v;
+}
+
 // ------------------------------------------------------------------------------------------
 // R2C along the contiguous axis: pairs of real rows (a + i b) per complex FFT.
 // ------------------------------------------------------------------------------------------
@@ -158,8 +168,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
         long long ra = 2 * p;
         T va = z.x, vb = z.y;
         if (MEAN64) {
-            va += (T)sbar[6 * ii + (int)(ra / I.rows)];
-            if (ra + 1 < nrows) vb += (T)sbar[6 * ii + (int)((ra + 1) / I.rows)];
+            va += (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
+            if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows));
         }
         dst[ra * N + idx] = va;
         if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
@@ -342,40 +352,30 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
 }
 
 // ------------------------------------------------------------------------------------------
-// FP32 plans: FP64 mean of each beta component from the row sums, and the mean stress
-// sigma_bar = -lam tr<b> d - mu (<b> + <b>^T), one block per instance (fixed summation order).
+// FP32 plans: FP64 mean of each beta component from the row sums; block (instance, component),
+// fixed-order strided sums and a fixed tree, so the result is deterministic.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_mean_stress(const InstDev* __restrict__ insts,
-                                                     const double* __restrict__ rowsum,
-                                                     double* __restrict__ sbar) {
+__global__ void __launch_bounds__(256) k_mean_beta(const InstDev* __restrict__ insts,
+                                                   const double* __restrict__ rowsum,
+                                                   double* __restrict__ mean9) {
     const InstDev& I = insts[blockIdx.x];
-    __shared__ double red[9][8];
-    __shared__ double mean[9];
+    const int c = blockIdx.y;
+    __shared__ double red[8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int c = 0; c < 9; ++c) {
-        double acc = 0.0;
-        for (long long r = tid; r < I.rows; r += blockDim.x) acc += rowsum[I.rsoff + c * (long long)I.rows + r];
+    const double* rs = rowsum + I.rsoff + (long long)c * I.rows;
+    double acc = 0.0;
+    for (int r = tid; r < I.rows; r += blockDim.x) acc += rs[r];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) red[c][warp] = acc;
-    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[warp] = acc;
     __syncthreads();
-    if (tid < 9) {
-        double acc = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += red[tid][w];
-        mean[tid] = acc * I.inv_cells;
-    }
-    __syncthreads();
-    if (tid < 6) {
-        const int ia[6] = {0, 0, 0, 1, 1, 2};
-        const int ja[6] = {0, 1, 2, 1, 2, 2};
-        int i = ia[tid], j = ja[tid];
-        double tr = mean[0] + mean[4] + mean[8];
-        double v = -I.mu * (mean[3 * i + j] + mean[3 * j + i]);
-        if (i == j) v -= I.lamb * tr;
-        sbar[6 * blockIdx.x + tid] = v;
+    if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        mean9[9 * blockIdx.x + c] = s * I.inv_cells;
     }
 }
+
 
 // ------------------------------------------------------------------------------------------
 // Host launch sequence
@@ -390,7 +390,7 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     if (f32) {
         k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum);
-        k_mean_stress<<<P.n_inst, 256, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
+        k_mean_beta<<<dim3(P.n_inst, 9), 256, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr);

@@ -235,3 +235,50 @@ def test_fp32_form_error_against_fp64():
     e32, m32 = p32.observables(b32)
     assert abs(e32[0] - e64[0]) <= 1e-5 * abs(e64[0])
     assert abs(m32[0] - m64[0]) <= 1e-6 * max(abs(m64[0]), 1e-3)
+
+
+@pytest.mark.parametrize("shape,load", [((12, 40, 72), None), ((10, 24, 64), (-0.025, -0.025, 0.05))])
+def test_tma_staged_planes_against_oracle(shape, load):
+    """3-D grids wide enough for the TMA plane path (x >= 40): edge tiles in x and y, FP64."""
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 31)
+    p = O.Params(mu=1.0, nu=0.3, load_rate=load)
+    plan = cdd.Plan([cdd.Instance(shape, load_rate=load)], "f64")
+    beta = plan.pack([b0])
+    rhs, speed = plan.flux(beta, 0.0)
+    ref_rhs, ref_speed = O.full_flux(b0, 0.0, p)
+    torch.cuda.synchronize()
+    assert rel(plan.field_view(rhs, 0).cpu().numpy(), ref_rhs) < 1e-12
+    assert rel(speed.cpu().numpy().reshape(shape), ref_speed) < 1e-12
+    plan.set_time(0.0, 1e30)
+    plan.step(beta)
+    ref, _ = O.rk3_step(b0, 0.0, 1e30, p)
+    assert rel(plan.field_view(beta, 0).cpu().numpy(), ref) < 1e-11
+    plan.check_status()
+
+
+def test_tma_fp32_matches_fp64_and_batch_mixes_paths():
+    """FP32 TMA path against FP64, and a batch mixing TMA-staged and thread-staged instances."""
+    shapes = [(16, 24, 80), (12, 12, 12), (32, 32)]
+    fields = [cdd.gaussian_random_field(s, 0.06, 0.05, 40 + i) for i, s in enumerate(shapes)]
+    insts = [cdd.Instance(s) for s in shapes]
+    p64 = cdd.Plan(insts, "f64")
+    p32 = cdd.Plan(insts, "f32")
+    b64 = p64.pack(fields)
+    b32 = p32.pack(fields)
+    for p in (p64, p32):
+        p.set_time(0.0, 1e30)
+    for _ in range(3):
+        p64.step(b64)
+        p32.step(b32)
+    for i in range(len(shapes)):
+        x64 = p64.field_view(b64, i).cpu().numpy()
+        x32 = p32.field_view(b32, i).cpu().numpy().astype(np.float64)
+        assert rel(x32, x64) < 2e-6, i
+        single = cdd.Plan([insts[i]], "f64")
+        bs = single.pack([fields[i]])
+        single.set_time(0.0, 1e30)
+        for _ in range(3):
+            single.step(bs)
+        assert torch.equal(single.field_view(bs, 0), p64.field_view(b64, i))
+    p64.check_status()
+    p32.check_status()
