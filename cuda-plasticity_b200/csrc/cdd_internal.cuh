@@ -269,7 +269,7 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
 // Run all stages of `lp` on the lines of `lay`, starting in buffer a (b is scratch of the same
 // layout). Returns the buffer that holds the result. Every thread of the block must call this.
 template <typename V, bool INV, typename Lay>
-__device__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
+__device__ __forceinline__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
                         int tid, int nt) {
     const int n = lp.n;
     const V* tw = twbase + lp.tw;

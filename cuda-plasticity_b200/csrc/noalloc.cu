@@ -183,15 +183,15 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         const int comps = (k == PASS_R2C) ? 9 : 6;
         long long npairs = ((long long)comps * I.rows + 1) / 2;
         const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
-        int Pl = (int)((40 * 1024) / line_bytes);
+        int Pl = (velt == 8 ? 4096 : 2048) / I.nl;
         if (Pl < 1) Pl = 1;
         if (Pl > npairs) Pl = (int)npairs;
         PassTile& t = I.tile[k];
         t.lines = Pl;
-        t.threads = 256;
+        t.threads = (velt == 8) ? 256 : 128;
         t.blocks = (int)((npairs + Pl - 1) / Pl);
         t.tiles_a = 1;
-        P.pass[k].threads = 256;
+        P.pass[k].threads = t.threads;
         P.pass[k].smem = 2 * (size_t)Pl * line_bytes;
     }
     for (int k : {PASS_MID_F, PASS_MID_I}) {
@@ -209,16 +209,16 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     }
     {
         PassTile& t = I.tile[PASS_GREEN];
-        int W = 16;
-        while (W > 1 && 2 * (size_t)9 * (I.n0 * W + W) * velt > 200 * 1024) W >>= 1;
-        if (2 * (size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
+        int W = (int)(32 / velt);
+        while (W > 1 && (size_t)12 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
+        if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
             return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: axis-0 length too large for the k-space pass");
         t.lines = W;
-        t.threads = 512;
+        t.threads = 256;
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
-        P.pass[PASS_GREEN].threads = 512;
-        P.pass[PASS_GREEN].smem = 2 * (size_t)9 * (I.n0 * W + W) * velt;
+        P.pass[PASS_GREEN].threads = 256;
+        P.pass[PASS_GREEN].smem = (size_t)12 * (I.n0 * W + W) * velt;
     }
     for (int k = 0; k < NUM_PASSES; ++k) {
         blocks[k] = I.tile[k].blocks;

@@ -163,12 +163,12 @@ int build_shapes(cdd_plan* p, size_t elt) {
             const int comps = (k == PASS_R2C) ? 9 : 6;
             long long npairs = ((long long)comps * I.rows + 1) / 2;
             const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
-            int P = (int)((40 * 1024) / line_bytes);
+            int P = (velt == 8 ? 4096 : 2048) / I.nl;   // radix-16 stages: one butterfly per thread
             if (P < 1) P = 1;
             if (P > npairs) P = (int)npairs;
             PassTile& t = I.tile[k];
             t.lines = P;
-            t.threads = 256;
+            t.threads = (velt == 8) ? 256 : 128;
             t.blocks = (int)((npairs + P - 1) / P);
             t.tiles_a = 1;
             size_t sm = 2 * (size_t)P * line_bytes;
@@ -193,15 +193,15 @@ int build_shapes(cdd_plan* p, size_t elt) {
         // fused Green pass along axis 0: 9 components x W columns, ping-pong
         {
             PassTile& t = I.tile[PASS_GREEN];
-            int W = 16;
-            while (W > 1 && 2 * (size_t)9 * (I.n0 * W + W) * velt > 200 * 1024) W >>= 1;
-            if (2 * (size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
+            int W = (int)(32 / velt);   // 32-byte row segments
+            while (W > 1 && (size_t)12 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
+            if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
                 return fail(CDD_ERR_SHAPE, "axis-0 length %d too large for the fused k-space pass", I.n0);
             t.lines = W;
-            t.threads = 512;
+            t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
-            size_t sm = 2 * (size_t)9 * (I.n0 * W + W) * velt;
+            size_t sm = (size_t)12 * (I.n0 * W + W) * velt;
             if (sm > smem_max[PASS_GREEN]) smem_max[PASS_GREEN] = sm;
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }
@@ -217,7 +217,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
     for (int k = 0; k < NUM_PASSES; ++k) {
         LaunchShape& L = C.pass[k];
         L.blocks = pre[k].back();
-        L.threads = (k == PASS_GREEN) ? 512 : 256;
+        L.threads = (k == PASS_R2C || k == PASS_C2R) ? (velt == 8 ? 256 : 128) : 256;
         L.smem = smem_max[k];
         if (L.smem > smem_all) smem_all = L.smem;
         CDD_CUDA(dalloc(p, (void**)&L.d_pre, sizeof(int) * (n + 1)));
@@ -286,7 +286,6 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
     if (precision != CDD_F64 && precision != CDD_F32) return fail(CDD_ERR_ARG, "bad precision %d", precision);
     *out = nullptr;
     cdd_plan* p = new cdd_plan();
-    cudaGetDevice(&p->device);
     PlanCore& C = p->core;
     C.n_inst = n_inst;
     C.precision = precision;
@@ -383,6 +382,7 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
         I.load_mu = d.load_mu;
         I.load_lamb = 2. * d.load_mu * d.load_nu / (1. - 2. * d.load_nu);
     }
+    cudaGetDevice(&p->device);
     C.field_elems = foff;
     C.stress_elems = soff;
     C.cells = coff;

@@ -27,9 +27,26 @@
 namespace cdd {
 
 constexpr int ROW_THREADS = 256;
-constexpr int GREEN_THREADS = 512;
+constexpr int GREEN_THREADS = 256;
 
 __host__ __device__ inline int rows_ld(int n) { return n + (n >> 4) + 1; }
+
+// Four consecutive reals: one 16-byte access for float, two for double (16-byte aligned).
+__device__ __forceinline__ void load4(const float* p, float* v) {
+    float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void load4(const double* p, double* v) {
+    double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void store4(float* p, const float* v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double* v) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
 
 // Mean stress -lam tr<b> d_ij - mu (<b>_ij + <b>_ji) of symmetric component o (xx xy xz yy yz zz).
 __device__ __forceinline__ double mean_stress(const InstDev& I, const double* m, int o) {
@@ -63,16 +80,36 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const int tid = threadIdx.x, nt = blockDim.x;
     const T* src = beta + I.foff;
 
-    for (int i = tid; i < P * N; i += nt) {
-        int pl = i / N, idx = i - pl * N;
-        long long p = (long long)lb * P + pl;
-        V z; z.x = 0; z.y = 0;
-        if (p < npairs) {
-            long long ra = 2 * p;
-            z.x = src[ra * N + idx];
-            if (ra + 1 < nrows) z.y = src[(ra + 1) * N + idx];
+    const bool vec = ((N & 3) == 0) && ((((uintptr_t)src) & 15) == 0);
+    if (vec) {
+#pragma unroll 4
+        for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
+            const int i = i4 << 2;
+            const int pl = i / N, idx = i - pl * N;
+            const long long p = (long long)lb * P + pl;
+            T a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
+            if (p < npairs) {
+                const long long ra = 2 * p;
+                load4(src + ra * N + idx, a);
+                if (ra + 1 < nrows) load4(src + (ra + 1) * N + idx, b);
+            }
+            V* d = s + pl * ld + row_pad(idx);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { V z; z.x = a[q]; z.y = b[q]; d[q] = z; }
         }
-        s[pl * ld + row_pad(idx)] = z;
+    } else {
+#pragma unroll 4
+        for (int i = tid; i < P * N; i += nt) {
+            int pl = i / N, idx = i - pl * N;
+            long long p = (long long)lb * P + pl;
+            V z; z.x = 0; z.y = 0;
+            if (p < npairs) {
+                long long ra = 2 * p;
+                z.x = src[ra * N + idx];
+                if (ra + 1 < nrows) z.y = src[(ra + 1) * N + idx];
+            }
+            s[pl * ld + row_pad(idx)] = z;
+        }
     }
     __syncthreads();
     if (MEAN64) {
@@ -135,6 +172,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
 
+#pragma unroll 4
     for (int i = tid; i < P * nh; i += nt) {
         int pl = i / nh, k = i - pl * nh;
         long long p = (long long)lb * P + pl;
@@ -160,19 +198,43 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     RowLayout lay{P, ld};
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
     T* dst = sigma + I.soff;
-    for (int i = tid; i < P * N; i += nt) {
-        int pl = i / N, idx = i - pl * N;
-        long long p = (long long)lb * P + pl;
-        if (p >= npairs) continue;
-        V z = s[pl * ld + row_pad(idx)];
-        long long ra = 2 * p;
-        T va = z.x, vb = z.y;
-        if (MEAN64) {
-            va += (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
-            if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows));
+    const bool vec = ((N & 3) == 0) && ((((uintptr_t)dst) & 15) == 0);
+    if (vec) {
+#pragma unroll 2
+        for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
+            const int i = i4 << 2;
+            const int pl = i / N, idx = i - pl * N;
+            const long long p = (long long)lb * P + pl;
+            if (p >= npairs) continue;
+            const long long ra = 2 * p;
+            T va[4], vb[4];
+            const V* sr = s + pl * ld + row_pad(idx);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { V z = sr[q]; va[q] = z.x; vb[q] = z.y; }
+            if (MEAN64) {
+                const T ma = (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
+                const T mb = (ra + 1 < nrows) ? (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows)) : (T)0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) { va[q] += ma; vb[q] += mb; }
+            }
+            store4(dst + ra * N + idx, va);
+            if (ra + 1 < nrows) store4(dst + (ra + 1) * N + idx, vb);
         }
-        dst[ra * N + idx] = va;
-        if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
+    } else {
+        for (int i = tid; i < P * N; i += nt) {
+            int pl = i / N, idx = i - pl * N;
+            long long p = (long long)lb * P + pl;
+            if (p >= npairs) continue;
+            V z = s[pl * ld + row_pad(idx)];
+            long long ra = 2 * p;
+            T va = z.x, vb = z.y;
+            if (MEAN64) {
+                va += (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
+                if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows));
+            }
+            dst[ra * N + idx] = va;
+            if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
+        }
     }
 }
 
@@ -202,6 +264,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int wv = min(W, nh - col0);
     const int tid = threadIdx.x, nt = blockDim.x;
     V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+#pragma unroll 4
     for (int i = tid; i < N * W; i += nt) {
         int e = i / W, w = i - e * W;
         V z; z.x = 0; z.y = 0;
@@ -269,12 +332,28 @@ __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz
     }
 }
 
+// Shared memory: 12 component slots of N x W (+W pad): slots 0..8 hold the 9 components, 9..11
+// are the ping-pong scratch. The transforms run three components at a time against the scratch;
+// when the stage count is odd the result is copied back to the component slots.
+template <typename V, bool INV>
+__device__ __forceinline__ void fft_group3(V* s, int g, int N, int W, int cs, const LinePlan& lp,
+                                           const V* __restrict__ tw, int tid, int nt) {
+    V* a = s + 3 * g * cs;
+    V* b = s + 9 * cs;
+    ColLayout lay{3 * W, W, cs};
+    V* r = fft_lines<V, INV>(a, b, lay, lp, tw, tid, nt);
+    if (r != a) {
+        for (int i = tid; i < 3 * cs; i += nt) a[i] = b[i];
+        __syncthreads();
+    }
+}
+
 template <typename T, bool MEAN64>
 __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restrict__ insts, int n_inst,
-                                                const int* __restrict__ pre,
-                                                typename VecOf<T>::type* __restrict__ spec,
-                                                const typename VecOf<T>::type* __restrict__ tw,
-                                                const T* __restrict__ ktab) {
+                                                         const int* __restrict__ pre,
+                                                         typename VecOf<T>::type* __restrict__ spec,
+                                                         const typename VecOf<T>::type* __restrict__ tw,
+                                                         const T* __restrict__ ktab) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -289,11 +368,12 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
     const int col0 = ta * W;
     const int wv = min(W, nh - col0);
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int cs = N * W + W;          // padded component stride in shared memory
+    const int cs = N * W + W;          // padded component slot in shared memory
     const long long estride = (I.nd == 3) ? (long long)I.n1 * nhp : (long long)nhp;
     const long long cstride = (long long)N * estride;
     V* base = spec + I.spoff + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0;
 
+#pragma unroll 4
     for (int i = tid; i < 9 * N * W; i += nt) {
         int c = i / (N * W);
         int rem = i - c * N * W;
@@ -303,12 +383,7 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
         s[c * cs + rem] = z;
     }
     __syncthreads();
-    V* s2 = s + 9 * cs;
-    {
-        ColLayout lay{9 * W, W, cs};
-        V* r = fft_lines<V, false>(s, s2, lay, I.lp_first, tw, tid, nt);
-        if (r != s) { V* t = s; s = s2; s2 = t; }
-    }
+    for (int g = 0; g < 3; ++g) fft_group3<V, false>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -339,10 +414,8 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
         for (int c = 0; c < 6; ++c) s[c * cs + i] = o[c];
     }
     __syncthreads();
-    {
-        ColLayout lay{6 * W, W, cs};
-        s = fft_lines<V, true>(s, s2, lay, I.lp_first, tw, tid, nt);
-    }
+    for (int g = 0; g < 2; ++g) fft_group3<V, true>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
+#pragma unroll 4
     for (int i = tid; i < 6 * N * W; i += nt) {
         int c = i / (N * W);
         int rem = i - c * N * W;
