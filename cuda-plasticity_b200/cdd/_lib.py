@@ -74,6 +74,12 @@ _PROTOS = {
     "cdd_observables": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "cdd_check_status": (ctypes.c_int, [ctypes.c_void_p]),
+    "cdd_flux_vjp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_flux_branches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    "cdd_stress_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_last_error": (ctypes.c_char_p, []),

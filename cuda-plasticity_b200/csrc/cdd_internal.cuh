@@ -333,9 +333,15 @@ struct PlanCore {
     double* d_obs = nullptr;         // per-instance energy, mean zz (2 per instance)
     int* d_status = nullptr;
     LaunchShape pass[NUM_PASSES];
+    LaunchShape adj[NUM_PASSES];     // adjoint stress pipeline: 6 components in, 9 out
     LaunchShape stencil;
     LaunchShape cellwise;            // elementwise kernels over cells
     LaunchShape obs;                 // observables: one thread per cell
+    LaunchShape vjp;                 // flux VJP: 128 cells per block
+    void* d_ubar = nullptr;          // adjoint scratch (allocated on first use): 54 derivative cotangents per cell
+    uint32_t* d_flags = nullptr;     // limiter selections, 4 words per cell
+    double* d_bload = nullptr;       // per-block load-cotangent partials (3 per block)
+    void* d_adj9 = nullptr;          // beta cotangent from the adjoint stress solve
 };
 
 // Tensor maps of one stage-input buffer for the TMA-staged instances (see stencil.cu).
@@ -346,6 +352,12 @@ struct StencilMapSet {
 
 // stress.cu
 cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st);
+cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st);
+cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st);
+// adjoint.cu
+cudaError_t launch_flux_branches(const PlanCore& P, const void* beta, double t, uint32_t* flags, cudaStream_t st);
+cudaError_t launch_flux_vjp(const PlanCore& P, const void* beta, double t, const void* gbar, void* sigbar,
+                            void* betabar, double* load_bar, cudaStream_t st);
 // stencil.cu
 enum StencilMode { M_FLUX = 0, M_STAGE1 = 1, M_STAGE2 = 2, M_STAGE3 = 3 };
 cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,

@@ -213,7 +213,28 @@ int build_shapes(cdd_plan* p, size_t elt) {
         pre_ob.push_back(pre_ob.back() + (int)((I.cells + 255) / 256));
         pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));
     }
+    // adjoint stress pipeline: 6 components through R2C and the forward axis-1 pass, 9 after
+    std::vector<int> apre[NUM_PASSES];
+    for (int k = 0; k < NUM_PASSES; ++k) apre[k].push_back(0);
+    for (int i = 0; i < n; ++i) {
+        const InstDev& I = p->inst[i];
+        int b[NUM_PASSES];
+        b[PASS_R2C] = (int)((((long long)6 * I.rows + 1) / 2 + I.tile[PASS_R2C].lines - 1) / I.tile[PASS_R2C].lines);
+        b[PASS_C2R] = (int)((((long long)9 * I.rows + 1) / 2 + I.tile[PASS_C2R].lines - 1) / I.tile[PASS_C2R].lines);
+        b[PASS_MID_F] = (I.nd == 3) ? 6 * I.n0 * I.tile[PASS_MID_F].tiles_a : 0;
+        b[PASS_MID_I] = (I.nd == 3) ? 9 * I.n0 * I.tile[PASS_MID_I].tiles_a : 0;
+        b[PASS_GREEN] = I.tile[PASS_GREEN].blocks;
+        for (int k = 0; k < NUM_PASSES; ++k) apre[k].push_back(apre[k].back() + b[k]);
+    }
     size_t smem_all = 0;
+    for (int k = 0; k < NUM_PASSES; ++k) {
+        LaunchShape& A = C.adj[k];
+        A.blocks = apre[k].back();
+        A.threads = (k == PASS_R2C || k == PASS_C2R) ? (velt == 8 ? 256 : 128) : 256;
+        A.smem = smem_max[k];
+        CDD_CUDA(dalloc(p, (void**)&A.d_pre, sizeof(int) * (n + 1)));
+        CDD_CUDA(cudaMemcpy(A.d_pre, apre[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
     for (int k = 0; k < NUM_PASSES; ++k) {
         LaunchShape& L = C.pass[k];
         L.blocks = pre[k].back();
@@ -227,6 +248,14 @@ int build_shapes(cdd_plan* p, size_t elt) {
     C.stencil.threads = 256;
     C.stencil.smem = stencil_smem_bytes(C.precision, C.any3d);
     CDD_CUDA(stencil_set_attributes(C.precision, C.stencil.smem < 48 * 1024 ? 48 * 1024 : C.stencil.smem));
+    {
+        std::vector<int> pre_v(1, 0);
+        for (int i = 0; i < n; ++i) pre_v.push_back(pre_v.back() + (int)((p->inst[i].cells + 127) / 128));
+        C.vjp.blocks = pre_v.back();
+        C.vjp.threads = 128;
+        CDD_CUDA(dalloc(p, (void**)&C.vjp.d_pre, sizeof(int) * (n + 1)));
+        CDD_CUDA(cudaMemcpy(C.vjp.d_pre, pre_v.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
     C.obs.blocks = pre_ob.back();
     C.obs.threads = 256;
     CDD_CUDA(dalloc(p, (void**)&C.obs.d_pre, sizeof(int) * (n + 1)));
@@ -576,6 +605,52 @@ int cdd_observables(cdd_plan* p, const void* beta, double* energy, double* mean_
         if (energy) energy[i] = obs[2 * i];
         if (mean_zz) mean_zz[i] = obs[2 * i + 1];
     }
+    return CDD_OK;
+}
+
+namespace {
+int ensure_adjoint_scratch(cdd_plan* p) {
+    PlanCore& C = p->core;
+    if (C.d_ubar) return CDD_OK;
+    const size_t elt = C.precision == CDD_F64 ? sizeof(double) : sizeof(float);
+    cudaError_t e;
+    if ((e = dalloc(p, &C.d_ubar, elt * 54 * (size_t)C.cells)) ||
+        (e = dalloc(p, (void**)&C.d_flags, sizeof(uint32_t) * 4 * (size_t)C.cells)) ||
+        (e = dalloc(p, (void**)&C.d_bload, sizeof(double) * 3 * (size_t)C.vjp.blocks)) ||
+        (e = dalloc(p, &C.d_adj9, elt * (size_t)C.field_elems)))
+        return fail(CDD_ERR_ALLOC, "adjoint scratch: %s", cudaGetErrorString(e));
+    return CDD_OK;
+}
+}  // namespace
+
+int cdd_flux_vjp(cdd_plan* p, const void* beta, double t, const void* gbar, void* betabar, void* sigbar6,
+                 double* load_bar, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !gbar || !betabar || !sigbar6) return fail(CDD_ERR_ARG, "null buffer");
+    if (int rc = ensure_adjoint_scratch(p)) return rc;
+    CDD_CUDA(launch_flux_vjp(p->core, beta, t, gbar, sigbar6, betabar, load_bar, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_flux_branches(cdd_plan* p, const void* beta, double t, uint32_t* flags, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !flags) return fail(CDD_ERR_ARG, "null buffer");
+    if (int rc = ensure_adjoint_scratch(p)) return rc;
+    CDD_CUDA(launch_flux_branches(p->core, beta, t, flags, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_stress_adjoint(cdd_plan* p, const void* sigbar6, void* betabar9, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!sigbar6 || !betabar9) return fail(CDD_ERR_ARG, "null buffer");
+    CDD_CUDA(launch_stress_adjoint(p->core, sigbar6, betabar9, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_stress_dnu(cdd_plan* p, const void* beta, void* out6, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !out6) return fail(CDD_ERR_ARG, "null buffer");
+    CDD_CUDA(launch_stress_dnu(p->core, beta, out6, (cudaStream_t)stream));
     return CDD_OK;
 }
 

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
                                                   const T* __restrict__ beta,
                                                   typename VecOf<T>::type* __restrict__ spec,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  double* __restrict__ rowsum) {
+                                                  double* __restrict__ rowsum, int ncomp, int from_stress) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -75,10 +75,10 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_R2C].lines, ld = rows_ld(N);
-    const long long nrows = 9LL * I.rows;
+    const long long nrows = (long long)ncomp * I.rows;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const T* src = beta + I.foff;
+    const T* src = beta + (from_stress ? I.soff : I.foff);
 
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)src) & 15) == 0);
     if (vec) {
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
                                                   const typename VecOf<T>::type* __restrict__ spec,
                                                   T* __restrict__ sigma,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  const double* __restrict__ sbar) {
+                                                  const double* __restrict__ sbar, int ncomp, int to_field) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_C2R].lines, ld = rows_ld(N), nh = I.nh;
-    const long long nrows = 6LL * I.rows;
+    const long long nrows = (long long)ncomp * I.rows;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     __syncthreads();
     RowLayout lay{P, ld};
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
-    T* dst = sigma + I.soff;
+    T* dst = sigma + (to_field ? I.foff : I.soff);
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)dst) & 15) == 0);
     if (vec) {
 #pragma unroll 2
@@ -332,6 +332,121 @@ __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz
     }
 }
 
+// Transpose of green_point (a real linear map from 9 to 6 complex components per k point):
+// cotangents of the 6 stress components in, cotangents of the 9 beta components out. Each line
+// reverses one line of green_point.
+template <typename T, typename V>
+__device__ __forceinline__ void green_point_adj(const V* sb, V* bb, T kx, T ky, T kz, bool kzero,
+                                                T lam, T mu, T A, T B, T scale) {
+    const T k[3] = {kx, ky, kz};
+    const T ksq = kx * kx + ky * ky + kz * kz;
+    const T ikse = (T)1 / (ksq + (T)ME);
+    const T ikqe = (T)1 / (ksq * ksq + (T)ME);
+    const T mask = kzero ? (T)0 : (T)1;
+    const int ia[6] = {0, 0, 0, 1, 1, 2};
+    const int ja[6] = {0, 1, 2, 1, 2, 2};
+    V gb[3], trb;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { gb[j].x = 0; gb[j].y = 0; }
+    trb.x = 0; trb.y = 0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) { bb[c].x = 0; bb[c].y = 0; }
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const int i = ia[o], j = ja[o];
+        V v = vscale(sb[o], scale);
+        gb[j].x += mu * k[i] * v.x; gb[j].y += mu * k[i] * v.y;
+        gb[i].x += mu * k[j] * v.x; gb[i].y += mu * k[j] * v.y;
+        bb[3 * i + j].x -= mu * v.x; bb[3 * i + j].y -= mu * v.y;
+        bb[3 * j + i].x -= mu * v.x; bb[3 * j + i].y -= mu * v.y;
+        if (i == j) { trb.x += lam * v.x; trb.y += lam * v.y; }
+    }
+    V s1b;
+    s1b.x = -trb.x; s1b.y = -trb.y;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { gb[i].x += k[i] * trb.x; gb[i].y += k[i] * trb.y; }
+    V ccb, pb[3], qb[3];
+    ccb.x = mask * (k[0] * gb[0].x + k[1] * gb[1].x + k[2] * gb[2].x);
+    ccb.y = mask * (k[0] * gb[0].y + k[1] * gb[1].y + k[2] * gb[2].y);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        pb[j].x = mask * ikse * gb[j].x; pb[j].y = mask * ikse * gb[j].y;
+        qb[j] = pb[j];
+    }
+    s1b.x += A * ikse * ccb.x; s1b.y += A * ikse * ccb.y;
+    V rb;
+    rb.x = -B * ikqe * ccb.x; rb.y = -B * ikqe * ccb.y;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { qb[m].x += k[m] * rb.x; qb[m].y += k[m] * rb.y; }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            bb[3 * j + n].x += qb[j].x * k[n]; bb[3 * j + n].y += qb[j].y * k[n];   // q_j = b_jn k_n
+            bb[3 * n + j].x += k[n] * pb[j].x; bb[3 * n + j].y += k[n] * pb[j].y;   // p_j = k_m b_mj
+        }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) { bb[4 * m].x += s1b.x; bb[4 * m].y += s1b.y; }
+}
+
+// d sigma / d nu at fixed mu of green_point: A = nu/(1-nu), B = 1/(1-nu) and lam = 2 mu nu/(1-2nu)
+// give dA = dB = 1/(1-nu)^2 and dlam = 2 mu/(1-2nu)^2.
+template <typename T, typename V>
+__device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, T kz, bool kzero,
+                                                T lam, T mu, T A, T B, T scale, T nu) {
+    const T k[3] = {kx, ky, kz};
+    const T ksq = kx * kx + ky * ky + kz * kz;
+    const T ikse = (T)1 / (ksq + (T)ME);
+    const T ikqe = (T)1 / (ksq * ksq + (T)ME);
+    const T dA = (T)1 / ((1 - nu) * (1 - nu)), dB = dA;
+    const T dlam = (T)2 * mu / ((1 - 2 * nu) * (1 - 2 * nu));
+    V s1 = vadd(vadd(b[0], b[4]), b[8]);
+    V p[3], q[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        p[j].x = k[0] * b[j].x + k[1] * b[3 + j].x + k[2] * b[6 + j].x;
+        p[j].y = k[0] * b[j].y + k[1] * b[3 + j].y + k[2] * b[6 + j].y;
+        q[j].x = b[3 * j].x * k[0] + b[3 * j + 1].x * k[1] + b[3 * j + 2].x * k[2];
+        q[j].y = b[3 * j].y * k[0] + b[3 * j + 1].y * k[1] + b[3 * j + 2].y * k[2];
+    }
+    V r;
+    r.x = k[0] * q[0].x + k[1] * q[1].x + k[2] * q[2].x;
+    r.y = k[0] * q[0].y + k[1] * q[1].y + k[2] * q[2].y;
+    const T mask = kzero ? (T)0 : (T)1;
+    V cc, dcc;
+    cc.x = A * s1.x * ikse - B * r.x * ikqe;
+    cc.y = A * s1.y * ikse - B * r.y * ikqe;
+    dcc.x = dA * s1.x * ikse - dB * r.x * ikqe;
+    dcc.y = dA * s1.y * ikse - dB * r.y * ikqe;
+    V g[3], dg[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        g[j].x = mask * (k[j] * cc.x + (p[j].x + q[j].x) * ikse);
+        g[j].y = mask * (k[j] * cc.y + (p[j].y + q[j].y) * ikse);
+        dg[j].x = mask * k[j] * dcc.x;
+        dg[j].y = mask * k[j] * dcc.y;
+    }
+    V tr, dtr;
+    tr.x = k[0] * g[0].x + k[1] * g[1].x + k[2] * g[2].x - s1.x;
+    tr.y = k[0] * g[0].y + k[1] * g[1].y + k[2] * g[2].y - s1.y;
+    dtr.x = k[0] * dg[0].x + k[1] * dg[1].x + k[2] * dg[2].x;
+    dtr.y = k[0] * dg[0].y + k[1] * dg[1].y + k[2] * dg[2].y;
+    const int ia[6] = {0, 0, 0, 1, 1, 2};
+    const int ja[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const int i = ia[o], j = ja[o];
+        V v;
+        v.x = mu * (k[i] * dg[j].x + k[j] * dg[i].x);
+        v.y = mu * (k[i] * dg[j].y + k[j] * dg[i].y);
+        if (i == j) {
+            v.x += dlam * tr.x + lam * dtr.x;
+            v.y += dlam * tr.y + lam * dtr.y;
+        }
+        out[o] = vscale(v, scale);
+    }
+}
+
 // Shared memory: 12 component slots of N x W (+W pad): slots 0..8 hold the 9 components, 9..11
 // are the ping-pong scratch. The transforms run three components at a time against the scratch;
 // when the stage count is odd the result is copied back to the component slots.
@@ -348,7 +463,7 @@ __device__ __forceinline__ void fft_group3(V* s, int g, int N, int W, int cs, co
     }
 }
 
-template <typename T, bool MEAN64>
+template <typename T, bool MEAN64, int GMODE>
 __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restrict__ insts, int n_inst,
                                                          const int* __restrict__ pre,
                                                          typename VecOf<T>::type* __restrict__ spec,
@@ -373,8 +488,10 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
     const long long cstride = (long long)N * estride;
     V* base = spec + I.spoff + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0;
 
+    constexpr int NIN = (GMODE == 1) ? 6 : 9;     // components in / out of the k-space pass
+    constexpr int NOUT = (GMODE == 1) ? 9 : 6;
 #pragma unroll 4
-    for (int i = tid; i < 9 * N * W; i += nt) {
+    for (int i = tid; i < NIN * N * W; i += nt) {
         int c = i / (N * W);
         int rem = i - c * N * W;
         int e = rem / W, w = rem - e * W;
@@ -383,7 +500,7 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
         s[c * cs + rem] = z;
     }
     __syncthreads();
-    for (int g = 0; g < 3; ++g) fft_group3<V, false>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -406,17 +523,19 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
             kz = (T)0;
             kzero = (e == 0 && kh == 0);
         }
-        V b[9], o[6];
+        V b[NIN], o[NOUT];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) b[c] = s[c * cs + i];
-        green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64);
+        for (int c = 0; c < NIN; ++c) b[c] = s[c * cs + i];
+        if constexpr (GMODE == 0) green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64);
+        else if constexpr (GMODE == 1) green_point_adj<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale);
+        else green_point_dnu<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) s[c * cs + i] = o[c];
+        for (int c = 0; c < NOUT; ++c) s[c * cs + i] = o[c];
     }
     __syncthreads();
-    for (int g = 0; g < 2; ++g) fft_group3<V, true>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
 #pragma unroll 4
-    for (int i = tid; i < 6 * N * W; i += nt) {
+    for (int i = tid; i < NOUT * N * W; i += nt) {
         int c = i / (N * W);
         int rem = i - c * N * W;
         int e = rem / W, w = rem - e * W;
@@ -462,31 +581,66 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     const LaunchShape* L = P.pass;
     if (f32) {
         k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, 9, 0);
         k_mean_beta<<<dim3(P.n_inst, 9), 256, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, 9, 0);
     }
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
     if (f32)
-        k_green<T, true><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+        k_green<T, true, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
     else
-        k_green<T, false><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+        k_green<T, false, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
     if (f32)
         k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, 6, 0);
     else
         k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, 6, 0);
     return cudaGetLastError();
+}
+
+// Adjoint (GMODE 1: stress cotangent, 6 components in stress layout -> beta cotangent, 9 components
+// in field layout) and the nu-derivative of the stress (GMODE 2: 9 -> 6). Both keep the k = 0
+// mode in the transforms (no FP64 mean path).
+template <typename T, int GMODE>
+static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* out, cudaStream_t st) {
+    typedef typename VecOf<T>::type V;
+    V* spec = (V*)P.d_spec;
+    const V* tw = (const V*)P.d_tw;
+    const LaunchShape* L = (GMODE == 1) ? P.adj : P.pass;
+    const int nin = (GMODE == 1) ? 6 : 9, nout = (GMODE == 1) ? 9 : 6;
+    k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, nin, GMODE == 1 ? 1 : 0);
+    if (L[PASS_MID_F].blocks > 0)
+        k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
+    k_green<T, false, GMODE><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+    if (L[PASS_MID_I].blocks > 0)
+        k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
+    k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, nout, GMODE == 1 ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st) {
+    if (P.precision == CDD_F32) return run_stress_variant<float, 1>(P, sigbar6, betabar9, st);
+    return run_stress_variant<double, 1>(P, sigbar6, betabar9, st);
+}
+
+cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st) {
+    if (P.precision == CDD_F32) return run_stress_variant<float, 2>(P, beta, out6, st);
+    return run_stress_variant<double, 2>(P, beta, out6, st);
 }
 
 cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st) {
@@ -498,14 +652,17 @@ template <typename T>
 static cudaError_t set_attr_t(size_t smem) {
     cudaError_t e;
     int v = (int)smem;
-    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_fft_mid<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_fft_mid<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
+    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, true>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, false>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, true>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, false>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_fft_mid<T, true>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_fft_mid<T, false>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, true, 0>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, false, 0>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, false, 1>, A, v))) return e;
+    if ((e = cudaFuncSetAttribute(k_green<T, false, 2>, A, v))) return e;
     return cudaSuccess;
 }
 

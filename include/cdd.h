@@ -3,8 +3,9 @@
  *
  * One library, libcdd.so (sm_100a), built from cuda-plasticity_b200/csrc. Every entry point takes
  * plain pointers and sizes; device buffers are raw device pointers, streams are cudaStream_t
- * passed as void*. No entry point allocates memory except cdd_plan_create, which allocates the
- * plan's scratch (k-space spectra, stage buffers, reduction partials) once.
+ * passed as void*. Device memory is allocated only by cdd_plan_create (the plan's scratch: k-space
+ * spectra, stage buffers, reduction partials) and, on the first adjoint call on a plan, by the
+ * adjoint entry points (their scratch, kept until cdd_plan_destroy).
  *
  * Field layout ("packed field"): instances are concatenated; instance i starts at element
  * cdd_plan_field_offset(plan, i) and holds 9 components in the order xx, xy, xz, yx, yy, yz,
@@ -26,6 +27,8 @@
  */
 #ifndef CDD_H
 #define CDD_H
+
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -128,6 +131,40 @@ int cdd_run(cdd_plan* plan, void* beta, int n_steps, int use_graph, void* stream
  * Synchronises the stream. */
 int cdd_observables(cdd_plan* plan, const void* beta, double* energy, double* mean_zz,
                     void* stream);
+
+/* ---- adjoint (reverse-mode) building blocks ----
+ * Vector-Jacobian product of the flux at time t: with rhs = L(beta) = flux(beta, sigma(beta) + load),
+ * given gbar = d(loss)/d(rhs) (packed 9-component field) it writes
+ *   betabar = (dL/dbeta)^T gbar (packed 9-component field, overwritten),
+ *   sigbar6 = d(loss)/d(total stress) at every cell (packed 6-component field, off-diagonal entries
+ *             carry both (i,j) and (j,i)),
+ * and adds sum over cells of the diagonal of sigbar (the applied-load cotangent, 3 per instance)
+ * to the device array load_bar (may be NULL). The limiter selections and the corners attaining
+ * the directional speed maxima are those of the forward evaluation at beta.
+ * Reverse of BetaPDynamics.CalculateFlux (CentralUpwindHJBetaPDynamics3D.py L218-221 ->
+ * CentralUpwindHJ3D.py L189-271); the reference has no adjoint. Allocates the plan's adjoint
+ * scratch (54 derivative cotangents and 4 flag words per cell) on first use. */
+int cdd_flux_vjp(cdd_plan* plan, const void* beta, double t, const void* gbar, void* betabar,
+                 void* sigbar6, double* load_bar, void* stream);
+
+/* Branch record of the flux at beta and time t: the branches that cdd_flux_vjp differentiates
+ * through. flags (device): 4 words per cell, packed per instance like the field (instance i at
+ * 4 * (its field offset / 9)), word q of cell x at q * cells + x. Limiter slot s = 3 * component +
+ * axis holds 4 bits in word s / 8 at bit 4 * (s % 8): bits 0-1 the selection of the forward
+ * one-sided derivative's minmod (0 zero, 1 first argument, 2 second), bits 2-3 the backward one's.
+ * Bits 12-31 of word 3 hold, base 9, the corner (index + 1; 0 = the zero entry) attaining the max
+ * and then the min of each axis' corner velocity (CentralUpwindHJ3D.py L197-234). Two states
+ * with equal records lie on the same smooth piece of the flux. The reference has no counterpart. */
+int cdd_flux_branches(cdd_plan* plan, const void* beta, double t, uint32_t* flags, void* stream);
+
+/* Transposed stress operator: betabar9 = S^T sigbar6 (packed 6 -> packed 9 components,
+ * overwritten), S = the map of cdd_stress. Adjoint of PlasticityState.CalculateSigma
+ * (PlasticityState.py L85-127). */
+int cdd_stress_adjoint(cdd_plan* plan, const void* sigbar6, void* betabar9, void* stream);
+
+/* Derivative of the internal stress with respect to nu at fixed mu and beta:
+ * out6 = (dS/dnu) beta (packed 6 components). (dS/dmu) beta = S beta / mu needs no call. */
+int cdd_stress_dnu(cdd_plan* plan, const void* beta, void* out6, void* stream);
 
 /* Device status flags accumulated by kernels (CDD_ERR_NONFINITE, ...); clears them. */
 int cdd_check_status(cdd_plan* plan);
