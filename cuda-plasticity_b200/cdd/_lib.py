@@ -49,6 +49,8 @@ class CDDError(RuntimeError):
 
 _lib = None
 
+CDD_PBAR = 9   # doubles per instance in the parameter cotangent of cdd_step_adjoint
+
 _PROTOS = {
     "cdd_plan_create": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_void_p)]),
@@ -78,6 +80,11 @@ _PROTOS = {
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_flux_branches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
                                          ctypes.c_void_p]),
+    "cdd_plan_record_elems": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "cdd_step_record": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_step_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,

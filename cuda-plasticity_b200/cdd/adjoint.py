@@ -5,14 +5,13 @@ Forward: u_{n+1} = Step(u_n) with the three stages of FieldMover.CalculateOneFix
 time t_n, for n_steps steps from u_0; loss J = E(u_N) + w_zz * mean(u_N,zz) with E the elastic
 energy (PlasticityState.CalculateElasticEnergy L317-330 summed over cells).
 
-Reverse, per step (cotangent F2b of u_{n+1}; F0, F1 recomputed from u_n):
-    ub  = F2b / 3 ;  F1b = 2/3 F2b + L_{F1}^T (2/3 dt F2b)
-    ub += 3/4 F1b ;  F0b = 1/4 F1b + L_{F0}^T (1/4 dt F1b)
-    ub += F0b + L_u^T (dt F0b)
-where L_v^T g = cdd_flux_vjp (stencil VJP with recorded limiter branches + transposed Green's
-function). Checkpoints every ``checkpoint_every`` steps; the states inside a segment are recomputed
-from its checkpoint. Parameter gradients: mu and nu through the stress operator
-((dS/dmu) v = S v / mu, (dS/dnu) v by cdd_stress_dnu), through the load conversion
+Reverse, per step (cotangent F2b of u_{n+1}; stage states, stresses and k-space data recorded
+by cdd_step_record while re-running the step's checkpoint segment), in cdd_step_adjoint:
+    F1b = 2/3 F2b + 2/3 dt L_{F1}^T F2b ;  F0b = 1/4 F1b + 1/4 dt L_{F0}^T F1b
+    ub  = 1/3 F2b + 3/4 F1b + F0b + dt L_u^T F0b
+with L_v^T the flux VJP (stencil VJP with recorded limiter branches + transposed Green's function).
+Parameter gradients: mu through the stress (S ~ mu), nu through lambda (pointwise) and through the
+Green's function coefficients (a Parseval sum in k-space), both also through the load conversion
 (load_i = lamb tr(eps) + 2 mu eps_i with the instance's mu, nu) and through E; the applied strain
 rate as rate = r (-1/2, -1/2, 1) (traceless), eps = rate (t - t0).
 """
@@ -58,6 +57,10 @@ class Rollout:
 
     shape, mu, nu: grid and material; rate_zz: r of the traceless applied strain rate
     r (-1/2, -1/2, 1) (None: no load); dt: fixed step; precision "f64" or "f32".
+    The forward keeps a copy of the state every ``checkpoint_every`` steps; the reverse sweep
+    re-runs each segment from its checkpoint with cdd_step_record (saving stage states, stresses
+    and k-space data) and walks it backwards with cdd_step_adjoint. Nothing synchronises the host
+    until the parameter cotangents are read at the end.
     """
 
     def __init__(self, shape, mu, nu, rate_zz, dt, n_steps, precision="f32", checkpoint_every=20,
@@ -75,11 +78,15 @@ class Rollout:
         self.lib = self.plan.lib
         self.cells = int(np.prod(self.shape))
         self.checkpoints = {}
+        self.rec_elems = int(self.lib.cdd_plan_record_elems(self.plan.handle))
+        self._records = None
+
+    def time(self, n):
+        return self.t0 + n * self.dt
 
     # ------------------------------------------------------------------ forward
-    def _step(self, u, n):
-        self.plan.set_time(self.t0 + n * self.dt, 1e300)
-        self.plan.step_fixed(u, self.dt)
+    def _step(self, u, n, rec=None):
+        check(self.lib.cdd_step_record(self.plan.handle, _ptr(u), self.time(n), self.dt, _ptr(rec), _stream()))
 
     def forward(self, beta0):
         """Run n_steps from beta0 (packed field, plan dtype); returns (u_N, loss as float)."""
@@ -97,63 +104,40 @@ class Rollout:
 
     def branch_trace(self, beta0):
         """Branch records (cdd_flux_branches) of the 3 * n_steps flux evaluations of the trajectory
-        from beta0, at the states the reverse sweep differentiates at: an int32 tensor of shape
-        (3 * n_steps, 4 * cells). Two initial states with equal traces lie on the same smooth
+        from beta0, at the stage states the reverse sweep differentiates at: an int32 tensor of
+        shape (3 * n_steps, 4 * cells). Two initial states with equal traces lie on the same smooth
         piece of the loss."""
         p = self.plan
         out = torch.empty((3 * self.n_steps, 4 * self.cells), dtype=torch.int32, device=p.device)
+        rec = self._record_buffer(1)[0]
         u = beta0.detach().clone()
-        dt = self.dt
         for n in range(self.n_steps):
-            t = self.t0 + n * dt
-            F0 = u + dt * self._flux(u, t)
-            F1 = 0.75 * u + 0.25 * F0 + 0.25 * dt * self._flux(F0, t)
-            for k, v in enumerate((u, F0, F1)):
-                check(self.lib.cdd_flux_branches(p.handle, _ptr(v), float(t), _ptr(out[3 * n + k]), _stream()))
-            self._step(u, n)
+            self._step(u, n, rec)
+            for k, part in enumerate(self._record_parts(rec)):
+                check(self.lib.cdd_flux_branches(p.handle, _ptr(part), self.time(n), _ptr(out[3 * n + k]),
+                                                 _stream()))
         return out
 
     # ------------------------------------------------------------------ reverse
-    def _flux(self, v, t):
-        rhs, _ = self.plan.flux(v, t, want_speed=False)
-        return rhs
+    def _record_buffer(self, k):
+        if self._records is None or self._records.shape[0] < k:
+            el = torch.tensor([], dtype=self.plan.dtype).element_size()
+            pad = 256 // el
+            raw = torch.empty(k * self.rec_elems + pad, dtype=self.plan.dtype, device=self.plan.device)
+            off = (-raw.data_ptr() % 256) // el
+            self._raw = raw
+            self._records = raw[off:off + k * self.rec_elems].view(k, self.rec_elems)
+        return self._records
 
-    def _vjp(self, v, t, g, grads):
-        """Returns L_v^T g and accumulates parameter gradients."""
-        p = self.plan
-        vb = torch.zeros(p.field_elems, dtype=p.dtype, device=p.device)
-        sb = torch.zeros(p.stress_elems, dtype=p.dtype, device=p.device)
-        lb = torch.zeros(3, dtype=torch.float64, device=p.device)
-        check(self.lib.cdd_flux_vjp(p.handle, _ptr(v), float(t), _ptr(g), _ptr(vb), _ptr(sb), _ptr(lb),
-                                    _stream()))
-        self._param_terms(v, sb, lb, t, grads)
-        return vb
-
-    def _param_terms(self, v, sb, lb, t, grads):
-        p = self.plan
-        mu, nu = self.mu, self.nu
-        s_int = p.stress_view(p.stress(v), 0)
-        s_nu = p.empty_stress()
-        check(self.lib.cdd_stress_dnu(p.handle, _ptr(v), _ptr(s_nu), _stream()))
-        sbd = p.stress_view(sb, 0).double()
-        grads["mu"] += float((sbd * s_int.double()).sum()) / mu
-        grads["nu"] += float((sbd * p.stress_view(s_nu, 0).double()).sum())
-        if self.rate_zz is not None:
-            L = lb.cpu().numpy()
-            eps = self.rate_zz * CZZ * (t - self.t0)
-            lamb = 2.0 * mu * nu / (1.0 - 2.0 * nu)
-            tr = eps.sum()
-            dload_dmu = lamb / mu * tr + 2.0 * eps
-            dload_dnu = 2.0 * mu / (1.0 - 2.0 * nu) ** 2 * tr * np.ones(3)
-            dload_dr = (lamb * CZZ.sum() + 2.0 * mu * CZZ) * (t - self.t0)
-            grads["mu"] += float(L @ dload_dmu)
-            grads["nu"] += float(L @ dload_dnu)
-            grads["rate_zz"] += float(L @ dload_dr)
+    def _record_parts(self, rec):
+        """Views of the states u, F0, F1 inside a record (the first three 256-byte aligned parts)."""
+        el = rec.element_size()
+        step = -(-self.plan.field_elems * el // 256) * 256 // el
+        return [rec[i * step:i * step + self.plan.field_elems] for i in range(3)]
 
     def backward(self):
         """Gradients of the loss: (d/d beta0 as a packed field, dict of mu, nu, rate_zz)."""
         p = self.plan
-        grads = {"mu": 0.0, "nu": 0.0, "rate_zz": 0.0}
         mu, nu = self.mu, self.nu
         u = self.uN
         # loss terms at the final state
@@ -168,31 +152,34 @@ class Rollout:
         tr = (s6[0] + s6[3] + s6[5]).double()
         s_nu = p.empty_stress()
         check(self.lib.cdd_stress_dnu(p.handle, _ptr(u), _ptr(s_nu), _stream()))
-        grads["mu"] += float(-E / mu + (sE.double() * s6.double()).sum() / mu)
-        grads["nu"] += float((-(tr * tr) / (4.0 * mu * (1.0 + nu) ** 2)).sum()
-                             + (sE.double() * p.stress_view(s_nu, 0).double()).sum())
+        g_mu_loss = -E / mu + (sE.double() * s6.double()).sum() / mu
+        g_nu_loss = (-(tr * tr) / (4.0 * mu * (1.0 + nu) ** 2)).sum() + \
+            (sE.double() * p.stress_view(s_nu, 0).double()).sum()
         # reverse sweep over checkpoint segments
-        dt = self.dt
-        starts = sorted(self.checkpoints)
-        for s0 in reversed(starts):
+        pbar = torch.zeros(_lib.CDD_PBAR, dtype=torch.float64, device=p.device)
+        recs = self._record_buffer(self.K)
+        for s0 in sorted(self.checkpoints, reverse=True):
             s1 = min(s0 + self.K, self.n_steps)
-            states = [self.checkpoints[s0].clone()]
-            for n in range(s0, s1 - 1):
-                v = states[-1].clone()
-                self._step(v, n)
-                states.append(v)
+            v = self.checkpoints[s0].clone()
+            for n in range(s0, s1):
+                self._step(v, n, recs[n - s0])
             for n in range(s1 - 1, s0 - 1, -1):
-                un = states[n - s0]
-                t = self.t0 + n * dt
-                F0 = un + dt * self._flux(un, t)
-                F1 = 0.75 * un + 0.25 * F0 + 0.25 * dt * self._flux(F0, t)
-                F2b = ub
-                ub_new = F2b / 3.0
-                F1b = (2.0 / 3.0) * F2b + self._vjp(F1, t, (2.0 / 3.0) * dt * F2b, grads)
-                ub_new += 0.75 * F1b
-                F0b = 0.25 * F1b + self._vjp(F0, t, 0.25 * dt * F1b, grads)
-                ub_new += F0b + self._vjp(un, t, dt * F0b, grads)
-                ub = ub_new
+                check(self.lib.cdd_step_adjoint(p.handle, _ptr(recs[n - s0]), self.time(n), self.dt, _ptr(ub),
+                                                _ptr(pbar), _stream()))
+        pb = pbar.cpu().numpy()
+        lamb = 2.0 * mu * nu / (1.0 - 2.0 * nu)
+        dlam = 2.0 * mu / (1.0 - 2.0 * nu) ** 2
+        dA = 1.0 / (1.0 - nu) ** 2
+        grads = {"mu": float(g_mu_loss) + pb[0] / mu,
+                 "nu": float(g_nu_loss) + pb[1] * dlam / (2.0 * mu + 3.0 * lamb) + pb[2] * dA,
+                 "rate_zz": 0.0}
+        if self.rate_zz is not None:
+            # load_i(t) = lamb tr(eps) + 2 mu eps_i, eps = rate (t - t0), rate = r CZZ (traceless)
+            L, Lt = pb[3:6], pb[6:9]
+            rate = self.rate_zz * CZZ
+            grads["mu"] += float(Lt @ (lamb / mu * rate.sum() + 2.0 * rate))
+            grads["nu"] += float(Lt @ (dlam * rate.sum() * np.ones(3)))
+            grads["rate_zz"] += float(Lt @ (lamb * CZZ.sum() + 2.0 * mu * CZZ))
         p.check_status()
         return ub, grads
 

@@ -76,6 +76,7 @@ __device__ __forceinline__ double bsum(double v, double* red) {
 }
 
 constexpr int VJP_THREADS = 128;
+constexpr int VJP_PARTS = 5;     // per-block partials: <sigbar, sigma>, tr tr, diag sigbar (3)
 
 template <typename T, int ND>
 __device__ __forceinline__ void vjp_cell(const InstDev& I, long long cl, bool valid, const T* __restrict__ beta,
@@ -122,8 +123,8 @@ __device__ __forceinline__ void vjp_cell(const InstDev& I, long long cl, bool va
     }
     const T* sp6 = sig + I.soff + cl;
     T S[3][3];
+    T s6[6];
     {
-        T s6[6];
 #pragma unroll
         for (int c = 0; c < 6; ++c) s6[c] = sp6[c * cells];
         S[0][0] = (T)((double)s6[0] + add[0]);
@@ -490,9 +491,18 @@ __device__ __forceinline__ void vjp_cell(const InstDev& I, long long cl, bool va
         sb[3 * cells] = Sb[1][1];
         sb[4 * cells] = Sb[1][2] + Sb[2][1];
         sb[5 * cells] = Sb[2][2];
-        lsum[0] += (double)Sb[0][0];
-        lsum[1] += (double)Sb[1][1];
-        lsum[2] += (double)Sb[2][2];
+        // parameter partials: <sigbar, sigma_int> (mu), tr sigbar tr sigma_int (nu through lambda),
+        // and the diagonal of sigbar (the applied load)
+        const double sb6[6] = {(double)Sb[0][0], (double)(Sb[0][1] + Sb[1][0]), (double)(Sb[0][2] + Sb[2][0]),
+                               (double)Sb[1][1], (double)(Sb[1][2] + Sb[2][1]), (double)Sb[2][2]};
+        double dot = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) dot += sb6[c] * (double)s6[c];
+        lsum[0] += dot;
+        lsum[1] += (sb6[0] + sb6[3] + sb6[5]) * ((double)s6[0] + (double)s6[3] + (double)s6[5]);
+        lsum[2] += sb6[0];
+        lsum[3] += sb6[3];
+        lsum[4] += sb6[5];
     }
     if (ubar) {
         T* ub = ubar + 54 * I.coff + cl;
@@ -533,15 +543,16 @@ __global__ void __launch_bounds__(VJP_THREADS) k_vjp_cells(const InstDev* __rest
     const InstDev& I = insts[ii];
     const long long cell = (long long)(blockIdx.x - pre[ii]) * VJP_THREADS + threadIdx.x;
     const bool valid = cell < I.cells;
-    double lsum[3] = {0.0, 0.0, 0.0};
+    double lsum[VJP_PARTS] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (I.nd == 3)
         vjp_cell<T, 3>(I, valid ? cell : 0, valid, beta, sig, gbar, t, ubar, flags, sigbar, lsum);
     else
         vjp_cell<T, 2>(I, valid ? cell : 0, valid, beta, sig, gbar, t, ubar, flags, sigbar, lsum);
+    if (!sigbar) return;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < VJP_PARTS; ++i) {
         double s = bsum<T>(lsum[i], red);
-        if (threadIdx.x == 0) bload[3 * blockIdx.x + i] = s;
+        if (threadIdx.x == 0) bload[VJP_PARTS * blockIdx.x + i] = s;
     }
 }
 
@@ -567,10 +578,18 @@ __device__ __forceinline__ float coef_m(int q, int s) {
     }
 }
 
+// out = c (L^T g) + a1 x1 + a2 x2 + a3 x3 (absent x terms skipped), L^T g = ih * gather + addend.
+template <typename T>
+struct Axpy {
+    T c;
+    const T* x[3];
+    T a[3];
+};
+
 template <typename T, int ND>
 __device__ __forceinline__ void gather_cell(const InstDev& I, long long y, const T* __restrict__ ubar,
                                             const uint32_t* __restrict__ flags, const T* __restrict__ addend,
-                                            T* __restrict__ out) {
+                                            const Axpy<T>& ax, T* out) {
     const long long cells = I.cells;
     Nbr nb[ND];
     if (ND == 3) {
@@ -608,9 +627,14 @@ __device__ __forceinline__ void gather_cell(const InstDev& I, long long y, const
                 acc += up * (T)coef_p(q, (int)(f & 3u)) + um * (T)coef_m(q, (int)(f >> 2));
             }
         }
+        const long long o = I.foff + (long long)c * cells + y;
         T v = acc * ih;
-        if (addend) v += addend[I.foff + (long long)c * cells + y];
-        out[I.foff + (long long)c * cells + y] = v;
+        if (addend) v += addend[o];
+        v *= ax.c;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (ax.x[k]) v += ax.a[k] * ax.x[k][o];
+        out[o] = v;
     }
 }
 
@@ -618,13 +642,14 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_vjp_gather(const InstDev* __restrict__ insts, int n_inst,
                                                     const int* __restrict__ pre, const T* __restrict__ ubar,
                                                     const uint32_t* __restrict__ flags,
-                                                    const T* __restrict__ addend, T* __restrict__ out) {
+                                                    const T* __restrict__ addend, const Axpy<T> ax,
+                                                    T* out) {   // out may alias an x term (same element)
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
     const long long y = (long long)(blockIdx.x - pre[ii]) * blockDim.x + threadIdx.x;
     if (y >= I.cells) return;
-    if (I.nd == 3) gather_cell<T, 3>(I, y, ubar, flags, addend, out);
-    else gather_cell<T, 2>(I, y, ubar, flags, addend, out);
+    if (I.nd == 3) gather_cell<T, 3>(I, y, ubar, flags, addend, ax, out);
+    else gather_cell<T, 2>(I, y, ubar, flags, addend, ax, out);
 }
 
 // Per-instance sums of the block partials of the load cotangent, added to the caller's array.
@@ -634,9 +659,44 @@ __global__ void __launch_bounds__(256) k_vjp_load_reduce(const int* __restrict__
     const int ii = blockIdx.x;
     for (int i = 0; i < 3; ++i) {
         double acc = 0.0;
-        for (int b = pre[ii] + threadIdx.x; b < pre[ii + 1]; b += blockDim.x) acc += bload[3 * b + i];
+        for (int b = pre[ii] + threadIdx.x; b < pre[ii + 1]; b += blockDim.x) acc += bload[VJP_PARTS * b + 2 + i];
         acc = bsum<double>(acc, red);
         if (threadIdx.x == 0) out[3 * ii + i] += acc;
+    }
+}
+
+// Parameter cotangents of one stage, scaled by the stage weight c and added to pbar (CDD_PBAR
+// doubles per instance): [0] <sigbar, sigma_int>, [1] tr sigbar . tr sigma_int, [2] the k-space
+// sum of the nu derivative per unit dA (from the green-block partials), [3..5] the diagonal of
+// sigbar (load), [6..8] the same times (t - load_t0).
+__global__ void __launch_bounds__(256) k_param_reduce(const InstDev* __restrict__ insts,
+                                                      const int* __restrict__ pre_v, const double* __restrict__ bpart,
+                                                      const int* __restrict__ pre_g, const double* __restrict__ gpart,
+                                                      double c, double t, double* __restrict__ pbar) {
+    __shared__ double red[8];
+    const int ii = blockIdx.x;
+    double v[VJP_PARTS + 1];
+    for (int i = 0; i < VJP_PARTS; ++i) {
+        double acc = 0.0;
+        for (int b = pre_v[ii] + threadIdx.x; b < pre_v[ii + 1]; b += blockDim.x) acc += bpart[VJP_PARTS * b + i];
+        v[i] = bsum<double>(acc, red);
+    }
+    {
+        double acc = 0.0;
+        if (gpart)
+            for (int b = pre_g[ii] + threadIdx.x; b < pre_g[ii + 1]; b += blockDim.x) acc += gpart[b];
+        v[VJP_PARTS] = bsum<double>(acc, red);
+    }
+    if (threadIdx.x == 0) {
+        double* o = pbar + CDD_PBAR * ii;
+        const double tl = t - insts[ii].load_t0;
+        o[0] += c * v[0];
+        o[1] += c * v[1];
+        o[2] += c * v[5];
+        for (int i = 0; i < 3; ++i) {
+            o[3 + i] += c * v[2 + i];
+            o[6 + i] += c * tl * v[2 + i];
+        }
     }
 }
 
@@ -654,6 +714,43 @@ cudaError_t launch_flux_branches(const PlanCore& P, const void* beta, double t, 
         k_vjp_cells<double><<<V.blocks, VJP_THREADS, 0, st>>>(P.d_inst, P.n_inst, V.d_pre, (const double*)beta,
                                                              (const double*)P.d_sigma, nullptr, t, nullptr, flags,
                                                              nullptr, P.d_bload);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vjp_stage(const PlanCore& P, const void* v, const void* sig_v, const void* phi_v, double t,
+                             const void* gbar, double c, const void* const x[3], const double a[3], void* out,
+                             double* pbar, cudaStream_t st) {
+    const LaunchShape& V = P.vjp;
+    const LaunchShape& G = P.obs;
+    cudaError_t e;
+    const bool f32 = (P.precision == CDD_F32);
+    if (f32)
+        k_vjp_cells<float><<<V.blocks, VJP_THREADS, 0, st>>>(P.d_inst, P.n_inst, V.d_pre, (const float*)v,
+                                                            (const float*)sig_v, (const float*)gbar, t,
+                                                            (float*)P.d_ubar, P.d_flags, (float*)P.d_sb6, P.d_bload);
+    else
+        k_vjp_cells<double><<<V.blocks, VJP_THREADS, 0, st>>>(P.d_inst, P.n_inst, V.d_pre, (const double*)v,
+                                                             (const double*)sig_v, (const double*)gbar, t,
+                                                             (double*)P.d_ubar, P.d_flags, (double*)P.d_sb6,
+                                                             P.d_bload);
+    if ((e = cudaGetLastError())) return e;
+    if ((e = launch_stress_adjoint(P, P.d_sb6, P.d_adj9, st, pbar ? phi_v : nullptr, pbar ? P.d_gpart : nullptr)))
+        return e;
+    if (pbar) {
+        k_param_reduce<<<P.n_inst, 256, 0, st>>>(P.d_inst, V.d_pre, P.d_bload, P.adj[PASS_GREEN].d_pre,
+                                                 phi_v ? P.d_gpart : nullptr, c, t, pbar);
+        if ((e = cudaGetLastError())) return e;
+    }
+    if (f32) {
+        Axpy<float> ax{(float)c, {(const float*)x[0], (const float*)x[1], (const float*)x[2]},
+                       {(float)a[0], (float)a[1], (float)a[2]}};
+        k_vjp_gather<float><<<G.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, G.d_pre, (const float*)P.d_ubar, P.d_flags,
+                                                     (const float*)P.d_adj9, ax, (float*)out);
+    } else {
+        Axpy<double> ax{c, {(const double*)x[0], (const double*)x[1], (const double*)x[2]}, {a[0], a[1], a[2]}};
+        k_vjp_gather<double><<<G.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, G.d_pre, (const double*)P.d_ubar,
+                                                      P.d_flags, (const double*)P.d_adj9, ax, (double*)out);
+    }
     return cudaGetLastError();
 }
 
@@ -676,12 +773,15 @@ cudaError_t launch_flux_vjp(const PlanCore& P, const void* beta, double t, const
     if ((e = cudaGetLastError())) return e;
     if (load_bar) k_vjp_load_reduce<<<P.n_inst, 256, 0, st>>>(V.d_pre, P.d_bload, load_bar);
     if ((e = launch_stress_adjoint(P, sigbar, P.d_adj9, st))) return e;
-    if (P.precision == CDD_F32)
+    if (P.precision == CDD_F32) {
+        const Axpy<float> ax{1.f, {nullptr, nullptr, nullptr}, {0.f, 0.f, 0.f}};
         k_vjp_gather<float><<<G.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, G.d_pre, (const float*)P.d_ubar, P.d_flags,
-                                                     (const float*)P.d_adj9, (float*)betabar);
-    else
+                                                     (const float*)P.d_adj9, ax, (float*)betabar);
+    } else {
+        const Axpy<double> ax{1.0, {nullptr, nullptr, nullptr}, {0.0, 0.0, 0.0}};
         k_vjp_gather<double><<<G.blocks, 256, 0, st>>>(P.d_inst, P.n_inst, G.d_pre, (const double*)P.d_ubar,
-                                                      P.d_flags, (const double*)P.d_adj9, (double*)betabar);
+                                                      P.d_flags, (const double*)P.d_adj9, ax, (double*)betabar);
+    }
     return cudaGetLastError();
 }
 

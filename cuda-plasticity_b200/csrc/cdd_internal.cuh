@@ -340,8 +340,12 @@ struct PlanCore {
     LaunchShape vjp;                 // flux VJP: 128 cells per block
     void* d_ubar = nullptr;          // adjoint scratch (allocated on first use): 54 derivative cotangents per cell
     uint32_t* d_flags = nullptr;     // limiter selections, 4 words per cell
-    double* d_bload = nullptr;       // per-block load-cotangent partials (3 per block)
+    double* d_bload = nullptr;       // per-block parameter partials of the VJP (VJP_PARTS per block)
     void* d_adj9 = nullptr;          // beta cotangent from the adjoint stress solve
+    void* d_sb6 = nullptr;           // stress cotangent of one stage (6 components)
+    double* d_gpart = nullptr;       // per-green-block partials of the Parseval nu sum
+    void* d_f0b = nullptr;           // reverse RK3: cotangents of F0 and F1
+    void* d_f1b = nullptr;
 };
 
 // Tensor maps of one stage-input buffer for the TMA-staged instances (see stencil.cu).
@@ -351,11 +355,19 @@ struct StencilMapSet {
 };
 
 // stress.cu
-cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st);
-cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st);
+// phi (optional): per k point of the input, s1 / kSq - r / kSqSq (see k_green), for the nu gradient.
+cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st, void* phi = nullptr);
+// phi / part (optional): phi of the state, per-green-block partials of the Parseval nu sum.
+cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st,
+                                  const void* phi = nullptr, double* part = nullptr);
 cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st);
 // adjoint.cu
 cudaError_t launch_flux_branches(const PlanCore& P, const void* beta, double t, uint32_t* flags, cudaStream_t st);
+// One stage of the reverse sweep: out = c L_v^T g + sum a_k x_k (x_k may be null), with v's stress
+// sig_v and k-space phi_v precomputed; parameter cotangents (scaled by c) added to pbar if non-null.
+cudaError_t launch_vjp_stage(const PlanCore& P, const void* v, const void* sig_v, const void* phi_v, double t,
+                             const void* gbar, double c, const void* const x[3], const double a[3], void* out,
+                             double* pbar, cudaStream_t st);
 cudaError_t launch_flux_vjp(const PlanCore& P, const void* beta, double t, const void* gbar, void* sigbar,
                             void* betabar, double* load_bar, cudaStream_t st);
 // stencil.cu
@@ -367,6 +379,7 @@ cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const vo
 bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* base, StencilMapSet& maps);
 bool stencil_tma_eligible(const InstDev& I, int precision);
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
+cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st);
 cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaStream_t st);
 cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st);
 cudaError_t stencil_set_attributes(int precision, size_t smem);

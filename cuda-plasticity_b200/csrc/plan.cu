@@ -616,10 +616,39 @@ int ensure_adjoint_scratch(cdd_plan* p) {
     cudaError_t e;
     if ((e = dalloc(p, &C.d_ubar, elt * 54 * (size_t)C.cells)) ||
         (e = dalloc(p, (void**)&C.d_flags, sizeof(uint32_t) * 4 * (size_t)C.cells)) ||
-        (e = dalloc(p, (void**)&C.d_bload, sizeof(double) * 3 * (size_t)C.vjp.blocks)) ||
-        (e = dalloc(p, &C.d_adj9, elt * (size_t)C.field_elems)))
+        (e = dalloc(p, (void**)&C.d_bload, sizeof(double) * 5 * (size_t)C.vjp.blocks)) ||
+        (e = dalloc(p, &C.d_adj9, elt * (size_t)C.field_elems)) ||
+        (e = dalloc(p, &C.d_sb6, elt * (size_t)C.stress_elems)) ||
+        (e = dalloc(p, (void**)&C.d_gpart, sizeof(double) * (size_t)C.adj[PASS_GREEN].blocks)) ||
+        (e = dalloc(p, &C.d_f0b, elt * (size_t)C.field_elems)) ||
+        (e = dalloc(p, &C.d_f1b, elt * (size_t)C.field_elems)))
         return fail(CDD_ERR_ALLOC, "adjoint scratch: %s", cudaGetErrorString(e));
     return CDD_OK;
+}
+
+// Step record: u, F0, F1 (fields), their stresses, their phi spectra; every part starts on a
+// 256-byte boundary (offsets in elements).
+struct RecLayout {
+    long long u, f0, f1, su, sf0, sf1, pu, pf0, pf1, total;
+};
+
+RecLayout rec_layout(const PlanCore& C) {
+    const long long elt = C.precision == CDD_F64 ? 8 : 4;
+    const long long a = 256 / elt;
+    auto up = [a](long long n) { return (n + a - 1) / a * a; };
+    const long long F = up(C.field_elems), S = up(C.stress_elems), Ph = up(2 * (C.spec_elems / 9));
+    RecLayout r;
+    r.u = 0;
+    r.f0 = F;
+    r.f1 = 2 * F;
+    r.su = 3 * F;
+    r.sf0 = 3 * F + S;
+    r.sf1 = 3 * F + 2 * S;
+    r.pu = 3 * F + 3 * S;
+    r.pf0 = r.pu + Ph;
+    r.pf1 = r.pu + 2 * Ph;
+    r.total = r.pu + 3 * Ph;
+    return r;
 }
 }  // namespace
 
@@ -651,6 +680,87 @@ int cdd_stress_dnu(cdd_plan* p, const void* beta, void* out6, void* stream) {
     if (int rc = check_plan(p)) return rc;
     if (!beta || !out6) return fail(CDD_ERR_ARG, "null buffer");
     CDD_CUDA(launch_stress_dnu(p->core, beta, out6, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+long long cdd_plan_record_elems(const cdd_plan* p) {
+    if (!p) return -1;
+    return rec_layout(p->core).total;
+}
+
+int cdd_step_record(cdd_plan* p, void* beta, double t, double dt, void* rec, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta) return fail(CDD_ERR_ARG, "null buffer");
+    if (!(dt >= 0)) return fail(CDD_ERR_ARG, "dt must be >= 0");
+    if (rec && ((uintptr_t)rec & 255)) return fail(CDD_ERR_ARG, "record must be 256-byte aligned");
+    cudaStream_t st = (cudaStream_t)stream;
+    PlanCore& C = p->core;
+    const size_t elt = C.precision == CDD_F64 ? sizeof(double) : sizeof(float);
+    if (!rec) {
+        CDD_CUDA(launch_set_clock(C, t, st));
+        return record_step(p, beta, st, 1, dt);
+    }
+    const RecLayout L = rec_layout(C);
+    char* r = (char*)rec;
+    void* u = r + L.u * elt;
+    void* f0 = r + L.f0 * elt;
+    void* f1 = r + L.f1 * elt;
+    void* s_u = r + L.su * elt;
+    void* s_f0 = r + L.sf0 * elt;
+    void* s_f1 = r + L.sf1 * elt;
+    // the stencil reads the stress of its input from core.d_sigma: point a copy at the record's
+    PlanCore K = C;
+    CDD_CUDA(launch_set_clock(C, t, st));
+    CDD_CUDA(cudaMemcpyAsync(u, beta, elt * (size_t)C.field_elems, cudaMemcpyDeviceToDevice, st));
+    CDD_CUDA(launch_stress(C, beta, s_u, st, r + L.pu * elt));
+    K.d_sigma = s_u;
+    CDD_CUDA(launch_stencil(K, M_STAGE1, beta, beta, f0, nullptr, 0.0, user_maps(p, beta), st));
+    CDD_CUDA(launch_dt(C, 1, dt, st));
+    CDD_CUDA(launch_axpy_f0(C, beta, f0, st));
+    CDD_CUDA(launch_stress(C, f0, s_f0, st, r + L.pf0 * elt));
+    K.d_sigma = s_f0;
+    StencilMapSet m0, m1;
+    encode_stencil_maps(C, p->inst.data(), f0, m0);
+    CDD_CUDA(launch_stencil(K, M_STAGE2, f0, beta, f1, nullptr, 0.0, m0, st));
+    CDD_CUDA(launch_stress(C, f1, s_f1, st, r + L.pf1 * elt));
+    K.d_sigma = s_f1;
+    encode_stencil_maps(C, p->inst.data(), f1, m1);
+    CDD_CUDA(launch_stencil(K, M_STAGE3, f1, beta, beta, nullptr, 0.0, m1, st));
+    return CDD_OK;
+}
+
+int cdd_step_adjoint(cdd_plan* p, const void* rec, double t, double dt, void* ubar, double* pbar, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!rec || !ubar) return fail(CDD_ERR_ARG, "null buffer");
+    if (int rc = ensure_adjoint_scratch(p)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    PlanCore& C = p->core;
+    const size_t elt = C.precision == CDD_F64 ? sizeof(double) : sizeof(float);
+    const RecLayout L = rec_layout(C);
+    const char* r = (const char*)rec;
+    const void* u = r + L.u * elt;
+    const void* f0 = r + L.f0 * elt;
+    const void* f1 = r + L.f1 * elt;
+    // stage 3: F2 = 1/3 u + 2/3 F1 + 2/3 dt L(F1)
+    {
+        const void* x[3] = {ubar, nullptr, nullptr};
+        const double a[3] = {2.0 / 3.0, 0.0, 0.0};
+        CDD_CUDA(launch_vjp_stage(C, f1, r + L.sf1 * elt, r + L.pf1 * elt, t, ubar, 2.0 / 3.0 * dt, x, a, C.d_f1b,
+                                  pbar, st));
+    }
+    // stage 2: F1 = 3/4 u + 1/4 F0 + 1/4 dt L(F0)
+    {
+        const void* x[3] = {C.d_f1b, nullptr, nullptr};
+        const double a[3] = {0.25, 0.0, 0.0};
+        CDD_CUDA(launch_vjp_stage(C, f0, r + L.sf0 * elt, r + L.pf0 * elt, t, C.d_f1b, 0.25 * dt, x, a, C.d_f0b,
+                                  pbar, st));
+    }
+    // stage 1: F0 = u + dt L(u); u also feeds F1 (3/4) and F2 (1/3) directly
+    {
+        const void* x[3] = {C.d_f0b, ubar, C.d_f1b};
+        const double a[3] = {1.0, 1.0 / 3.0, 0.75};
+        CDD_CUDA(launch_vjp_stage(C, u, r + L.su * elt, r + L.pu * elt, t, C.d_f0b, dt, x, a, ubar, pbar, st));
+    }
     return CDD_OK;
 }
 

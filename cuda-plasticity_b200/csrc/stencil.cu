@@ -832,6 +832,20 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
     return any;
 }
 
+// Start every instance's clock at t with no end time (fixed-dt steps at a caller-given time).
+__global__ void k_set_clock(InstClock* __restrict__ clk, int n_inst, double t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_inst) {
+        clk[i].t = t;
+        clk[i].t_end = 1.0e300;
+    }
+}
+
+cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st) {
+    k_set_clock<<<(P.n_inst + 127) / 128, 128, 0, st>>>(P.d_clock, P.n_inst, t);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st) {
     k_dt<<<P.n_inst, 256, 0, st>>>(P.d_inst, P.stencil.d_pre, P.d_bmax, P.d_bsum, P.d_clock, P.d_obs,
                                    P.d_status, fixed, dt_fixed);

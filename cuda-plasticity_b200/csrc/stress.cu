@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
 // ------------------------------------------------------------------------------------------
 template <typename T, typename V>
 __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz, bool kzero,
-                                            T lam, T mu, T A, T B, T scale, bool drop_k0) {
+                                            T lam, T mu, T A, T B, T scale, bool drop_k0, V* phi_out) {
     const T k[3] = {kx, ky, kz};
     const T ksq = kx * kx + ky * ky + kz * kz;
     const T ikse = (T)1 / (ksq + (T)ME);
@@ -307,6 +307,12 @@ __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz
     cc.x = A * s1.x * ikse - B * r.x * ikqe;
     cc.y = A * s1.y * ikse - B * r.y * ikqe;
     const T mask = kzero ? (T)0 : (T)1;
+    if (phi_out) {
+        // phi = s1 / kSq - r / kSqSq: g_j depends on nu only through k_j (dA s1 / kSq - dB r / kSqSq)
+        // with dA = dB, so d sigma / d nu at this k point is a multiple of phi (minus the lambda term)
+        phi_out->x = mask * (s1.x * ikse - r.x * ikqe);
+        phi_out->y = mask * (s1.y * ikse - r.y * ikqe);
+    }
     V g[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
@@ -463,12 +469,20 @@ __device__ __forceinline__ void fft_group3(V* s, int g, int N, int W, int cs, co
     }
 }
 
+// phi (optional, one complex value per k point, laid out like one spectrum component with the
+// instance base spoff / 9): GMODE 0 writes phi of the input; GMODE 1 reads the phi of the state
+// whose stress the cotangent belongs to and writes, per block, the partial Parseval sum
+// sum_k w_k Re(conj(sigbar_hat) . (2 mu k k + lam kSq I) phi) / cells (w_k = 1 on the first and
+// the Nyquist half-axis column, 2 elsewhere): the A/B part of <sigbar, (d sigma / d nu) beta>
+// per unit dA.
 template <typename T, bool MEAN64, int GMODE>
 __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restrict__ insts, int n_inst,
                                                          const int* __restrict__ pre,
                                                          typename VecOf<T>::type* __restrict__ spec,
                                                          const typename VecOf<T>::type* __restrict__ tw,
-                                                         const T* __restrict__ ktab) {
+                                                         const T* __restrict__ ktab,
+                                                         typename VecOf<T>::type* __restrict__ phi,
+                                                         double* __restrict__ part) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -506,6 +520,8 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
     const T B = (T)(2.0 * (I.lamb + I.mu) / (I.lamb + 2.0 * I.mu));
     const T scale = (T)I.inv_cells;
+    V* phib = phi ? phi + I.spoff / 9 + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0 : nullptr;
+    double pacc = 0.0;
     for (int i = tid; i < N * W; i += nt) {
         int e = i / W, w = i - e * W;
         int kh = col0 + w;
@@ -526,11 +542,45 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
         V b[NIN], o[NOUT];
 #pragma unroll
         for (int c = 0; c < NIN; ++c) b[c] = s[c * cs + i];
-        if constexpr (GMODE == 0) green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64);
-        else if constexpr (GMODE == 1) green_point_adj<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale);
-        else green_point_dnu<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
+        if constexpr (GMODE == 0) {
+            V ph;
+            green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64, phib ? &ph : nullptr);
+            if (phib) phib[e * estride + w] = ph;
+        } else if constexpr (GMODE == 1) {
+            if (phib) {
+                const V ph = phib[e * estride + w];
+                const double k3[3] = {(double)kx, (double)ky, (double)kz};
+                const double ksq = k3[0] * k3[0] + k3[1] * k3[1] + k3[2] * k3[2];
+                const int ia[6] = {0, 0, 0, 1, 1, 2}, ja[6] = {0, 1, 2, 1, 2, 2};
+                double acc = 0.0;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    double cf = 2.0 * (double)I.mu * k3[ia[c]] * k3[ja[c]];
+                    if (ia[c] == ja[c]) cf += I.lamb * ksq;
+                    acc += cf * ((double)b[c].x * (double)ph.x + (double)b[c].y * (double)ph.y);
+                }
+                const bool edge = (kh == 0) || (2 * kh == I.nl);
+                pacc += (edge ? 1.0 : 2.0) * acc;
+            }
+            green_point_adj<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale);
+        } else {
+            green_point_dnu<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
+        }
 #pragma unroll
         for (int c = 0; c < NOUT; ++c) s[c * cs + i] = o[c];
+    }
+    if (GMODE == 1 && part) {
+        // fixed-order block reduction (deterministic); the FFT below re-synchronises the block
+        __shared__ double red[GREEN_THREADS / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pacc += __shfl_xor_sync(0xffffffffu, pacc, o);
+        if ((tid & 31) == 0) red[tid >> 5] = pacc;
+        __syncthreads();
+        if (tid == 0) {
+            double sum = 0.0;
+            for (int w = 0; w < nt / 32; ++w) sum += red[w];
+            part[blockIdx.x] = sum * I.inv_cells;
+        }
     }
     __syncthreads();
     for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
@@ -573,7 +623,7 @@ __global__ void __launch_bounds__(256) k_mean_beta(const InstDev* __restrict__ i
 // Host launch sequence
 // ------------------------------------------------------------------------------------------
 template <typename T>
-static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st) {
+static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, void* phi, cudaStream_t st) {
     typedef typename VecOf<T>::type V;
     const bool f32 = (P.precision == CDD_F32);
     V* spec = (V*)P.d_spec;
@@ -592,10 +642,10 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
             P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
     if (f32)
         k_green<T, true, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
     else
         k_green<T, false, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
@@ -612,7 +662,8 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
 // in field layout) and the nu-derivative of the stress (GMODE 2: 9 -> 6). Both keep the k = 0
 // mode in the transforms (no FP64 mean path).
 template <typename T, int GMODE>
-static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* out, cudaStream_t st) {
+static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* out, const void* phi, double* part,
+                                      cudaStream_t st) {
     typedef typename VecOf<T>::type V;
     V* spec = (V*)P.d_spec;
     const V* tw = (const V*)P.d_tw;
@@ -624,7 +675,7 @@ static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* o
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
     k_green<T, false, GMODE><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k);
+        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, part);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
@@ -633,19 +684,20 @@ static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* o
     return cudaGetLastError();
 }
 
-cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st) {
-    if (P.precision == CDD_F32) return run_stress_variant<float, 1>(P, sigbar6, betabar9, st);
-    return run_stress_variant<double, 1>(P, sigbar6, betabar9, st);
+cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st,
+                                  const void* phi, double* part) {
+    if (P.precision == CDD_F32) return run_stress_variant<float, 1>(P, sigbar6, betabar9, phi, part, st);
+    return run_stress_variant<double, 1>(P, sigbar6, betabar9, phi, part, st);
 }
 
 cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st) {
-    if (P.precision == CDD_F32) return run_stress_variant<float, 2>(P, beta, out6, st);
-    return run_stress_variant<double, 2>(P, beta, out6, st);
+    if (P.precision == CDD_F32) return run_stress_variant<float, 2>(P, beta, out6, nullptr, nullptr, st);
+    return run_stress_variant<double, 2>(P, beta, out6, nullptr, nullptr, st);
 }
 
-cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st) {
-    if (P.precision == CDD_F32) return run_stress<float>(P, beta, sigma, st);
-    return run_stress<double>(P, beta, sigma, st);
+cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st, void* phi) {
+    if (P.precision == CDD_F32) return run_stress<float>(P, beta, sigma, phi, st);
+    return run_stress<double>(P, beta, sigma, phi, st);
 }
 
 template <typename T>

@@ -166,6 +166,38 @@ int cdd_stress_adjoint(cdd_plan* plan, const void* sigbar6, void* betabar9, void
  * out6 = (dS/dnu) beta (packed 6 components). (dS/dmu) beta = S beta / mu needs no call. */
 int cdd_stress_dnu(cdd_plan* plan, const void* beta, void* out6, void* stream);
 
+/* ---- checkpointed reverse sweep of fixed-dt runs (no counterpart in the reference) ----
+ * A "step record" holds what the reverse of one fixed-dt step needs: the step's input u, its
+ * stage states F0 and F1 (FieldMover.py L38-58), their internal stresses and, per k point, the
+ * scalar spectrum s1 / kSq - r / kSqSq of each of the three states (s1 = trace, r = k.beta.k of
+ * the transformed beta), from which the nu gradient follows by Parseval without extra FFTs.
+ * cdd_plan_record_elems gives its size in plan elements (double or float); the caller owns the
+ * records (device memory, 256-byte aligned). */
+long long cdd_plan_record_elems(const cdd_plan* plan);
+
+/* One TVD-RK3 step of every instance with the fixed dt, starting at time t (the plan clock is set
+ * to t with no end time and advanced by dt). Bitwise the same update as cdd_set_time + cdd_step_fixed.
+ * rec (device, may be NULL): when given, the step's record is written there. No host
+ * synchronisation. */
+int cdd_step_record(cdd_plan* plan, void* beta, double t, double dt, void* rec, void* stream);
+
+/* Number of doubles per instance of the parameter cotangent array of cdd_step_adjoint. */
+#define CDD_PBAR 9
+
+/* Reverse of the step recorded in rec (taken at time t with the fixed dt): ubar holds the
+ * cotangent of the step's output on entry and that of its input u on return (packed field):
+ *   F1b = 2/3 ubar + 2/3 dt L_{F1}^T ubar,  F0b = 1/4 F1b + 1/4 dt L_{F0}^T F1b,
+ *   ubar <- 1/3 ubar + 3/4 F1b + F0b + dt L_u^T F0b,
+ * L_v^T the flux VJP of cdd_flux_vjp at v (recorded limiter selections and speed-max corners).
+ * pbar (device, CDD_PBAR doubles per instance, may be NULL): parameter cotangents of the three
+ * stages are added: [0] sum <sigbar, sigma_int> (d/d mu = [0] / mu), [1] sum tr(sigbar) tr(sigma_int)
+ * (d/d nu through lambda = [1] * dlambda/dnu / (2 mu + 3 lambda)), [2] the k-space part of d/d nu
+ * per unit d(lambda / (lambda + 2 mu))/dnu, [3..5] the diagonal of sigbar summed over cells (the
+ * applied-load cotangent), [6..8] the same times (t - load_t0). Each stage's terms carry its
+ * weight (2/3 dt, 1/4 dt, dt). No host synchronisation. */
+int cdd_step_adjoint(cdd_plan* plan, const void* rec, double t, double dt, void* ubar, double* pbar,
+                     void* stream);
+
 /* Device status flags accumulated by kernels (CDD_ERR_NONFINITE, ...); clears them. */
 int cdd_check_status(cdd_plan* plan);
 

@@ -197,3 +197,51 @@ def test_autograd_function_fp32_rollout():
     g64, grads = ro.backward()
     assert rel(b0.grad, g64) < 1e-4
     assert abs(float(mu.grad) - grads["mu"]) <= 1e-4 * abs(grads["mu"])
+
+
+def test_step_record_matches_fixed_step_bitwise():
+    shape = (10, 24, 64)                      # TMA-staged planes in FP32 and FP64
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 7)
+    for prec in ("f64", "f32"):
+        plan = cdd.Plan([cdd.Instance(shape, mu=1.2, nu=0.27, load_rate=tuple(0.04 * CZZ))], prec)
+        a = plan.pack([b0])
+        b = a.clone()
+        c = a.clone()
+        plan.set_time(0.3, 1e300)
+        plan.step_fixed(a, 1e-3)
+        _lib.check(plan.lib.cdd_step_record(plan.handle, P(b), 0.3, 1e-3, None, _stream()))
+        n = int(plan.lib.cdd_plan_record_elems(plan.handle))
+        raw = torch.empty(n + 64, dtype=plan.dtype, device=plan.device)
+        off = (-raw.data_ptr() % 256) // raw.element_size()
+        rec = raw[off:off + n]
+        _lib.check(plan.lib.cdd_step_record(plan.handle, P(c), 0.3, 1e-3, P(rec), _stream()))
+        assert torch.equal(a, b) and torch.equal(a, c), prec
+        assert torch.equal(rec[:plan.field_elems], plan.pack([b0]))   # the record starts with u
+
+
+def test_batched_step_adjoint_matches_single_instances():
+    """cdd_step_adjoint on a plan of two instances (different grids, materials and loads) equals
+    the single-instance results, parameter cotangents per instance included."""
+    specs = [((12, 16, 20), 1.0, 0.3, 0.05), ((16, 24), 1.3, 0.25, None)]
+    fields = [cdd.gaussian_random_field(s, 0.06, 0.05, 10 + i) for i, (s, *_r) in enumerate(specs)]
+    insts = [cdd.Instance(s, mu=m, nu=v, load_rate=None if r is None else tuple(r * CZZ)) for s, m, v, r in specs]
+
+    def run(plan, arrays, seeds):
+        u = plan.pack(arrays)
+        n = int(plan.lib.cdd_plan_record_elems(plan.handle))
+        raw = torch.empty(n + 64, dtype=plan.dtype, device=plan.device)
+        off = (-raw.data_ptr() % 256) // raw.element_size()
+        rec = raw[off:off + n]
+        _lib.check(plan.lib.cdd_step_record(plan.handle, P(u), 0.2, 2e-3, P(rec), _stream()))
+        ub = plan.pack(seeds)
+        pbar = torch.zeros(_lib.CDD_PBAR * len(arrays), dtype=torch.float64, device=plan.device)
+        _lib.check(plan.lib.cdd_step_adjoint(plan.handle, P(rec), 0.2, 2e-3, P(ub), P(pbar), _stream()))
+        return [plan.field_view(ub, i).clone() for i in range(len(arrays))], pbar.view(len(arrays), -1)
+
+    rng = np.random.default_rng(3)
+    seeds = [rng.standard_normal((9,) + s) for s, *_r in specs]
+    both, pb = run(cdd.Plan(insts, "f64"), fields, seeds)
+    for i in range(2):
+        one, pb1 = run(cdd.Plan([insts[i]], "f64"), [fields[i]], [seeds[i]])
+        assert rel(both[i], one[0]) < 1e-13
+        assert torch.allclose(pb[i], pb1[0], rtol=1e-12, atol=1e-14)
