@@ -41,7 +41,95 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=64, help="grid of the CPU baseline sample")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
+
+
+def ensemble_instances(seed):
+    """The 96-instance ensemble: 16 each of 256^2, 512^2, 48^3, 64^3, 96^3, 128^3 (58,916,864 cells
+    per stage); sigma ~ U[0.02, 0.08] L, traceless strain rate with rate_zz ~ U[0, 0.1]."""
+    import numpy as np
+    import cdd
+    rng = np.random.default_rng(seed)
+    shapes = [(256, 256), (512, 512), (48, 48, 48), (64, 64, 64), (96, 96, 96), (128, 128, 128)]
+    out = []
+    for sh in shapes:
+        for _ in range(16):
+            sig = float(rng.uniform(0.02, 0.08))
+            r = float(rng.uniform(0.0, 0.1))
+            out.append((sh, sig, int(rng.integers(1 << 30)),
+                        cdd.Instance(sh, mu=1.0, nu=0.3, cfl=0.25, load_rate=(-0.5 * r, -0.5 * r, r))))
+    return out
+
+
+def run_ensemble(dev, K, W, seed):
+    """Batched FP32 ensemble through one plan: every stage is one launch per kernel over all
+    instances, per-instance dt, the whole step in a CUDA graph."""
+    import torch
+    import cdd
+    from cdd.initial import gaussian_random_field_torch
+    spec = ensemble_instances(seed)
+    plan = cdd.Plan([s[3] for s in spec], "f32")
+    beta = plan.empty_field()
+    for i, (sh, sig, sd, _inst) in enumerate(spec):
+        plan.field_view(beta, i).copy_(gaussian_random_field_torch(sh, sig, 0.05, sd, device=dev))
+    plan.set_time(0.0, 1e30)
+    plan.run(beta, W, graph=True)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    plan.run(beta, K, graph=True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    plan.check_status()
+    t, dt, act = plan.get_time()
+    cells = plan.total_cells
+    return {"value": cells * 3 * K / el, "unit": UNIT, "ms_per_step": 1e3 * el / K, "steps": K,
+            "instances": len(spec), "cells_per_stage": cells, "dtype": "f32",
+            "dt_range": [float(dt.min()), float(dt.max())],
+            "workload": "96 instances: 16 each of 256^2, 512^2, 48^3, 64^3, 96^3, 128^3; sigma U[0.02,0.08] L, "
+                        "rate_zz U[0,0.1] traceless; one plan, one CUDA graph per step"}
+
+
+def run_adjoint(dev, seed):
+    """Adjoint cost: 64^3 FP32, 200 fixed-dt steps (dt from the step-0 CFL 0.25), checkpoints every
+    20 steps; loss = elastic energy + 10 mean beta_zz; gradients for beta0, mu, nu, rate_zz.
+    adj/fwd = reverse-sweep time (segment re-runs included) / forward time."""
+    import torch
+    import cdd
+    from cdd.adjoint import Rollout, CZZ
+    from cdd.initial import gaussian_random_field_torch
+    shape = (64, 64, 64)
+    b0 = gaussian_random_field_torch(shape, 0.05, 0.05, seed, device=dev)
+    probe = cdd.Plan([cdd.Instance(shape, load_rate=tuple(0.05 * CZZ))], "f32")
+    bp = probe.pack([b0])
+    _, speed = probe.flux(bp, 0.0)
+    dt = 0.25 / (64 * float(speed.max()))
+    del probe, bp
+    n = 200
+    ro = Rollout(shape, 1.0, 0.3, 0.05, dt, n, precision="f32", checkpoint_every=20)
+    beta = ro.plan.pack([b0])
+    ro.forward(beta)
+    ro.backward()                      # warm-up (allocations, attributes)
+    st = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    _, loss = ro.forward(beta)
+    ev[1].record(st)
+    _, grads = ro.backward()
+    ev[2].record(st)
+    torch.cuda.synchronize()
+    f = ev[0].elapsed_time(ev[1]) / 1e3
+    b = ev[1].elapsed_time(ev[2]) / 1e3
+    return {"value": b / f, "fwd_ms_per_step": 1e3 * f / n, "adj_ms_per_step": 1e3 * b / n,
+            "steps": n, "checkpoint_every": 20, "grid": list(shape), "dtype": "f32", "loss": loss,
+            "grads": {k: float(v) for k, v in grads.items()},
+            "workload": "64^3 FP32 rollout, 200 fixed-dt steps, checkpoints every 20; reverse sweep = "
+                        "segment re-run with step records + cdd_step_adjoint per step"}
 
 
 def workload(size, seed):
@@ -320,6 +408,13 @@ def main():
            "path": "cdd.Plan.step on a field copied in from pinned host memory and copied back every step"}
     clk = clocks.stop()
 
+    adj = None
+    ens = None
+    if world == 1 and not args.no_adjoint:
+        adj = run_adjoint(dev, 5)
+    if world == 1 and not args.no_ensemble:
+        ens = run_ensemble(dev, max(3, min(K, 5)), W, 2024)
+
     if world > 1:
         dist.barrier()
         del p32
@@ -356,7 +451,9 @@ def main():
         "fp64_plain": fp64,
         "fp32_over_fp64": (rate32 / fp64["value"]) if fp64 else None,
         "fp32_error_10_steps": err,
-        "adj_over_fwd": None,
+        "adj_over_fwd": adj["value"] if adj else None,
+        "adjoint": adj,
+        "ensemble_96": ens,
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_sample)
