@@ -12,20 +12,47 @@ constexpr int MAX_STAGES = 12;
 #define CDD_MAX_TMA_INSTANCES 16
 constexpr double ME = 2.220446049250313080847263336181640625e-16;   // DBL_EPSILON
 
+// Exact division by an invariant divisor d >= 1 for 0 <= n < 2^31 with one wide multiply and a
+// shift (Granlund & Montgomery 1994, round-up multiplier): l = ceil(log2 d),
+// M = ceil(2^(32 + l) / d) < 2^33, floor(n / d) = (n * M) >> (32 + l); n * M < 2^64 and
+// M d - 2^(32 + l) < d <= 2^l make it exact.
+struct FDiv {
+    unsigned long long M;
+    int l;
+    int d;
+};
+
+inline FDiv fdiv_make(int d) {
+    FDiv f;
+    f.d = d;
+    f.l = 0;
+    while ((1LL << f.l) < (long long)d) ++f.l;
+    const unsigned long long num = 1ULL << (32 + f.l);
+    f.M = num / (unsigned long long)d + ((num % (unsigned long long)d) ? 1ULL : 0ULL);
+    return f;
+}
+
+__host__ __device__ __forceinline__ int fdiv_q(const FDiv& f, int n) {
+    return (int)(((unsigned long long)(unsigned)n * f.M) >> (32 + f.l));
+}
+
 // One-dimensional FFT of length n as a sequence of Stockham stages of radix 2, 3, 4, 5, 8, 16.
 struct LinePlan {
     int n;
     int nst;
     int radix[MAX_STAGES];
     int tw;   // offset (complex elements) of this length's twiddle table w_n^k, k < n
+    FDiv nr[MAX_STAGES];   // stage st: butterflies per line n / radix[st]
+    FDiv ns[MAX_STAGES];   // stage st: span of the finished sub-transforms (product of earlier radices)
 };
 
 // Per-pass tiling of one instance (host-chosen, read by the kernels).
 struct PassTile {
     int blocks;    // blocks this instance contributes to the launch
-    int lines;     // rows kernel: line pairs per block; strided kernels: columns per block (W)
+    int lines;     // rows kernel: line pairs per block; strided kernels: columns per block (W, a power of 2)
     int threads;   // threads this instance needs (<= launch blockDim)
     int tiles_a;   // strided kernels: number of column tiles along the row
+    int lgw;       // strided kernels: log2(lines)
 };
 
 enum Pass { PASS_R2C = 0, PASS_MID_F, PASS_GREEN, PASS_MID_I, PASS_C2R, NUM_PASSES };
@@ -37,6 +64,8 @@ struct InstDev {
     int nl;                 // length of the contiguous (last) axis
     int nh;                 // nl / 2 + 1
     int nhp;                // padded spectrum row length (complex elements)
+    FDiv fd_nl, fd_nh;      // division by nl and nh
+    FDiv fd_rows;           // division by rows (component of a packed row index)
     int rows;               // real rows per component (cells / nl)
     long long cells;
     long long foff;         // offset of the packed 9-component field
@@ -221,32 +250,46 @@ __device__ __forceinline__ int row_pad(int a) { return a + (a >> 4); }
 struct RowLayout {   // lines are rows of length n, padded every 16 elements
     int lines, ld;
     __device__ __forceinline__ int addr(int l, int i) const { return l * ld + row_pad(i); }
-    static constexpr bool line_fast = false;
+    // butterfly g -> (line, butterfly index within the line): consecutive g walk one line
+    __device__ __forceinline__ void split(int g, const FDiv& nr, int& l, int& j) const {
+        l = fdiv_q(nr, g);
+        j = g - l * nr.d;
+    }
 };
 
-struct ColLayout {   // element i of line l = (c, w) at (c * cs) + i * w_count + w
-    int lines, wcount, cs;
+// K groups of 2^lgw columns: element i of line l = (c, w) at c * cs + (i << lgw) + w; consecutive
+// butterflies walk the lines (columns) so that neighbouring threads touch neighbouring words.
+template <int K>
+struct ColLayout {
+    int lgw, cs;
+    __device__ __forceinline__ int lines() const { return K << lgw; }
     __device__ __forceinline__ int addr(int l, int i) const {
-        int c = l / wcount;
-        int w = l - c * wcount;
-        return c * cs + i * wcount + w;
+        const int c = (K == 1) ? 0 : (l >> lgw);
+        const int w = l & ((1 << lgw) - 1);
+        return c * cs + (i << lgw) + w;
     }
-    static constexpr bool line_fast = true;
+    __device__ __forceinline__ void split(int g, const FDiv&, int& l, int& j) const {
+        j = (K == 1) ? (g >> lgw) : (g >> lgw) / K;
+        l = g - j * (K << lgw);
+    }
 };
+
+template <typename Lay> __device__ __forceinline__ int lay_lines(const Lay& lay) { return lay.lines; }
+template <int K> __device__ __forceinline__ int lay_lines(const ColLayout<K>& lay) { return lay.lines(); }
 
 template <int R, typename V, bool INV, typename Lay>
 __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restrict__ dst,
-                                          const Lay& lay, int n, int ns,
+                                          const Lay& lay, const FDiv& fnr, const FDiv& fns,
                                           const V* __restrict__ tw, int tid, int nt) {
-    const int nr = n / R;
-    const int twstep = n / (ns * R);
-    const int total = lay.lines * nr;
+    const int nr = fnr.d;
+    const int ns = fns.d;
+    const int twstep = fdiv_q(fns, nr);     // n / (ns R)
+    const int total = lay_lines(lay) * nr;
 #pragma unroll 1
     for (int g = tid; g < total; g += nt) {
         int l, j;
-        if (Lay::line_fast) { l = g % lay.lines; j = g / lay.lines; }
-        else { j = g % nr; l = g / nr; }
-        const int jm = j % ns;
+        lay.split(g, fnr, l, j);
+        const int jm = j - fdiv_q(fns, j) * ns;
         V v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -271,22 +314,21 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
 template <typename V, bool INV, typename Lay>
 __device__ __forceinline__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
                         int tid, int nt) {
-    const int n = lp.n;
     const V* tw = twbase + lp.tw;
-    int ns = 1;
     V* src = a;
     V* dst = b;
     for (int st = 0; st < lp.nst; ++st) {
         const int R = lp.radix[st];
+        const FDiv& fnr = lp.nr[st];
+        const FDiv& fns = lp.ns[st];
         switch (R) {
-            case 2: fft_stage<2, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
-            case 3: fft_stage<3, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
-            case 4: fft_stage<4, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
-            case 5: fft_stage<5, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
-            case 8: fft_stage<8, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
-            default: fft_stage<16, V, INV>(src, dst, lay, n, ns, tw, tid, nt); break;
+            case 2: fft_stage<2, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
+            case 3: fft_stage<3, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
+            case 4: fft_stage<4, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
+            case 5: fft_stage<5, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
+            case 8: fft_stage<8, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
+            default: fft_stage<16, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
         }
-        ns *= R;
         V* t = src; src = dst; dst = t;
     }
     return src;

@@ -69,7 +69,13 @@ bool na_line_plan(int n, LinePlan& lp) {
     for (int i = 0; i < c; ++i) r.push_back(5);
     if ((int)r.size() > MAX_STAGES) return false;
     lp.nst = (int)r.size();
-    for (int i = 0; i < lp.nst; ++i) lp.radix[i] = r[i];
+    int ns = 1;
+    for (int i = 0; i < lp.nst; ++i) {
+        lp.radix[i] = r[i];
+        lp.nr[i] = fdiv_make(n / r[i]);
+        lp.ns[i] = fdiv_make(ns);
+        ns *= r[i];
+    }
     return true;
 }
 
@@ -131,8 +137,11 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     I.nl = (I.nd == 3) ? I.n2 : I.n1;
     I.nh = I.nl / 2 + 1;
     I.nhp = (I.nh + 7) & ~7;
+    I.fd_nl = fdiv_make(I.nl);
+    I.fd_nh = fdiv_make(I.nh);
     I.cells = (long long)I.n0 * I.n1 * I.n2;
     I.rows = (int)(I.cells / I.nl);
+    I.fd_rows = fdiv_make(I.rows);
     I.mu = d->mu;
     I.nu = d->nu;
     I.lamb = 2. * d->mu * d->nu / (1. - 2. * d->nu);
@@ -202,6 +211,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         int W = (int)(128 / velt);
         while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
         t.lines = W;
+        while ((1 << t.lgw) < W) ++t.lgw;
         t.threads = 256;
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = comps * I.n0 * t.tiles_a;
@@ -214,6 +224,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
             return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: axis-0 length too large for the k-space pass");
         t.lines = W;
+        while ((1 << t.lgw) < W) ++t.lgw;
         t.threads = 256;
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;

@@ -62,7 +62,13 @@ bool make_line_plan(int n, LinePlan& lp) {
     for (int i = 0; i < c; ++i) r.push_back(5);
     if ((int)r.size() > MAX_STAGES) return false;
     lp.nst = (int)r.size();
-    for (int i = 0; i < lp.nst; ++i) lp.radix[i] = r[i];
+    int ns = 1;
+    for (int i = 0; i < lp.nst; ++i) {
+        lp.radix[i] = r[i];
+        lp.nr[i] = fdiv_make(n / r[i]);
+        lp.ns[i] = fdiv_make(ns);
+        ns *= r[i];
+    }
     return true;
 }
 
@@ -183,6 +189,8 @@ int build_shapes(cdd_plan* p, size_t elt) {
             int W = (int)(128 / velt);
             while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
             t.lines = W;
+            t.lgw = 0;
+            while ((1 << t.lgw) < W) ++t.lgw;
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = comps * I.n0 * t.tiles_a;
@@ -198,6 +206,8 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
                 return fail(CDD_ERR_SHAPE, "axis-0 length %d too large for the fused k-space pass", I.n0);
             t.lines = W;
+            t.lgw = 0;
+            while ((1 << t.lgw) < W) ++t.lgw;
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
@@ -354,8 +364,11 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
         I.nl = (I.nd == 3) ? I.n2 : I.n1;
         I.nh = I.nl / 2 + 1;
         I.nhp = (I.nh + 7) & ~7;
+        I.fd_nl = fdiv_make(I.nl);
+        I.fd_nh = fdiv_make(I.nh);
         I.cells = (long long)I.n0 * I.n1 * I.n2;
         I.rows = (int)(I.cells / I.nl);
+        I.fd_rows = fdiv_make(I.rows);
         I.foff = foff; foff += 9 * I.cells;
         I.soff = soff; soff += 6 * I.cells;
         I.coff = coff; coff += I.cells;

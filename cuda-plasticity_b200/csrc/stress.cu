@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
 #pragma unroll 4
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
             const int i = i4 << 2;
-            const int pl = i / N, idx = i - pl * N;
+            const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
             const long long p = (long long)lb * P + pl;
             T a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
             if (p < npairs) {
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     } else {
 #pragma unroll 4
         for (int i = tid; i < P * N; i += nt) {
-            int pl = i / N, idx = i - pl * N;
+            int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
             long long p = (long long)lb * P + pl;
             V z; z.x = 0; z.y = 0;
             if (p < npairs) {
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const int nh = I.nh;
     V* dst = spec + I.spoff;
     for (int i = tid; i < P * nh; i += nt) {
-        int pl = i / nh, k = i - pl * nh;
+        int pl = fdiv_q(I.fd_nh, i), k = i - pl * nh;
         long long p = (long long)lb * P + pl;
         if (p >= npairs) continue;
         V zk = s[pl * ld + row_pad(k)];
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
 
 #pragma unroll 4
     for (int i = tid; i < P * nh; i += nt) {
-        int pl = i / nh, k = i - pl * nh;
+        int pl = fdiv_q(I.fd_nh, i), k = i - pl * nh;
         long long p = (long long)lb * P + pl;
         V A, B;
         A.x = A.y = B.x = B.y = 0;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
 #pragma unroll 2
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
             const int i = i4 << 2;
-            const int pl = i / N, idx = i - pl * N;
+            const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
             const long long p = (long long)lb * P + pl;
             if (p >= npairs) continue;
             const long long ra = 2 * p;
@@ -212,8 +212,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
 #pragma unroll
             for (int q = 0; q < 4; ++q) { V z = sr[q]; va[q] = z.x; vb[q] = z.y; }
             if (MEAN64) {
-                const T ma = (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
-                const T mb = (ra + 1 < nrows) ? (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows)) : (T)0;
+                const T ma = (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
+                const T mb = (ra + 1 < nrows) ? (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)(ra + 1))) : (T)0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) { va[q] += ma; vb[q] += mb; }
             }
@@ -222,15 +222,15 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
         }
     } else {
         for (int i = tid; i < P * N; i += nt) {
-            int pl = i / N, idx = i - pl * N;
+            int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
             long long p = (long long)lb * P + pl;
             if (p >= npairs) continue;
             V z = s[pl * ld + row_pad(idx)];
             long long ra = 2 * p;
             T va = z.x, vb = z.y;
             if (MEAN64) {
-                va += (T)mean_stress(I, sbar + 9 * ii, (int)(ra / I.rows));
-                if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, (int)((ra + 1) / I.rows));
+                va += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
+                if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)(ra + 1)));
             }
             dst[ra * N + idx] = va;
             if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const InstDev& I = insts[ii];
     int lb = blockIdx.x - pre[ii];
     const PassTile& tl = I.tile[pass];
-    const int W = tl.lines, ta_n = tl.tiles_a;
+    const int W = tl.lines, lgw = tl.lgw, ta_n = tl.tiles_a;
     const int ta = lb % ta_n; lb /= ta_n;
     const int i0 = lb % I.n0;
     const int c = lb / I.n0;
@@ -266,16 +266,17 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
 #pragma unroll 4
     for (int i = tid; i < N * W; i += nt) {
-        int e = i / W, w = i - e * W;
+        const int e = i >> lgw, w = i & (W - 1);
         V z; z.x = 0; z.y = 0;
         if (w < wv) z = base[(long long)e * nhp + w];
         s[i] = z;
     }
     __syncthreads();
-    ColLayout lay{W, W, 0};
+    ColLayout<1> lay{lgw, 0};
     s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tw, tid, nt);
+#pragma unroll 4
     for (int i = tid; i < N * W; i += nt) {
-        int e = i / W, w = i - e * W;
+        const int e = i >> lgw, w = i & (W - 1);
         if (w < wv) base[(long long)e * nhp + w] = s[i];
     }
 }
@@ -457,11 +458,11 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
 // are the ping-pong scratch. The transforms run three components at a time against the scratch;
 // when the stage count is odd the result is copied back to the component slots.
 template <typename V, bool INV>
-__device__ __forceinline__ void fft_group3(V* s, int g, int N, int W, int cs, const LinePlan& lp,
+__device__ __forceinline__ void fft_group3(V* s, int g, int lgw, int cs, const LinePlan& lp,
                                            const V* __restrict__ tw, int tid, int nt) {
     V* a = s + 3 * g * cs;
     V* b = s + 9 * cs;
-    ColLayout lay{3 * W, W, cs};
+    ColLayout<3> lay{lgw, cs};
     V* r = fft_lines<V, INV>(a, b, lay, lp, tw, tid, nt);
     if (r != a) {
         for (int i = tid; i < 3 * cs; i += nt) a[i] = b[i];
@@ -476,7 +477,7 @@ __device__ __forceinline__ void fft_group3(V* s, int g, int N, int W, int cs, co
 // the Nyquist half-axis column, 2 elsewhere): the A/B part of <sigbar, (d sigma / d nu) beta>
 // per unit dA.
 template <typename T, bool MEAN64, int GMODE>
-__global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green(const InstDev* __restrict__ insts, int n_inst,
                                                          const int* __restrict__ pre,
                                                          typename VecOf<T>::type* __restrict__ spec,
                                                          const typename VecOf<T>::type* __restrict__ tw,
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
     const InstDev& I = insts[ii];
     int lb = blockIdx.x - pre[ii];
     const PassTile& tl = I.tile[PASS_GREEN];
-    const int W = tl.lines, ta_n = tl.tiles_a;
+    const int W = tl.lines, lgw = tl.lgw, ta_n = tl.tiles_a;
     const int ta = lb % ta_n;
     const int i1 = lb / ta_n;          // 0 in 2-D
     const int N = I.n0, nhp = I.nhp, nh = I.nh;
@@ -504,17 +505,18 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
 
     constexpr int NIN = (GMODE == 1) ? 6 : 9;     // components in / out of the k-space pass
     constexpr int NOUT = (GMODE == 1) ? 9 : 6;
+#pragma unroll 1
+    for (int c = 0; c < NIN; ++c) {
 #pragma unroll 4
-    for (int i = tid; i < NIN * N * W; i += nt) {
-        int c = i / (N * W);
-        int rem = i - c * N * W;
-        int e = rem / W, w = rem - e * W;
-        V z; z.x = 0; z.y = 0;
-        if (w < wv) z = base[c * cstride + e * estride + w];
-        s[c * cs + rem] = z;
+        for (int rem = tid; rem < N * W; rem += nt) {
+            const int e = rem >> lgw, w = rem & (W - 1);
+            V z; z.x = 0; z.y = 0;
+            if (w < wv) z = base[c * cstride + e * estride + w];
+            s[c * cs + rem] = z;
+        }
     }
     __syncthreads();
-    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tw, tid, nt);
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -523,7 +525,7 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
     V* phib = phi ? phi + I.spoff / 9 + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0 : nullptr;
     double pacc = 0.0;
     for (int i = tid; i < N * W; i += nt) {
-        int e = i / W, w = i - e * W;
+        const int e = i >> lgw, w = i & (W - 1);
         int kh = col0 + w;
         if (w >= wv) continue;
         T kx, ky, kz;
@@ -583,13 +585,14 @@ __global__ void __launch_bounds__(GREEN_THREADS) k_green(const InstDev* __restri
         }
     }
     __syncthreads();
-    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, N, W, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tw, tid, nt);
+#pragma unroll 1
+    for (int c = 0; c < NOUT; ++c) {
 #pragma unroll 4
-    for (int i = tid; i < NOUT * N * W; i += nt) {
-        int c = i / (N * W);
-        int rem = i - c * N * W;
-        int e = rem / W, w = rem - e * W;
-        if (w < wv) base[c * cstride + e * estride + w] = s[c * cs + rem];
+        for (int rem = tid; rem < N * W; rem += nt) {
+            const int e = rem >> lgw, w = rem & (W - 1);
+            if (w < wv) base[c * cstride + e * estride + w] = s[c * cs + rem];
+        }
     }
 }
 
@@ -700,21 +703,34 @@ cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cuda
     return run_stress<double>(P, beta, sigma, phi, st);
 }
 
+// Raise a kernel's dynamic shared-memory limit to smem, clamped to what the device allows next to
+// the kernel's own static shared memory.
+template <typename F>
+static cudaError_t set_dyn_smem(F* fn, size_t smem) {
+    int dev = 0, optin = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, fn))) return e;
+    const long long lim = (long long)optin - (long long)fa.sharedSizeBytes;
+    const long long v = (long long)smem < lim ? (long long)smem : lim;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v);
+}
+
 template <typename T>
 static cudaError_t set_attr_t(size_t smem) {
     cudaError_t e;
-    int v = (int)smem;
-    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, true>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_r2c_rows<T, false>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, true>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_c2r_rows<T, false>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_fft_mid<T, true>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_fft_mid<T, false>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, true, 0>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, false, 0>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, false, 1>, A, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_green<T, false, 2>, A, v))) return e;
+    if ((e = set_dyn_smem(k_r2c_rows<T, true>, smem))) return e;
+    if ((e = set_dyn_smem(k_r2c_rows<T, false>, smem))) return e;
+    if ((e = set_dyn_smem(k_c2r_rows<T, true>, smem))) return e;
+    if ((e = set_dyn_smem(k_c2r_rows<T, false>, smem))) return e;
+    if ((e = set_dyn_smem(k_fft_mid<T, true>, smem))) return e;
+    if ((e = set_dyn_smem(k_fft_mid<T, false>, smem))) return e;
+    if ((e = set_dyn_smem(k_green<T, true, 0>, smem))) return e;
+    if ((e = set_dyn_smem(k_green<T, false, 0>, smem))) return e;
+    if ((e = set_dyn_smem(k_green<T, false, 1>, smem))) return e;
+    if ((e = set_dyn_smem(k_green<T, false, 2>, smem))) return e;
     return cudaSuccess;
 }
 
