@@ -737,7 +737,7 @@ cudaError_t launch_vjp_stage(const PlanCore& P, const void* v, const void* sig_v
     if ((e = launch_stress_adjoint(P, P.d_sb6, P.d_adj9, st, pbar ? phi_v : nullptr, pbar ? P.d_gpart : nullptr)))
         return e;
     if (pbar) {
-        k_param_reduce<<<P.n_inst, 256, 0, st>>>(P.d_inst, V.d_pre, P.d_bload, P.adj[PASS_GREEN].d_pre,
+        k_param_reduce<<<P.n_inst, 256, 0, st>>>(P.d_inst, V.d_pre, P.d_bload, P.pass[PASS_GREEN].d_pre,
                                                  phi_v ? P.d_gpart : nullptr, c, t, pbar);
         if ((e = cudaGetLastError())) return e;
     }

@@ -375,7 +375,6 @@ struct PlanCore {
     double* d_obs = nullptr;         // per-instance energy, mean zz (2 per instance)
     int* d_status = nullptr;
     LaunchShape pass[NUM_PASSES];
-    LaunchShape adj[NUM_PASSES];     // adjoint stress pipeline: 6 components in, 9 out
     LaunchShape stencil;
     LaunchShape cellwise;            // elementwise kernels over cells
     LaunchShape obs;                 // observables: one thread per cell

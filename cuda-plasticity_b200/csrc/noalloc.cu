@@ -189,7 +189,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     size_t smem_need = 48 * 1024;
     int blocks[NUM_PASSES] = {0, 0, 0, 0, 0};
     for (int k : {PASS_R2C, PASS_C2R}) {
-        const int comps = (k == PASS_R2C) ? 9 : 6;
+        const int comps = 6;
         long long npairs = ((long long)comps * I.rows + 1) / 2;
         const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
         int Pl = (velt == 8 ? 4096 : 2048) / I.nl;
@@ -207,7 +207,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         PassTile& t = I.tile[k];
         P.pass[k].threads = 256;
         if (I.nd != 3) continue;
-        const int comps = (k == PASS_MID_F) ? 9 : 6;
+        const int comps = 6;
         int W = (int)(128 / velt);
         while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
         t.lines = W;
@@ -220,8 +220,8 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     {
         PassTile& t = I.tile[PASS_GREEN];
         int W = (int)(32 / velt);
-        while (W > 1 && (size_t)12 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
-        if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
+        while (W > 1 && (size_t)9 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
+        if ((size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
             return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: axis-0 length too large for the k-space pass");
         t.lines = W;
         while ((1 << t.lgw) < W) ++t.lgw;
@@ -229,7 +229,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
         P.pass[PASS_GREEN].threads = 256;
-        P.pass[PASS_GREEN].smem = (size_t)12 * (I.n0 * W + W) * velt;
+        P.pass[PASS_GREEN].smem = (size_t)9 * (I.n0 * W + W) * velt;
     }
     for (int k = 0; k < NUM_PASSES; ++k) {
         blocks[k] = I.tile[k].blocks;

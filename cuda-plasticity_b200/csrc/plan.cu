@@ -165,8 +165,9 @@ int build_shapes(cdd_plan* p, size_t elt) {
     for (int i = 0; i < n; ++i) {
         InstDev& I = p->inst[i];
         // rows kernels (R2C: 9 components, C2R: 6); ping-pong buffers of P padded rows
+        // the transforms carry the 6 components of sym(beta) (forward) or of the stress cotangent
         for (int k : {PASS_R2C, PASS_C2R}) {
-            const int comps = (k == PASS_R2C) ? 9 : 6;
+            const int comps = 6;
             long long npairs = ((long long)comps * I.rows + 1) / 2;
             const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
             int P = (velt == 8 ? 4096 : 2048) / I.nl;   // radix-16 stages: one butterfly per thread
@@ -185,7 +186,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
         for (int k : {PASS_MID_F, PASS_MID_I}) {
             PassTile& t = I.tile[k];
             if (I.nd != 3) { t.blocks = 0; t.lines = t.threads = t.tiles_a = 0; continue; }
-            const int comps = (k == PASS_MID_F) ? 9 : 6;
+            const int comps = 6;
             int W = (int)(128 / velt);
             while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
             t.lines = W;
@@ -198,12 +199,12 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;
         }
-        // fused Green pass along axis 0: 9 components x W columns, ping-pong
+        // fused Green pass along axis 0: 6 component slots + 3 scratch slots of W columns
         {
             PassTile& t = I.tile[PASS_GREEN];
             int W = (int)(32 / velt);   // 32-byte row segments
-            while (W > 1 && (size_t)12 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
-            if ((size_t)12 * (I.n0 * W + W) * velt > 220 * 1024)
+            while (W > 1 && (size_t)9 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
+            if ((size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
                 return fail(CDD_ERR_SHAPE, "axis-0 length %d too large for the fused k-space pass", I.n0);
             t.lines = W;
             t.lgw = 0;
@@ -211,7 +212,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
-            size_t sm = (size_t)12 * (I.n0 * W + W) * velt;
+            size_t sm = (size_t)9 * (I.n0 * W + W) * velt;
             if (sm > smem_max[PASS_GREEN]) smem_max[PASS_GREEN] = sm;
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }
@@ -223,28 +224,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
         pre_ob.push_back(pre_ob.back() + (int)((I.cells + 255) / 256));
         pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));
     }
-    // adjoint stress pipeline: 6 components through R2C and the forward axis-1 pass, 9 after
-    std::vector<int> apre[NUM_PASSES];
-    for (int k = 0; k < NUM_PASSES; ++k) apre[k].push_back(0);
-    for (int i = 0; i < n; ++i) {
-        const InstDev& I = p->inst[i];
-        int b[NUM_PASSES];
-        b[PASS_R2C] = (int)((((long long)6 * I.rows + 1) / 2 + I.tile[PASS_R2C].lines - 1) / I.tile[PASS_R2C].lines);
-        b[PASS_C2R] = (int)((((long long)9 * I.rows + 1) / 2 + I.tile[PASS_C2R].lines - 1) / I.tile[PASS_C2R].lines);
-        b[PASS_MID_F] = (I.nd == 3) ? 6 * I.n0 * I.tile[PASS_MID_F].tiles_a : 0;
-        b[PASS_MID_I] = (I.nd == 3) ? 9 * I.n0 * I.tile[PASS_MID_I].tiles_a : 0;
-        b[PASS_GREEN] = I.tile[PASS_GREEN].blocks;
-        for (int k = 0; k < NUM_PASSES; ++k) apre[k].push_back(apre[k].back() + b[k]);
-    }
     size_t smem_all = 0;
-    for (int k = 0; k < NUM_PASSES; ++k) {
-        LaunchShape& A = C.adj[k];
-        A.blocks = apre[k].back();
-        A.threads = (k == PASS_R2C || k == PASS_C2R) ? (velt == 8 ? 256 : 128) : 256;
-        A.smem = smem_max[k];
-        CDD_CUDA(dalloc(p, (void**)&A.d_pre, sizeof(int) * (n + 1)));
-        CDD_CUDA(cudaMemcpy(A.d_pre, apre[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    }
     for (int k = 0; k < NUM_PASSES; ++k) {
         LaunchShape& L = C.pass[k];
         L.blocks = pre[k].back();
@@ -632,7 +612,7 @@ int ensure_adjoint_scratch(cdd_plan* p) {
         (e = dalloc(p, (void**)&C.d_bload, sizeof(double) * 5 * (size_t)C.vjp.blocks)) ||
         (e = dalloc(p, &C.d_adj9, elt * (size_t)C.field_elems)) ||
         (e = dalloc(p, &C.d_sb6, elt * (size_t)C.stress_elems)) ||
-        (e = dalloc(p, (void**)&C.d_gpart, sizeof(double) * (size_t)C.adj[PASS_GREEN].blocks)) ||
+        (e = dalloc(p, (void**)&C.d_gpart, sizeof(double) * (size_t)C.pass[PASS_GREEN].blocks)) ||
         (e = dalloc(p, &C.d_f0b, elt * (size_t)C.field_elems)) ||
         (e = dalloc(p, &C.d_f1b, elt * (size_t)C.field_elems)))
         return fail(CDD_ERR_ALLOC, "adjoint scratch: %s", cudaGetErrorString(e));

@@ -166,21 +166,51 @@ __device__ __forceinline__ void applied_load(const InstDev& I, double t, double*
     for (int i = 0; i < 3; ++i) add[i] = I.load_lamb * tr + 2.0 * I.load_mu * eps[i];
 }
 
-template <typename T, int ND, int MODE>
-__device__ __forceinline__ void stencil_cell(const InstDev& I, int ii, long long cl, bool valid,
-                                             const TileView<T, ND>& tv, const T* bn, T* out,
-                                             const T* __restrict__ sig, T* __restrict__ speed_out,
-                                             const InstClock* __restrict__ clk, double t_flux,
-                                             double& vmax, double& esum, double& zsum) {
-    const T ih = (T)I.inv_h, ih2 = (T)(I.inv_h * I.inv_h), hh = (T)(0.5 * I.h);
-    const long long cells = I.cells;
+// Per block constants of one stage: the applied-load stress (FP64) and, for the stage updates,
+// dt and whether the instance is still active.
+struct StageConst {
+    double ld[3];
+    double dt;
+    bool active;
+};
 
-    // total stress at the cell: internal + applied load (FP64), symmetric
+template <int MODE>
+__device__ __forceinline__ StageConst stage_const(const InstDev& I, const InstClock& ck, double t_flux) {
+    StageConst k;
     // load time: the step-start time in all three stages (FieldMover.py L62, L123, L133); stage 1
     // runs before the dt kernel advances t, stages 2 and 3 after it (t_stage holds the start).
-    const double tload = (MODE == M_FLUX) ? t_flux : ((MODE == M_STAGE1) ? clk[ii].t : clk[ii].t_stage);
-    double ld[3];
-    applied_load(I, tload, ld);
+    const double tload = (MODE == M_FLUX) ? t_flux : ((MODE == M_STAGE1) ? ck.t : ck.t_stage);
+    applied_load(I, tload, k.ld);
+    k.dt = ck.dt;
+    k.active = ck.active != 0;
+    return k;
+}
+
+template <typename T, int ND, int MODE>
+__device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, bool valid,
+                                             const TileView<T, ND>& tv, const T* bn, T* out,
+                                             const T* __restrict__ sig, T* __restrict__ speed_out,
+                                             const StageConst& kc_block, const InstClock& ck, double t_flux,
+                                             double& vmax, double& esum, double& zsum) {
+    const T ih = (T)I.inv_h;
+    const long long cells = I.cells;
+    // FP32 reads the block's stage constants from shared memory; FP64 (no registers to spare across
+    // the march) re-derives them per cell
+    StageConst kc_cell;
+    if constexpr (sizeof(T) == 8) kc_cell = stage_const<MODE>(I, ck, t_flux);
+    const StageConst& kc = (sizeof(T) == 8) ? kc_cell : kc_block;
+    // beta_n of the stage update: in FP32 issued first so that the loads overlap the flux
+    // computation (FP64 loads them at the end: no registers to spare)
+    constexpr bool UPD = (MODE == M_STAGE2 || MODE == M_STAGE3);
+    constexpr bool PRE = UPD && (sizeof(T) == 4);
+    T vn[UPD ? 9 : 1];
+    if constexpr (PRE) {
+        const T* un = bn + I.foff + cl;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) vn[c] = (valid && kc.active) ? un[c * cells] : (T)0;
+    }
+    const double* ld = kc.ld;
+    // total stress at the cell: internal + applied load (FP64), symmetric
     const T* sp = sig + I.soff + cl;
     T S[3][3];
     {
@@ -449,14 +479,15 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, int ii, long long
             esum += (sq - I.nu / (1.0 + I.nu) * tr * tr) / (4.0 * I.mu);
             zsum += (double)tv.center(8);
         }
-    } else {
-        if (valid && clk[ii].active) {
-            const T dt = (T)clk[ii].dt;
-            const T* un = bn + I.foff + cl;
+    } else if constexpr (UPD) {
+        if (valid && kc.active) {
+            const T dt = (T)kc.dt;
             T* o = out + I.foff + cl;
-            T vn[9];
+            if constexpr (!PRE) {
+                const T* un = bn + I.foff + cl;
 #pragma unroll
-            for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
+                for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
+            }
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 T vs = tv.center(c);
@@ -563,6 +594,8 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     } else {
         load_box(0, 0, true);
     }
+    __shared__ StageConst kc;   // FP32: read per cell from shared memory (keeps registers free)
+    if (sizeof(T) == 4 && tid == 0) kc = stage_const<MODE>(I, clk[ii], t_flux);
     __syncthreads();
     double vmax = 0.0, esum = 0.0, zsum = 0.0;
     TileView<T, ND> tv;
@@ -583,8 +616,8 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             tv.so[2] = 0;
         }
         const long long cl = ((long long)z * nY + y) * nX + x;
-        stencil_cell<T, ND, MODE>(I, ii, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, clk, t_flux,
-                                  vmax, esum, zsum);
+        stencil_cell<T, ND, MODE>(I, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, kc, clk[ii], t_flux, vmax,
+                                  esum, zsum);
         if (ND == 3 && more) {
             if (use_tma) {
                 if (NS == 5) {

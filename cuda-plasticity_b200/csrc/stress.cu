@@ -48,18 +48,43 @@ __device__ __forceinline__ void store4(double* p, const double* v) {
     reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }
 
-// Mean stress -lam tr<b> d_ij - mu (<b>_ij + <b>_ji) of symmetric component o (xx xy xz yy yz zz).
+// Symmetric component o = (SYM_I[o], SYM_J[o]): xx xy xz yy yz zz.
+__device__ __constant__ int SYM_I[6] = {0, 0, 0, 1, 1, 2};
+__device__ __constant__ int SYM_J[6] = {0, 1, 2, 1, 2, 2};
+
+// Mean stress -lam tr<s> d_ij - 2 mu <s>_ij of symmetric component o, from the means m of the six
+// components of s = sym(beta) (= -lam tr<b> d - mu (<b> + <b>^T)).
 __device__ __forceinline__ double mean_stress(const InstDev& I, const double* m, int o) {
-    const int ia[6] = {0, 0, 0, 1, 1, 2};
-    const int ja[6] = {0, 1, 2, 1, 2, 2};
-    const int i = ia[o], j = ja[o];
-    double v = -I.mu * (m[3 * i + j] + m[3 * j + i]);
-    if (i == j) v -= I.lamb * (m[0] + m[4] + m[8]);
+    double v = -2.0 * I.mu * m[o];
+    if (o == 0 || o == 3 || o == 5) v -= I.lamb * (m[0] + m[3] + m[5]);
     return v;
 }
 
+// The stress depends on beta only through its symmetric part s = (beta + beta^T) / 2 (every term of
+// the Green contraction and of sigma is symmetric in beta), so the transforms carry 6 components.
+// Source rows of the 6-component R2C input, row ra = component o * rows + r:
+//   RS_STRESS: row ra of a 6-component stress-layout array (p == q);
+//   RS_SYM:    rows of beta_ij and beta_ji (p == q on the diagonal).
+// The value is (p + q) / 2, exact when p == q.
+enum RowSource { RS_STRESS = 1, RS_SYM = 2 };
+
+template <typename T>
+__device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mode, long long ra, const T*& p,
+                                         const T*& q) {
+    if (mode == RS_STRESS) {
+        p = q = base + I.soff + ra * I.nl;
+        return;
+    }
+    const int o = fdiv_q(I.fd_rows, (int)ra);
+    const long long r = ra - (long long)o * I.rows;
+    const int i = SYM_I[o], j = SYM_J[o];
+    p = base + I.foff + (long long)(3 * i + j) * I.cells + r * I.nl;
+    q = base + I.foff + (long long)(3 * j + i) * I.cells + r * I.nl;
+}
+
 // ------------------------------------------------------------------------------------------
-// R2C along the contiguous axis: pairs of real rows (a + i b) per complex FFT.
+// R2C along the contiguous axis of the 6 input components (see RowSource): pairs of real rows
+// (a + i b) per complex FFT. FP32 plans also record FP64 sums of the rows (the k = 0 mode).
 // ------------------------------------------------------------------------------------------
 template <typename T, bool MEAN64>
 __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restrict__ insts, int n_inst,
@@ -67,7 +92,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
                                                   const T* __restrict__ beta,
                                                   typename VecOf<T>::type* __restrict__ spec,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  double* __restrict__ rowsum, int ncomp, int from_stress) {
+                                                  double* __restrict__ rowsum, int mode) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -75,14 +100,15 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_R2C].lines, ld = rows_ld(N);
-    const long long nrows = (long long)ncomp * I.rows;
+    const long long nrows = 6LL * I.rows;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const T* src = beta + (from_stress ? I.soff : I.foff);
+    const T half = (T)0.5;
 
-    const bool vec = ((N & 3) == 0) && ((((uintptr_t)src) & 15) == 0);
+    const bool vec = ((N & 3) == 0) && ((((uintptr_t)(beta + I.foff)) & 15) == 0) &&
+                     ((((uintptr_t)(beta + I.soff)) & 15) == 0) && ((I.cells & 3) == 0);
     if (vec) {
-#pragma unroll 4
+#pragma unroll 2
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
             const int i = i4 << 2;
             const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
@@ -90,23 +116,40 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
             T a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
             if (p < npairs) {
                 const long long ra = 2 * p;
-                load4(src + ra * N + idx, a);
-                if (ra + 1 < nrows) load4(src + (ra + 1) * N + idx, b);
+                const T *pa, *qa;
+                T u[4], v[4];
+                src_rows(I, beta, mode, ra, pa, qa);
+                load4(pa + idx, u);
+                load4(qa + idx, v);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q] = half * (u[q] + v[q]);
+                if (ra + 1 < nrows) {
+                    src_rows(I, beta, mode, ra + 1, pa, qa);
+                    load4(pa + idx, u);
+                    load4(qa + idx, v);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) b[q] = half * (u[q] + v[q]);
+                }
             }
             V* d = s + pl * ld + row_pad(idx);
 #pragma unroll
             for (int q = 0; q < 4; ++q) { V z; z.x = a[q]; z.y = b[q]; d[q] = z; }
         }
     } else {
-#pragma unroll 4
+#pragma unroll 2
         for (int i = tid; i < P * N; i += nt) {
             int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
             long long p = (long long)lb * P + pl;
             V z; z.x = 0; z.y = 0;
             if (p < npairs) {
                 long long ra = 2 * p;
-                z.x = src[ra * N + idx];
-                if (ra + 1 < nrows) z.y = src[(ra + 1) * N + idx];
+                const T *pa, *qa;
+                src_rows(I, beta, mode, ra, pa, qa);
+                z.x = half * (pa[idx] + qa[idx]);
+                if (ra + 1 < nrows) {
+                    src_rows(I, beta, mode, ra + 1, pa, qa);
+                    z.y = half * (pa[idx] + qa[idx]);
+                }
             }
             s[pl * ld + row_pad(idx)] = z;
         }
@@ -150,16 +193,35 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
 }
 
 // ------------------------------------------------------------------------------------------
-// C2R along the contiguous axis for the 6 stress components (pairs of half spectra).
+// C2R along the contiguous axis of 6 components (pairs of half spectra), row ra = o * rows + r:
+//   RD_STRESS:    to row ra of a 6-component stress-layout array (+ the FP64 mean stress of FP32
+//                 plans);
+//   RD_SYM_FIELD: to rows (i, j) and (j, i) of a 9-component field (the cotangent of beta from
+//                 that of its symmetric part: d/d beta_ij = d/d beta_ji = the symmetric entry).
 // The imaginary parts of the k = 0 and Nyquist bins are dropped (numpy irfft semantics).
 // ------------------------------------------------------------------------------------------
+enum RowDest { RD_STRESS = 0, RD_SYM_FIELD = 1 };
+
+template <typename T>
+__device__ __forceinline__ void dst_rows(const InstDev& I, T* base, int mode, long long ra, T*& p, T*& q) {
+    if (mode == RD_STRESS) {
+        p = q = base + I.soff + ra * I.nl;
+        return;
+    }
+    const int o = fdiv_q(I.fd_rows, (int)ra);
+    const long long r = ra - (long long)o * I.rows;
+    const int i = SYM_I[o], j = SYM_J[o];
+    p = base + I.foff + (long long)(3 * i + j) * I.cells + r * I.nl;
+    q = base + I.foff + (long long)(3 * j + i) * I.cells + r * I.nl;
+}
+
 template <typename T, bool MEAN64>
 __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restrict__ insts, int n_inst,
                                                   const int* __restrict__ pre,
                                                   const typename VecOf<T>::type* __restrict__ spec,
-                                                  T* __restrict__ sigma,
+                                                  T* __restrict__ out,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  const double* __restrict__ sbar, int ncomp, int to_field) {
+                                                  const double* __restrict__ sbar, int mode) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -167,7 +229,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_C2R].lines, ld = rows_ld(N), nh = I.nh;
-    const long long nrows = (long long)ncomp * I.rows;
+    const long long nrows = 6LL * I.rows;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
@@ -197,8 +259,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     __syncthreads();
     RowLayout lay{P, ld};
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
-    T* dst = sigma + (to_field ? I.foff : I.soff);
-    const bool vec = ((N & 3) == 0) && ((((uintptr_t)dst) & 15) == 0);
+    const bool vec = ((N & 3) == 0) && ((((uintptr_t)(out + I.soff)) & 15) == 0) &&
+                     ((((uintptr_t)(out + I.foff)) & 15) == 0) && ((I.cells & 3) == 0);
     if (vec) {
 #pragma unroll 2
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
@@ -217,8 +279,15 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
 #pragma unroll
                 for (int q = 0; q < 4; ++q) { va[q] += ma; vb[q] += mb; }
             }
-            store4(dst + ra * N + idx, va);
-            if (ra + 1 < nrows) store4(dst + (ra + 1) * N + idx, vb);
+            T *pd, *qd;
+            dst_rows(I, out, mode, ra, pd, qd);
+            store4(pd + idx, va);
+            if (qd != pd) store4(qd + idx, va);
+            if (ra + 1 < nrows) {
+                dst_rows(I, out, mode, ra + 1, pd, qd);
+                store4(pd + idx, vb);
+                if (qd != pd) store4(qd + idx, vb);
+            }
         }
     } else {
         for (int i = tid; i < P * N; i += nt) {
@@ -232,8 +301,15 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
                 va += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
                 if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)(ra + 1)));
             }
-            dst[ra * N + idx] = va;
-            if (ra + 1 < nrows) dst[(ra + 1) * N + idx] = vb;
+            T *pd, *qd;
+            dst_rows(I, out, mode, ra, pd, qd);
+            pd[idx] = va;
+            if (qd != pd) qd[idx] = va;
+            if (ra + 1 < nrows) {
+                dst_rows(I, out, mode, ra + 1, pd, qd);
+                pd[idx] = vb;
+                if (qd != pd) qd[idx] = vb;
+            }
         }
     }
 }
@@ -454,14 +530,14 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
     }
 }
 
-// Shared memory: 12 component slots of N x W (+W pad): slots 0..8 hold the 9 components, 9..11
+// Shared memory: 9 component slots of N x W (+W pad): slots 0..5 hold the 6 components, 6..8
 // are the ping-pong scratch. The transforms run three components at a time against the scratch;
 // when the stage count is odd the result is copied back to the component slots.
 template <typename V, bool INV>
 __device__ __forceinline__ void fft_group3(V* s, int g, int lgw, int cs, const LinePlan& lp,
                                            const V* __restrict__ tw, int tid, int nt) {
     V* a = s + 3 * g * cs;
-    V* b = s + 9 * cs;
+    V* b = s + 6 * cs;   // slots 6..8: scratch
     ColLayout<3> lay{lgw, cs};
     V* r = fft_lines<V, INV>(a, b, lay, lp, tw, tid, nt);
     if (r != a) {
@@ -503,8 +579,10 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     const long long cstride = (long long)N * estride;
     V* base = spec + I.spoff + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0;
 
-    constexpr int NIN = (GMODE == 1) ? 6 : 9;     // components in / out of the k-space pass
-    constexpr int NOUT = (GMODE == 1) ? 9 : 6;
+    // components in / out of the k-space pass: sym(beta) -> sigma (0), sigma cotangent -> cotangent of
+    // sym(beta) (1), sym(beta) -> d sigma / d nu (2); all symmetric, 6 components
+    constexpr int NIN = 6;
+    constexpr int NOUT = 6;
 #pragma unroll 1
     for (int c = 0; c < NIN; ++c) {
 #pragma unroll 4
@@ -544,9 +622,11 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         V b[NIN], o[NOUT];
 #pragma unroll
         for (int c = 0; c < NIN; ++c) b[c] = s[c * cs + i];
+        // the symmetric 3 x 3 matrix of the six components (row-major, b9[3i + j])
+        const V b9[9] = {b[0], b[1], b[2], b[1], b[3], b[4], b[2], b[4], b[5]};
         if constexpr (GMODE == 0) {
             V ph;
-            green_point<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64, phib ? &ph : nullptr);
+            green_point<T, V>(b9, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64, phib ? &ph : nullptr);
             if (phib) phib[e * estride + w] = ph;
         } else if constexpr (GMODE == 1) {
             if (phib) {
@@ -564,9 +644,18 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
                 const bool edge = (kh == 0) || (2 * kh == I.nl);
                 pacc += (edge ? 1.0 : 2.0) * acc;
             }
-            green_point_adj<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale);
+            V bb[9];
+            green_point_adj<T, V>(b, bb, kx, ky, kz, kzero, lam, mu, A, B, scale);
+            // cotangent of beta_ij (= of beta_ji) through s_ij = (beta_ij + beta_ji) / 2
+            const T hf = (T)0.5;
+            o[0] = bb[0];
+            o[1].x = hf * (bb[1].x + bb[3].x); o[1].y = hf * (bb[1].y + bb[3].y);
+            o[2].x = hf * (bb[2].x + bb[6].x); o[2].y = hf * (bb[2].y + bb[6].y);
+            o[3] = bb[4];
+            o[4].x = hf * (bb[5].x + bb[7].x); o[4].y = hf * (bb[5].y + bb[7].y);
+            o[5] = bb[8];
         } else {
-            green_point_dnu<T, V>(b, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
+            green_point_dnu<T, V>(b9, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
         }
 #pragma unroll
         for (int c = 0; c < NOUT; ++c) s[c * cs + i] = o[c];
@@ -600,23 +689,33 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
 // FP32 plans: FP64 mean of each beta component from the row sums; block (instance, component),
 // fixed-order strided sums and a fixed tree, so the result is deterministic.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_mean_beta(const InstDev* __restrict__ insts,
-                                                   const double* __restrict__ rowsum,
-                                                   double* __restrict__ mean9) {
+__global__ void __launch_bounds__(1024) k_mean_beta(const InstDev* __restrict__ insts,
+                                                    const double* __restrict__ rowsum,
+                                                    double* __restrict__ mean9) {
     const InstDev& I = insts[blockIdx.x];
     const int c = blockIdx.y;
-    __shared__ double red[8];
+    __shared__ double red[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double* rs = rowsum + I.rsoff + (long long)c * I.rows;
-    double acc = 0.0;
-    for (int r = tid; r < I.rows; r += blockDim.x) acc += rs[r];
+    // four independent accumulators per thread keep several loads in flight; fixed order throughout
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const int nt = blockDim.x;
+    int r = tid;
+    for (; r + 3 * nt < I.rows; r += 4 * nt) {
+        a0 += rs[r];
+        a1 += rs[r + nt];
+        a2 += rs[r + 2 * nt];
+        a3 += rs[r + 3 * nt];
+    }
+    for (; r < I.rows; r += nt) a0 += rs[r];
+    double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) red[warp] = acc;
     __syncthreads();
     if (tid == 0) {
         double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        for (int w = 0; w < (nt >> 5); ++w) s += red[w];
         mean9[9 * blockIdx.x + c] = s * I.inv_cells;
     }
 }
@@ -634,11 +733,11 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     const LaunchShape* L = P.pass;
     if (f32) {
         k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, 9, 0);
-        k_mean_beta<<<dim3(P.n_inst, 9), 256, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM);
+        k_mean_beta<<<dim3(P.n_inst, 6), 1024, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, 9, 0);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, RS_SYM);
     }
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
@@ -654,26 +753,25 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
             P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
     if (f32)
         k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, 6, 0);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS);
     else
         k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, 6, 0);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS);
     return cudaGetLastError();
 }
 
-// Adjoint (GMODE 1: stress cotangent, 6 components in stress layout -> beta cotangent, 9 components
-// in field layout) and the nu-derivative of the stress (GMODE 2: 9 -> 6). Both keep the k = 0
-// mode in the transforms (no FP64 mean path).
+// Adjoint (GMODE 1: stress cotangent, 6 components in stress layout -> beta cotangent, written to all
+// 9 components of a field) and the nu-derivative of the stress (GMODE 2: beta -> 6 components).
+// Both keep the k = 0 mode in the transforms (no FP64 mean path).
 template <typename T, int GMODE>
 static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* out, const void* phi, double* part,
                                       cudaStream_t st) {
     typedef typename VecOf<T>::type V;
     V* spec = (V*)P.d_spec;
     const V* tw = (const V*)P.d_tw;
-    const LaunchShape* L = (GMODE == 1) ? P.adj : P.pass;
-    const int nin = (GMODE == 1) ? 6 : 9, nout = (GMODE == 1) ? 9 : 6;
+    const LaunchShape* L = P.pass;
     k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, nin, GMODE == 1 ? 1 : 0);
+        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, GMODE == 1 ? RS_STRESS : RS_SYM);
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
@@ -683,7 +781,7 @@ static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* o
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
     k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, nout, GMODE == 1 ? 1 : 0);
+        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, GMODE == 1 ? RD_SYM_FIELD : RD_STRESS);
     return cudaGetLastError();
 }
 
