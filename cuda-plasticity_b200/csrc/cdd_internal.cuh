@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/cdd.h"
 
 namespace cdd {
@@ -44,7 +46,37 @@ struct LinePlan {
     int tw;   // offset (complex elements) of this length's twiddle table w_n^k, k < n
     FDiv nr[MAX_STAGES];   // stage st: butterflies per line n / radix[st]
     FDiv ns[MAX_STAGES];   // stage st: span of the finished sub-transforms (product of earlier radices)
+    int twst[MAX_STAGES];  // stage st: offset (even, complex elements) of its twiddle rows
 };
+
+// Radix rounded up to even: the length of one twiddle row (pairs load as one 16-byte vector).
+__host__ __device__ constexpr int tw_row(int R) { return R + (R & 1); }
+
+// Twiddle rows of every stage of lp in butterfly order: row jm of stage st holds
+// w_n^(r jm n / (ns R)), r < R (then (1, 0) padding), ns = lp.ns[st].d, from the length-n table
+// already at re/im[lp.tw ...]. Appends to re/im and sets lp.twst. Over all stages the rows take
+// sum_st ns_st tw_row(R_st) <= 2n entries.
+inline void append_stage_twiddles(LinePlan& lp, std::vector<double>& re, std::vector<double>& im) {
+    const int n = lp.n;
+    for (int st = 0; st < lp.nst; ++st) {
+        if (re.size() & 1) { re.push_back(1.0); im.push_back(0.0); }   // even start: 16-byte rows
+        lp.twst[st] = (int)re.size();
+        const int R = lp.radix[st], ns = lp.ns[st].d, Rp = tw_row(R);
+        const int twstep = n / (ns * R);
+        for (int jm = 0; jm < ns; ++jm)
+            for (int r = 0; r < Rp; ++r) {
+                if (r < R) {
+                    const int k = (int)(((long long)r * jm * twstep) % n);
+                    const double wr = re[lp.tw + k], wi = im[lp.tw + k];
+                    re.push_back(wr);
+                    im.push_back(wi);
+                } else {
+                    re.push_back(1.0);
+                    im.push_back(0.0);
+                }
+            }
+    }
+}
 
 // Per-pass tiling of one instance (host-chosen, read by the kernels).
 struct PassTile {
@@ -112,6 +144,27 @@ template <typename V> __device__ __forceinline__ V vmul(V a, V b) {
     V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
 }
 template <typename V> __device__ __forceinline__ V vconj(V a) { a.y = -a.y; return a; }
+// a * conj(w)
+template <typename V> __device__ __forceinline__ V vmulc(V a, V w) {
+    V r; r.x = a.x * w.x + a.y * w.y; r.y = a.y * w.x - a.x * w.y; return r;
+}
+
+// One twiddle row (R values) of a stage: 16-byte vector loads (two float2 or one double2 each).
+template <int R>
+__device__ __forceinline__ void load_tw_row(const float2* __restrict__ row, float2* w) {
+    const float4* q = reinterpret_cast<const float4*>(row);
+#pragma unroll
+    for (int k = 0; k < tw_row(R) / 2; ++k) {
+        const float4 v = __ldg(q + k);
+        w[2 * k] = make_float2(v.x, v.y);
+        if (2 * k + 1 < R) w[2 * k + 1] = make_float2(v.z, v.w);
+    }
+}
+template <int R>
+__device__ __forceinline__ void load_tw_row(const double2* __restrict__ row, double2* w) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) w[k] = __ldg(row + k);
+}
 template <typename V, typename T> __device__ __forceinline__ V vscale(V a, T s) { a.x *= s; a.y *= s; return a; }
 template <typename V> __device__ __forceinline__ V vmake(double x, double y) {
     V r; r.x = (decltype(r.x))x; r.y = (decltype(r.y))y; return r;
@@ -280,10 +333,9 @@ template <int K> __device__ __forceinline__ int lay_lines(const ColLayout<K>& la
 template <int R, typename V, bool INV, typename Lay>
 __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restrict__ dst,
                                           const Lay& lay, const FDiv& fnr, const FDiv& fns,
-                                          const V* __restrict__ tw, int tid, int nt) {
+                                          const V* __restrict__ twrows, int tid, int nt) {
     const int nr = fnr.d;
     const int ns = fns.d;
-    const int twstep = fdiv_q(fns, nr);     // n / (ns R)
     const int total = lay_lines(lay) * nr;
 #pragma unroll 1
     for (int g = tid; g < total; g += nt) {
@@ -291,15 +343,17 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
         lay.split(g, fnr, l, j);
         const int jm = j - fdiv_q(fns, j) * ns;
         V v[R];
+        if (ns == 1) {   // first stage: all twiddles are 1
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            V a = src[lay.addr(l, j + r * nr)];
-            if (r > 0 && jm != 0) {
-                V w = __ldg(&tw[r * jm * twstep]);
-                if (INV) w.y = -w.y;
-                a = vmul(a, w);
+            for (int r = 0; r < R; ++r) v[r] = src[lay.addr(l, j + r * nr)];
+        } else {
+            V w[R];
+            load_tw_row<R>(twrows + jm * tw_row(R), w);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const V a = src[lay.addr(l, j + r * nr)];
+                v[r] = (r == 0) ? a : (INV ? vmulc(a, w[r]) : vmul(a, w[r]));
             }
-            v[r] = a;
         }
         dft<R, V, INV>(v);
         const int jd = (j - jm) * R + jm;
@@ -314,13 +368,13 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
 template <typename V, bool INV, typename Lay>
 __device__ __forceinline__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
                         int tid, int nt) {
-    const V* tw = twbase + lp.tw;
     V* src = a;
     V* dst = b;
     for (int st = 0; st < lp.nst; ++st) {
         const int R = lp.radix[st];
         const FDiv& fnr = lp.nr[st];
         const FDiv& fns = lp.ns[st];
+        const V* tw = twbase + lp.twst[st];
         switch (R) {
             case 2: fft_stage<2, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
             case 3: fft_stage<3, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;

@@ -147,24 +147,25 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
     I.lamb = 2. * d->mu * d->nu / (1. - 2. * d->nu);
     I.inv_cells = 1.0 / (double)I.cells;
     std::vector<double> twre, twim, ktab;
-    std::map<int, int> tw_off;
+    std::map<int, LinePlan> lp_done;
     LinePlan* lps[3] = {&I.lp_last, &I.lp_mid, &I.lp_first};
     int lens[3] = {I.nl, I.nd == 3 ? I.n1 : I.n0, I.n0};
     for (int k = 0; k < 3; ++k) {
         if (!na_line_plan(lens[k], *lps[k]))
             return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: no FFT plan for length " + std::to_string(lens[k]));
-        auto it = tw_off.find(lens[k]);
-        if (it == tw_off.end()) {
-            int off = (int)twre.size();
+        auto it = lp_done.find(lens[k]);
+        if (it == lp_done.end()) {
+            lps[k]->tw = (int)twre.size();
             for (int j = 0; j < lens[k]; ++j) {
                 double re, im;
                 na_twiddle(lens[k], j, re, im);
                 twre.push_back(re);
                 twim.push_back(im);
             }
-            it = tw_off.emplace(lens[k], off).first;
+            append_stage_twiddles(*lps[k], twre, twim);
+            it = lp_done.emplace(lens[k], *lps[k]).first;
         }
-        lps[k]->tw = it->second;
+        *lps[k] = it->second;
     }
     if (I.nd == 3) {
         I.koff0 = (int)ktab.size();

@@ -311,7 +311,7 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
     const size_t elt = precision == CDD_F64 ? sizeof(double) : sizeof(float);
     p->desc.assign(inst, inst + n_inst);
     p->inst.resize(n_inst);
-    std::map<int, int> tw_off;
+    std::map<int, LinePlan> lp_done;   // line plans (with twiddle offsets) by length
     std::vector<double> twre, twim;
     std::vector<double> ktab;
     long long foff = 0, soff = 0, coff = 0, spoff = 0, rsoff = 0;
@@ -361,18 +361,19 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
                 free_plan(p);
                 return fail(CDD_ERR_SHAPE, "instance %d: no FFT plan for length %d", i, lens[k]);
             }
-            auto it = tw_off.find(lens[k]);
-            if (it == tw_off.end()) {
-                int off = (int)twre.size();
+            auto it = lp_done.find(lens[k]);
+            if (it == lp_done.end()) {
+                lps[k]->tw = (int)twre.size();
                 for (int kk = 0; kk < lens[k]; ++kk) {
                     long double re, im;
                     twiddle(lens[k], kk, re, im);
                     twre.push_back((double)re);
                     twim.push_back((double)im);
                 }
-                it = tw_off.emplace(lens[k], off).first;
+                append_stage_twiddles(*lps[k], twre, twim);
+                it = lp_done.emplace(lens[k], *lps[k]).first;
             }
-            lps[k]->tw = it->second;
+            *lps[k] = it->second;
         }
         // k tables (FourierSpaceTools.py L26-55)
         if (I.nd == 3) {

@@ -251,25 +251,38 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
     // from shared memory (register budget).
     constexpr bool KEEPU = (sizeof(T) == 4);
     T Ukeep[KEEPU ? ND : 1][2][9];
+    if constexpr (KEEPU) {
+        // all derivatives first (shared memory only), so that the stress loads issued above have
+        // the whole derivative evaluation to arrive before the first use
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        T U[ND][2][3];
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
+        for (int c = 0; c < 9; ++c)
 #pragma unroll
             for (int d = 0; d < ND; ++d) {
                 T v5[5];
-                tv.load5(3 * l + j, d, v5);
-                derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                tv.load5(c, d, v5);
+                derivs5(v5, ih, Ukeep[d][0][c], Ukeep[d][1][c]);
             }
-        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        T U[ND][2][3];
         if constexpr (KEEPU) {
 #pragma unroll
             for (int d = 0; d < ND; ++d)
 #pragma unroll
                 for (int s = 0; s < 2; ++s)
 #pragma unroll
-                    for (int l = 0; l < 3; ++l) Ukeep[d][s][3 * l + j] = U[d][s][l];
+                    for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
+        } else {
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T v5[5];
+                    tv.load5(3 * l + j, d, v5);
+                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                }
+            }
         }
         T Sj[3], Sdj[3];
 #pragma unroll
