@@ -47,6 +47,7 @@ struct LinePlan {
     FDiv nr[MAX_STAGES];   // stage st: butterflies per line n / radix[st]
     FDiv ns[MAX_STAGES];   // stage st: span of the finished sub-transforms (product of earlier radices)
     int twst[MAX_STAGES];  // stage st: offset (even, complex elements) of its twiddle rows
+    int twspan;            // elements from twst[0] to the end of the last stage's rows
 };
 
 // Radix rounded up to even: the length of one twiddle row (pairs load as one 16-byte vector).
@@ -76,6 +77,16 @@ inline void append_stage_twiddles(LinePlan& lp, std::vector<double>& re, std::ve
                 }
             }
     }
+    lp.twspan = (int)re.size() - lp.twst[0];
+}
+
+// Copy the twiddle rows of lp (global table tw) into shared memory at dst (16-byte aligned);
+// fft_lines then reads them with rebase = lp.twst[0]. The caller synchronises before use.
+template <typename V>
+__device__ __forceinline__ void stage_tw_to_smem(const LinePlan& lp, const V* __restrict__ tw, V* dst, int tid,
+                                                 int nt) {
+    const V* src = tw + lp.twst[0];
+    for (int i = tid; i < lp.twspan; i += nt) dst[i] = __ldg(src + i);
 }
 
 // Per-pass tiling of one instance (host-chosen, read by the kernels).
@@ -150,12 +161,13 @@ template <typename V> __device__ __forceinline__ V vmulc(V a, V w) {
 }
 
 // One twiddle row (R values) of a stage: 16-byte vector loads (two float2 or one double2 each).
+// Plain loads: the rows live in shared memory (copied per block) or in global memory.
 template <int R>
 __device__ __forceinline__ void load_tw_row(const float2* __restrict__ row, float2* w) {
     const float4* q = reinterpret_cast<const float4*>(row);
 #pragma unroll
     for (int k = 0; k < tw_row(R) / 2; ++k) {
-        const float4 v = __ldg(q + k);
+        const float4 v = q[k];
         w[2 * k] = make_float2(v.x, v.y);
         if (2 * k + 1 < R) w[2 * k + 1] = make_float2(v.z, v.w);
     }
@@ -163,7 +175,7 @@ __device__ __forceinline__ void load_tw_row(const float2* __restrict__ row, floa
 template <int R>
 __device__ __forceinline__ void load_tw_row(const double2* __restrict__ row, double2* w) {
 #pragma unroll
-    for (int k = 0; k < R; ++k) w[k] = __ldg(row + k);
+    for (int k = 0; k < R; ++k) w[k] = row[k];
 }
 template <typename V, typename T> __device__ __forceinline__ V vscale(V a, T s) { a.x *= s; a.y *= s; return a; }
 template <typename V> __device__ __forceinline__ V vmake(double x, double y) {
@@ -367,14 +379,14 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
 // layout). Returns the buffer that holds the result. Every thread of the block must call this.
 template <typename V, bool INV, typename Lay>
 __device__ __forceinline__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
-                        int tid, int nt) {
+                        int tid, int nt, int rebase = 0) {
     V* src = a;
     V* dst = b;
     for (int st = 0; st < lp.nst; ++st) {
         const int R = lp.radix[st];
         const FDiv& fnr = lp.nr[st];
         const FDiv& fns = lp.ns[st];
-        const V* tw = twbase + lp.twst[st];
+        const V* tw = twbase + (lp.twst[st] - rebase);
         switch (R) {
             case 2: fft_stage<2, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;
             case 3: fft_stage<3, V, INV>(src, dst, lay, fnr, fns, tw, tid, nt); break;

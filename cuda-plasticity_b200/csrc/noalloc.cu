@@ -202,7 +202,8 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.blocks = (int)((npairs + Pl - 1) / Pl);
         t.tiles_a = 1;
         P.pass[k].threads = t.threads;
-        P.pass[k].smem = 2 * (size_t)Pl * line_bytes;
+        P.pass[k].smem = ((2 * (size_t)Pl * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
+                         (size_t)I.lp_last.twspan * velt;
     }
     for (int k : {PASS_MID_F, PASS_MID_I}) {
         PassTile& t = I.tile[k];
@@ -216,7 +217,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.threads = 256;
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = comps * I.n0 * t.tiles_a;
-        P.pass[k].smem = 2 * (size_t)W * I.n1 * velt;
+        P.pass[k].smem = 2 * (size_t)W * I.n1 * velt + (size_t)I.lp_mid.twspan * velt;
     }
     {
         PassTile& t = I.tile[PASS_GREEN];
@@ -230,7 +231,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
         P.pass[PASS_GREEN].threads = 256;
-        P.pass[PASS_GREEN].smem = (size_t)9 * (I.n0 * W + W) * velt;
+        P.pass[PASS_GREEN].smem = ((size_t)9 * (I.n0 * W + W) + 1) / 2 * 2 * velt + (size_t)I.lp_first.twspan * velt;
     }
     for (int k = 0; k < NUM_PASSES; ++k) {
         blocks[k] = I.tile[k].blocks;

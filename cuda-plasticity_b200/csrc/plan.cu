@@ -178,7 +178,8 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = (velt == 8) ? 256 : 128;
             t.blocks = (int)((npairs + P - 1) / P);
             t.tiles_a = 1;
-            size_t sm = 2 * (size_t)P * line_bytes;
+            size_t sm = ((2 * (size_t)P * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
+                        (size_t)I.lp_last.twspan * velt;   // buffers + twiddle rows
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;
         }
@@ -195,7 +196,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = comps * I.n0 * t.tiles_a;
-            size_t sm = 2 * (size_t)W * I.n1 * velt;
+            size_t sm = 2 * (size_t)W * I.n1 * velt + (size_t)I.lp_mid.twspan * velt;
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;
         }
@@ -212,7 +213,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = (I.nd == 3 ? I.n1 : 1) * t.tiles_a;
-            size_t sm = (size_t)9 * (I.n0 * W + W) * velt;
+            size_t sm = ((size_t)9 * (I.n0 * W + W) + 1) / 2 * 2 * velt + (size_t)I.lp_first.twspan * velt;
             if (sm > smem_max[PASS_GREEN]) smem_max[PASS_GREEN] = sm;
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }

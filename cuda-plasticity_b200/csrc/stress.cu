@@ -154,6 +154,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
             s[pl * ld + row_pad(idx)] = z;
         }
     }
+    V* tws = s + ((2 * P * ld + 1) & ~1);   // twiddle rows, 16-byte aligned after the buffers
+    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     __syncthreads();
     if (MEAN64) {
         const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
         }
     }
     RowLayout lay{P, ld};
-    s = fft_lines<V, false>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
+    s = fft_lines<V, false>(s, s + P * ld, lay, I.lp_last, tws, tid, nt, I.lp_last.twst[0]);
     const int nh = I.nh;
     V* dst = spec + I.spoff;
     for (int i = tid; i < P * nh; i += nt) {
@@ -256,9 +258,11 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
             s[pl * ld + row_pad(N - k)] = z;
         }
     }
+    V* tws = s + ((2 * P * ld + 1) & ~1);
+    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     __syncthreads();
     RowLayout lay{P, ld};
-    s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tw, tid, nt);
+    s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tws, tid, nt, I.lp_last.twst[0]);
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(out + I.soff)) & 15) == 0) &&
                      ((((uintptr_t)(out + I.foff)) & 15) == 0) && ((I.cells & 3) == 0);
     if (vec) {
@@ -340,16 +344,18 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int wv = min(W, nh - col0);
     const int tid = threadIdx.x, nt = blockDim.x;
     V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
-#pragma unroll 4
+#pragma unroll 8
     for (int i = tid; i < N * W; i += nt) {
         const int e = i >> lgw, w = i & (W - 1);
         V z; z.x = 0; z.y = 0;
         if (w < wv) z = base[(long long)e * nhp + w];
         s[i] = z;
     }
+    V* tws = s + 2 * N * W;
+    stage_tw_to_smem(I.lp_mid, tw, tws, tid, nt);
     __syncthreads();
     ColLayout<1> lay{lgw, 0};
-    s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tw, tid, nt);
+    s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tws, tid, nt, I.lp_mid.twst[0]);
 #pragma unroll 4
     for (int i = tid; i < N * W; i += nt) {
         const int e = i >> lgw, w = i & (W - 1);
@@ -535,11 +541,11 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
 // when the stage count is odd the result is copied back to the component slots.
 template <typename V, bool INV>
 __device__ __forceinline__ void fft_group3(V* s, int g, int lgw, int cs, const LinePlan& lp,
-                                           const V* __restrict__ tw, int tid, int nt) {
+                                           const V* __restrict__ tws, int tid, int nt) {
     V* a = s + 3 * g * cs;
     V* b = s + 6 * cs;   // slots 6..8: scratch
     ColLayout<3> lay{lgw, cs};
-    V* r = fft_lines<V, INV>(a, b, lay, lp, tw, tid, nt);
+    V* r = fft_lines<V, INV>(a, b, lay, lp, tws, tid, nt, lp.twst[0]);
     if (r != a) {
         for (int i = tid; i < 3 * cs; i += nt) a[i] = b[i];
         __syncthreads();
@@ -585,7 +591,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     constexpr int NOUT = 6;
 #pragma unroll 1
     for (int c = 0; c < NIN; ++c) {
-#pragma unroll 4
+#pragma unroll 8
         for (int rem = tid; rem < N * W; rem += nt) {
             const int e = rem >> lgw, w = rem & (W - 1);
             V z; z.x = 0; z.y = 0;
@@ -593,8 +599,10 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
             s[c * cs + rem] = z;
         }
     }
+    V* tws = s + ((9 * cs + 1) & ~1);   // twiddle rows after the 9 slots
+    stage_tw_to_smem(I.lp_first, tw, tws, tid, nt);
     __syncthreads();
-    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -674,7 +682,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         }
     }
     __syncthreads();
-    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tw, tid, nt);
+    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
 #pragma unroll 1
     for (int c = 0; c < NOUT; ++c) {
 #pragma unroll 4
