@@ -41,6 +41,27 @@ class cdd_instance(ctypes.Structure):
     ]
 
 
+class cdd_tuning(ctypes.Structure):
+    """Per-instance launch-shape choices (include/cdd.h); 0 keeps the built-in rule."""
+    _fields_ = [
+        ("fft_radix", ctypes.c_int),
+        ("rows_lines", ctypes.c_int),
+        ("mid_cols", ctypes.c_int),
+        ("green_cols", ctypes.c_int),
+        ("stencil_planes", ctypes.c_int),
+    ]
+
+    KEYS = ("fft_radix", "rows_lines", "mid_cols", "green_cols", "stencil_planes")
+
+    @classmethod
+    def from_dict(cls, d):
+        d = d or {}
+        return cls(*[int(d.get(k, 0) or 0) for k in cls.KEYS])
+
+    def to_dict(self):
+        return {k: int(getattr(self, k)) for k in self.KEYS}
+
+
 class CDDError(RuntimeError):
     def __init__(self, code, msg):
         self.code = code
@@ -52,6 +73,9 @@ _lib = None
 CDD_PBAR = 9   # doubles per instance in the parameter cotangent of cdd_step_adjoint
 
 _PROTOS = {
+    "cdd_plan_create_tuned": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(cdd_tuning), ctypes.POINTER(ctypes.c_void_p)]),
+    "cdd_plan_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(cdd_tuning)]),
     "cdd_plan_create": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "cdd_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -58,9 +58,15 @@ def _stream(stream=None):
 
 
 class Plan:
-    """A batch of instances at one precision ("f64" or "f32") on the current CUDA device."""
+    """A batch of instances at one precision ("f64" or "f32") on the current CUDA device.
 
-    def __init__(self, instances, precision="f64", device=None):
+    tuning: None (built-in launch shapes), a list with one dict per instance (keys of
+    ``_lib.cdd_tuning``: fft_radix, rows_lines, mid_cols, green_cols, stencil_planes; missing or 0
+    keeps the built-in rule), or "auto" (``cdd.autotune`` picks them by timing, cached per GPU,
+    precision and shape).
+    """
+
+    def __init__(self, instances, precision="f64", device=None, tuning=None):
         if isinstance(instances, Instance):
             instances = [instances]
         self.instances = list(instances)
@@ -73,13 +79,23 @@ class Plan:
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.lib = _lib.load()
         arr = (_lib.cdd_instance * len(self.instances))(*[i.to_c() for i in self.instances])
+        n = len(self.instances)
+        if isinstance(tuning, str):
+            if tuning != "auto":
+                raise ValueError("tuning must be None, a list of dicts or 'auto'")
+            from . import autotune
+            with torch.cuda.device(self.device):
+                tuning = [autotune.best(inst, precision) for inst in self.instances]
+        tune = None
+        if tuning is not None:
+            if len(tuning) != n:
+                raise ValueError("tuning needs one entry per instance")
+            tune = (_lib.cdd_tuning * n)(*[_lib.cdd_tuning.from_dict(t) for t in tuning])
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            check(self.lib.cdd_plan_create(arr, len(self.instances),
-                                           _lib.CDD_F64 if precision == "f64" else _lib.CDD_F32,
-                                           ctypes.byref(h)))
+            check(self.lib.cdd_plan_create_tuned(arr, n, _lib.CDD_F64 if precision == "f64" else _lib.CDD_F32,
+                                                 tune, ctypes.byref(h)))
         self.handle = h
-        n = len(self.instances)
         self.field_elems = int(self.lib.cdd_plan_field_elems(h))
         self.stress_elems = int(self.lib.cdd_plan_stress_elems(h))
         self.field_offsets = [int(self.lib.cdd_plan_field_offset(h, i)) for i in range(n)]
@@ -87,6 +103,12 @@ class Plan:
         self.cells = [int(self.lib.cdd_plan_cells(h, i)) for i in range(n)]
         self.total_cells = int(self.lib.cdd_plan_cells(h, -1))
         self.scratch_bytes = int(self.lib.cdd_plan_scratch_bytes(h))
+
+    def tuning(self, i=0):
+        """The launch shapes instance i runs with (dict)."""
+        t = _lib.cdd_tuning()
+        check(self.lib.cdd_plan_tuning(self.handle, int(i), ctypes.byref(t)))
+        return t.to_dict()
 
     # ------------------------------------------------------------------ lifetime
     def close(self):

@@ -490,8 +490,25 @@ cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st);
 cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaStream_t st);
 cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st);
 cudaError_t stencil_set_attributes(int precision, size_t smem);
+
+// Raise a kernel's dynamic shared-memory limit to smem, clamped to what the device allows next to
+// the kernel's own static shared memory. The limit is a property of the kernel function, shared by
+// every plan in the process, so plans always raise it to the device limit (SIZE_MAX) rather than
+// to their own need: a later plan must not lower it under an earlier plan's launches.
+template <typename F>
+inline cudaError_t set_dyn_smem_limit(F* fn, size_t smem) {
+    int dev = 0, optin = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, fn))) return e;
+    const long long lim = (long long)optin - (long long)fa.sharedSizeBytes;
+    const long long v = (smem < (size_t)lim) ? (long long)smem : lim;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v);
+}
 size_t stencil_smem_bytes(int precision, bool any3d);
-void stencil_geometry(InstDev& I);
+void stencil_geometry(InstDev& I, int planes = 0);
 cudaError_t stress_set_attributes(int precision, size_t max_smem);
 
 }  // namespace cdd

@@ -43,21 +43,22 @@ bool factor(int n, int& a, int& b, int& c) {
     return n == 1;
 }
 
-// Radix sequence for length n = 2^a 3^b 5^c: radix-16 stages for the power of two (an 8 x 4
-// pair instead of 16 x 2 when a = 1 mod 4), then radix 3 and radix 5 stages.
-bool make_line_plan(int n, LinePlan& lp) {
+// Radix sequence for length n = 2^a 3^b 5^c: stages of radix maxr = 2^e (16, 8 or 4) for the
+// power of two, the remainder as one smaller power-of-two stage (a radix-2 remainder after a
+// larger stage is folded into a (maxr/2, 4) pair), then radix 3 and radix 5 stages.
+bool make_line_plan(int n, LinePlan& lp, int maxr = 16) {
     int a, b, c;
     if (!factor(n, a, b, c) || a < 1) return false;
     std::memset(&lp, 0, sizeof lp);
     lp.n = n;
+    const int e = (maxr == 4) ? 2 : (maxr == 8) ? 3 : 4;
     std::vector<int> r;
-    int q = a / 4, m = a % 4;
-    if (m == 1 && q > 0) { q -= 1; m = 5; }
-    for (int i = 0; i < q; ++i) r.push_back(16);
-    if (m == 1) r.push_back(2);
-    else if (m == 2) r.push_back(4);
-    else if (m == 3) r.push_back(8);
-    else if (m == 5) { r.push_back(8); r.push_back(4); }
+    int q = a / e, m = a % e;
+    bool fold = (m == 1 && q > 0 && e >= 3);
+    if (fold) q -= 1;
+    for (int i = 0; i < q; ++i) r.push_back(1 << e);
+    if (fold) { r.push_back(1 << (e - 1)); r.push_back(4); }
+    else if (m > 0) r.push_back(1 << m);
     for (int i = 0; i < b; ++i) r.push_back(3);
     for (int i = 0; i < c; ++i) r.push_back(5);
     if ((int)r.size() > MAX_STAGES) return false;
@@ -127,6 +128,7 @@ struct cdd_plan {
     int device = 0;
     StencilMapSet maps_f0, maps_f1, maps_user;   // tensor maps of the stage inputs
     const void* maps_user_ptr = nullptr;
+    std::vector<cdd_tuning> tune;                 // requested (zeros: built-in), then effective
 };
 
 namespace {
@@ -170,7 +172,9 @@ int build_shapes(cdd_plan* p, size_t elt) {
             const int comps = 6;
             long long npairs = ((long long)comps * I.rows + 1) / 2;
             const size_t line_bytes = (size_t)(I.nl + (I.nl >> 4) + 1) * velt;
+            const cdd_tuning& tu = p->tune[i];
             int P = (velt == 8 ? 4096 : 2048) / I.nl;   // radix-16 stages: one butterfly per thread
+            if (tu.rows_lines > 0) P = tu.rows_lines;
             if (P < 1) P = 1;
             if (P > npairs) P = (int)npairs;
             PassTile& t = I.tile[k];
@@ -190,6 +194,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             const int comps = 6;
             int W = (int)(128 / velt);
             while (W > 1 && 2 * (size_t)W * I.n1 * velt > 96 * 1024) W >>= 1;
+            if (p->tune[i].mid_cols > 0) W = p->tune[i].mid_cols;
             t.lines = W;
             t.lgw = 0;
             while ((1 << t.lgw) < W) ++t.lgw;
@@ -205,8 +210,12 @@ int build_shapes(cdd_plan* p, size_t elt) {
             PassTile& t = I.tile[PASS_GREEN];
             int W = (int)(32 / velt);   // 32-byte row segments
             while (W > 1 && (size_t)9 * (I.n0 * W + W) * velt > 100 * 1024) W >>= 1;
-            if ((size_t)9 * (I.n0 * W + W) * velt > 220 * 1024)
+            if (p->tune[i].green_cols > 0) W = p->tune[i].green_cols;
+            if ((size_t)9 * (I.n0 * W + W) * velt > 220 * 1024) {
+                if (p->tune[i].green_cols > 0)
+                    return fail(CDD_ERR_ARG, "instance %d: tuning green_cols %d needs too much shared memory", i, W);
                 return fail(CDD_ERR_SHAPE, "axis-0 length %d too large for the fused k-space pass", I.n0);
+            }
             t.lines = W;
             t.lgw = 0;
             while ((1 << t.lgw) < W) ++t.lgw;
@@ -218,12 +227,26 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }
         for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(pre[k].back() + I.tile[k].blocks);
-        stencil_geometry(I);
+        stencil_geometry(I, p->tune[i].stencil_planes);
+        // effective launch shapes of this instance
+        p->tune[i].rows_lines = I.tile[PASS_R2C].lines;
+        p->tune[i].mid_cols = (I.nd == 3) ? I.tile[PASS_MID_F].lines : 0;
+        p->tune[i].green_cols = I.tile[PASS_GREEN].lines;
+        p->tune[i].stencil_planes = (I.nd == 3) ? I.st_zc : 0;
         I.tma_slot = -1;
         if (stencil_tma_eligible(I, C.precision) && n_tma < CDD_MAX_TMA_INSTANCES) I.tma_slot = n_tma++;
         pre_st.push_back(pre_st.back() + I.stencil_blocks);
         pre_ob.push_back(pre_ob.back() + (int)((I.cells + 255) / 256));
         pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));
+    }
+    {
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        for (int k = 0; k < NUM_PASSES; ++k)
+            if (optin > 0 && smem_max[k] + 1024 > (size_t)optin)
+                return fail(CDD_ERR_ARG, "launch shapes need %zu bytes of shared memory in FFT pass %d (limit %d)",
+                            smem_max[k], k, optin);
     }
     size_t smem_all = 0;
     for (int k = 0; k < NUM_PASSES; ++k) {
@@ -238,7 +261,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
     C.stencil.blocks = pre_st.back();
     C.stencil.threads = 256;
     C.stencil.smem = stencil_smem_bytes(C.precision, C.any3d);
-    CDD_CUDA(stencil_set_attributes(C.precision, C.stencil.smem < 48 * 1024 ? 48 * 1024 : C.stencil.smem));
+    CDD_CUDA(stencil_set_attributes(C.precision, SIZE_MAX));   // device limit (see set_dyn_smem_limit)
     {
         std::vector<int> pre_v(1, 0);
         for (int i = 0; i < n; ++i) pre_v.push_back(pre_v.back() + (int)((p->inst[i].cells + 127) / 128));
@@ -257,7 +280,8 @@ int build_shapes(cdd_plan* p, size_t elt) {
     C.cellwise.threads = 256;
     CDD_CUDA(dalloc(p, (void**)&C.cellwise.d_pre, sizeof(int) * (n + 1)));
     CDD_CUDA(cudaMemcpy(C.cellwise.d_pre, pre_cw.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    CDD_CUDA(stress_set_attributes(C.precision, smem_all < 48 * 1024 ? 48 * 1024 : smem_all));
+    CDD_CUDA(stress_set_attributes(C.precision, SIZE_MAX));   // device limit (see set_dyn_smem_limit)
+    (void)smem_all;
     return CDD_OK;
 }
 
@@ -301,18 +325,44 @@ const char* cdd_last_error(void) { return g_last_error.c_str(); }
 const char* cdd_version(void) { return "cdd-b200 0.1 (sm_100a)"; }
 
 int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_plan** out) {
+    return cdd_plan_create_tuned(inst, n_inst, precision, nullptr, out);
+}
+
+int cdd_plan_tuning(const cdd_plan* p, int i, cdd_tuning* out) {
+    if (!p || !out || i < 0 || i >= p->core.n_inst) return fail(CDD_ERR_ARG, "bad arguments to cdd_plan_tuning");
+    *out = p->tune[i];
+    return CDD_OK;
+}
+
+int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, const cdd_tuning* tune,
+                          cdd_plan** out) {
     g_last_error.clear();
     if (!inst || n_inst <= 0 || !out) return fail(CDD_ERR_ARG, "bad arguments to cdd_plan_create");
     if (precision != CDD_F64 && precision != CDD_F32) return fail(CDD_ERR_ARG, "bad precision %d", precision);
     *out = nullptr;
+    auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+    for (int i = 0; tune && i < n_inst; ++i) {
+        const cdd_tuning& t = tune[i];
+        if ((t.fft_radix && t.fft_radix != 4 && t.fft_radix != 8 && t.fft_radix != 16) ||
+            (t.rows_lines && (!pow2(t.rows_lines) || t.rows_lines > 256)) ||
+            (t.mid_cols && (!pow2(t.mid_cols) || t.mid_cols > 64)) ||
+            (t.green_cols && (!pow2(t.green_cols) || t.green_cols > 64)) || t.stencil_planes < 0 ||
+            t.fft_radix < 0 || t.rows_lines < 0 || t.mid_cols < 0 || t.green_cols < 0)
+            return fail(CDD_ERR_ARG, "instance %d: bad tuning (radix 4/8/16, powers of two: lines <= 256, "
+                                     "columns <= 64; planes >= 0)", i);
+    }
     cdd_plan* p = new cdd_plan();
+    p->tune.assign(n_inst, cdd_tuning{0, 0, 0, 0, 0});
+    if (tune) p->tune.assign(tune, tune + n_inst);
+    for (auto& t : p->tune)
+        if (!t.fft_radix) t.fft_radix = 16;
     PlanCore& C = p->core;
     C.n_inst = n_inst;
     C.precision = precision;
     const size_t elt = precision == CDD_F64 ? sizeof(double) : sizeof(float);
     p->desc.assign(inst, inst + n_inst);
     p->inst.resize(n_inst);
-    std::map<int, LinePlan> lp_done;   // line plans (with twiddle offsets) by length
+    std::map<int, LinePlan> lp_done;   // line plans (with twiddle offsets) by (length, largest radix)
     std::vector<double> twre, twim;
     std::vector<double> ktab;
     long long foff = 0, soff = 0, coff = 0, spoff = 0, rsoff = 0;
@@ -358,11 +408,12 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
         LinePlan* lps[3] = {&I.lp_last, &I.lp_mid, &I.lp_first};
         int lens[3] = {I.nl, I.nd == 3 ? I.n1 : I.n0, I.n0};
         for (int k = 0; k < 3; ++k) {
-            if (!make_line_plan(lens[k], *lps[k])) {
+            if (!make_line_plan(lens[k], *lps[k], p->tune[i].fft_radix)) {
                 free_plan(p);
                 return fail(CDD_ERR_SHAPE, "instance %d: no FFT plan for length %d", i, lens[k]);
             }
-            auto it = lp_done.find(lens[k]);
+            const int key = lens[k] * 32 + p->tune[i].fft_radix;
+            auto it = lp_done.find(key);
             if (it == lp_done.end()) {
                 lps[k]->tw = (int)twre.size();
                 for (int kk = 0; kk < lens[k]; ++kk) {
@@ -372,7 +423,7 @@ int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_pla
                     twim.push_back((double)im);
                 }
                 append_stage_twiddles(*lps[k], twre, twim);
-                it = lp_done.emplace(lens[k], *lps[k]).first;
+                it = lp_done.emplace(key, *lps[k]).first;
             }
             *lps[k] = it->second;
         }

@@ -924,11 +924,10 @@ cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st)
 template <typename T>
 static cudaError_t st_attr(size_t smem) {
     cudaError_t e;
-    int v = (int)smem;
-    if ((e = cudaFuncSetAttribute(k_stencil<T, M_FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_stencil<T, M_STAGE1>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(k_stencil<T, M_STAGE2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    return cudaFuncSetAttribute(k_stencil<T, M_STAGE3>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2>, smem))) return e;
+    return set_dyn_smem_limit(k_stencil<T, M_STAGE3>, smem);
 }
 
 cudaError_t stencil_set_attributes(int precision, size_t smem) {
@@ -941,7 +940,9 @@ size_t stencil_smem_bytes(int precision, bool any3d) {
     return (size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() * sizeof(double);
 }
 
-void stencil_geometry(InstDev& I) {
+// Blocks of the stencil: (x, y) tiles times chunks of planes along axis 0. Built-in rule: about
+// 1776 blocks (12 per SM); planes > 0 sets the chunk length instead.
+void stencil_geometry(InstDev& I, int planes) {
     const int nZ = (I.nd == 3) ? I.n0 : 1;
     const int nY = (I.nd == 3) ? I.n1 : I.n0;
     const int nX = (I.nd == 3) ? I.n2 : I.n1;
@@ -949,6 +950,7 @@ void stencil_geometry(InstDev& I) {
     int chunks = 1;
     if (I.nd == 3) {
         chunks = (1776 + tiles - 1) / tiles;
+        if (planes > 0) chunks = (nZ + planes - 1) / planes;
         if (chunks > nZ) chunks = nZ;
         if (chunks < 1) chunks = 1;
     }

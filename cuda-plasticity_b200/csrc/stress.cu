@@ -809,34 +809,19 @@ cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cuda
     return run_stress<double>(P, beta, sigma, phi, st);
 }
 
-// Raise a kernel's dynamic shared-memory limit to smem, clamped to what the device allows next to
-// the kernel's own static shared memory.
-template <typename F>
-static cudaError_t set_dyn_smem(F* fn, size_t smem) {
-    int dev = 0, optin = 0;
-    cudaError_t e;
-    if ((e = cudaGetDevice(&dev))) return e;
-    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
-    cudaFuncAttributes fa;
-    if ((e = cudaFuncGetAttributes(&fa, fn))) return e;
-    const long long lim = (long long)optin - (long long)fa.sharedSizeBytes;
-    const long long v = (long long)smem < lim ? (long long)smem : lim;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v);
-}
-
 template <typename T>
 static cudaError_t set_attr_t(size_t smem) {
     cudaError_t e;
-    if ((e = set_dyn_smem(k_r2c_rows<T, true>, smem))) return e;
-    if ((e = set_dyn_smem(k_r2c_rows<T, false>, smem))) return e;
-    if ((e = set_dyn_smem(k_c2r_rows<T, true>, smem))) return e;
-    if ((e = set_dyn_smem(k_c2r_rows<T, false>, smem))) return e;
-    if ((e = set_dyn_smem(k_fft_mid<T, true>, smem))) return e;
-    if ((e = set_dyn_smem(k_fft_mid<T, false>, smem))) return e;
-    if ((e = set_dyn_smem(k_green<T, true, 0>, smem))) return e;
-    if ((e = set_dyn_smem(k_green<T, false, 0>, smem))) return e;
-    if ((e = set_dyn_smem(k_green<T, false, 1>, smem))) return e;
-    if ((e = set_dyn_smem(k_green<T, false, 2>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_r2c_rows<T, true>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_r2c_rows<T, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_c2r_rows<T, true>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_c2r_rows<T, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_fft_mid<T, true>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_fft_mid<T, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, true, 0>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 0>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 1>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 2>, smem))) return e;
     return cudaSuccess;
 }
 

@@ -68,10 +68,31 @@ typedef struct cdd_instance {
 
 typedef struct cdd_plan cdd_plan;
 
+/* Per-instance launch-shape choices (no counterpart in the reference; the autotuner in
+ * cdd/autotune.py picks them by timing). 0 in a field keeps the built-in rule. Values that do
+ * not fit (not a power of two, shared memory over the device limit) are rejected with CDD_ERR_ARG.
+ * None changes the mathematics: results agree with the defaults to rounding. */
+typedef struct cdd_tuning {
+    int fft_radix;        /* largest radix of the FFT stage plans: 16 (built-in), 8 or 4 */
+    int rows_lines;       /* R2C / C2R passes: line pairs per block (power of two) */
+    int mid_cols;         /* axis-1 FFT pass (3-D): spectrum columns per block (power of two) */
+    int green_cols;       /* fused axis-0 FFT + Green pass: spectrum columns per block (power of two) */
+    int stencil_planes;   /* stencil (3-D): planes marched per block along axis 0 */
+} cdd_tuning;
+
 /* Create a plan for n_inst instances at the given precision on the current CUDA device.
  * Allocates all scratch. Replaces the per-run header generation + make of the reference's CUDA
  * path (Plasticity/RunCUDA.py L26-29, L194-214) and setupSystem (plasticity_kernel.cu L931-949). */
 int cdd_plan_create(const cdd_instance* inst, int n_inst, int precision, cdd_plan** out);
+
+/* cdd_plan_create with per-instance launch-shape choices (tune: n_inst entries, or NULL for the
+ * built-in rules). */
+int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, const cdd_tuning* tune,
+                          cdd_plan** out);
+
+/* The launch shapes a plan uses for instance i (the built-in rule's values where not tuned). */
+int cdd_plan_tuning(const cdd_plan* plan, int i, cdd_tuning* out);
+
 int cdd_plan_destroy(cdd_plan* plan);
 
 int cdd_plan_num_instances(const cdd_plan* plan);

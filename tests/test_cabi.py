@@ -74,3 +74,33 @@ def test_plan_create_rejects_bad_shapes_before_device_work():
             continue
         assert rc == _lib.CDD_ERR_SHAPE, shape
         assert not h.value
+
+
+def test_tuning_struct_layout_matches_ctypes(tmp_path):
+    from cdd import _lib
+    src = tmp_path / "tlayout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\n'
+                   'int main(void){printf("%%zu %%zu %%zu\\n", sizeof(cdd_tuning),'
+                   'offsetof(cdd_tuning, green_cols), offsetof(cdd_tuning, stencil_planes)); return 0;}\n' % HEADER)
+    exe = tmp_path / "tlayout"
+    subprocess.run(["gcc", "-std=c99", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    S = _lib.cdd_tuning
+    assert got == [ctypes.sizeof(S), S.green_cols.offset, S.stencil_planes.offset]
+
+
+def test_tuned_plan_rejects_bad_tuning_before_device_work():
+    from cdd import _lib
+    lib = _lib.load()
+    inst = _lib.cdd_instance()
+    inst.ndim = 3
+    for a in range(3):
+        inst.shape[a] = 16
+    inst.mu, inst.nu, inst.cfl = 1.0, 0.3, 0.25
+    for bad in [dict(fft_radix=32), dict(fft_radix=2), dict(mid_cols=12), dict(green_cols=128),
+                dict(rows_lines=3), dict(stencil_planes=-1)]:
+        t = _lib.cdd_tuning.from_dict(bad)
+        h = ctypes.c_void_p()
+        rc = lib.cdd_plan_create_tuned(ctypes.byref(inst), 1, _lib.CDD_F64, ctypes.byref(t), ctypes.byref(h))
+        assert rc == _lib.CDD_ERR_ARG, bad
+        assert "tuning" in lib.cdd_last_error().decode()
