@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=64, help="grid of the CPU baseline sample")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
     return ap.parse_args()
 
 
@@ -63,14 +64,14 @@ def ensemble_instances(seed):
     return out
 
 
-def run_ensemble(dev, K, W, seed):
+def run_ensemble(dev, K, W, seed, tuning):
     """Batched FP32 ensemble through one plan: every stage is one launch per kernel over all
     instances, per-instance dt, the whole step in a CUDA graph."""
     import torch
     import cdd
     from cdd.initial import gaussian_random_field_torch
     spec = ensemble_instances(seed)
-    plan = cdd.Plan([s[3] for s in spec], "f32")
+    plan = cdd.Plan([s[3] for s in spec], "f32", tuning=tuning)
     beta = plan.empty_field()
     for i, (sh, sig, sd, _inst) in enumerate(spec):
         plan.field_view(beta, i).copy_(gaussian_random_field_torch(sh, sig, 0.05, sd, device=dev))
@@ -94,7 +95,7 @@ def run_ensemble(dev, K, W, seed):
                         "rate_zz U[0,0.1] traceless; one plan, one CUDA graph per step"}
 
 
-def run_adjoint(dev, seed):
+def run_adjoint(dev, seed, tuning):
     """Adjoint cost: 64^3 FP32, 200 fixed-dt steps (dt from the step-0 CFL 0.25), checkpoints every
     20 steps; loss = elastic energy + 10 mean beta_zz; gradients for beta0, mu, nu, rate_zz.
     adj/fwd = reverse-sweep time (segment re-runs included) / forward time."""
@@ -110,7 +111,7 @@ def run_adjoint(dev, seed):
     dt = 0.25 / (64 * float(speed.max()))
     del probe, bp
     n = 200
-    ro = Rollout(shape, 1.0, 0.3, 0.05, dt, n, precision="f32", checkpoint_every=20)
+    ro = Rollout(shape, 1.0, 0.3, 0.05, dt, n, precision="f32", checkpoint_every=20, tuning=tuning)
     beta = ro.plan.pack([b0])
     ro.forward(beta)
     ro.backward()                      # warm-up (allocations, attributes)
@@ -321,11 +322,14 @@ def main():
 
     clocks.start()
     # ---------------- FP32 form (headline) ----------------
-    p32 = cdd.Plan([inst], "f32")
+    # launch shapes: the autotuner's choice for this GPU and shape (tuned before any timing)
+    tuning = None if args.no_tune else "auto"
+    p32 = cdd.Plan([inst], "f32", tuning=tuning)
     beta32 = p32.empty_field()
     beta32.copy_(b0.reshape(-1).to(torch.float32))
     p32.set_time(0.0, 1e30)
     p32.run(beta32, W, graph=True)
+    p32_tuning = p32.tuning(0)
     el32 = max_over_ranks(timed_run(p32, beta32, K))
     p32.check_status()
     rate32 = world * cells * 3 * K / el32
@@ -355,7 +359,7 @@ def main():
     fp64 = None
     err = None
     if not args.no_fp64:
-        p64 = cdd.Plan([inst], "f64")
+        p64 = cdd.Plan([inst], "f64", tuning=tuning)
         beta64 = p64.empty_field()
         beta64.copy_(b0.reshape(-1))
         p64.set_time(0.0, 1e30)
@@ -411,9 +415,9 @@ def main():
     adj = None
     ens = None
     if world == 1 and not args.no_adjoint:
-        adj = run_adjoint(dev, 5)
+        adj = run_adjoint(dev, 5, tuning)
     if world == 1 and not args.no_ensemble:
-        ens = run_ensemble(dev, max(3, min(K, 5)), W, 2024)
+        ens = run_ensemble(dev, max(3, min(K, 5)), W, 2024, tuning)
 
     if world > 1:
         dist.barrier()
@@ -435,7 +439,8 @@ def main():
                    "grid": list(shape), "mu": 1.0, "nu": 0.3, "cfl": 0.25, "Lambda": 0.0,
                    "strain_rate": [-0.025, -0.025, 0.05], "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (FP32 field %.0f MB)" % (9 * cells * 4 / 1e6),
-                   "timing": "CUDA graph of whole steps, CUDA events, max over ranks"},
+                   "timing": "CUDA graph of whole steps, CUDA events, max over ranks",
+                   "launch_shapes": p32_tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "kernel": "one RK3 stage (stress FFT passes + stencil/stage kernel)",

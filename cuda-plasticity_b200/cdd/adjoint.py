@@ -56,7 +56,8 @@ class Rollout:
     """Fixed-dt trajectory of one instance with its adjoint.
 
     shape, mu, nu: grid and material; rate_zz: r of the traceless applied strain rate
-    r (-1/2, -1/2, 1) (None: no load); dt: fixed step; precision "f64" or "f32".
+    r (-1/2, -1/2, 1) (None: no load); dt: fixed step; precision "f64" or "f32"; tuning: launch
+    shapes as for ``cdd.Plan`` (None, [dict] or "auto").
     The forward keeps a copy of the state every ``checkpoint_every`` steps; the reverse sweep
     re-runs each segment from its checkpoint with cdd_step_record (saving stage states, stresses
     and k-space data) and walks it backwards with cdd_step_adjoint. Nothing synchronises the host
@@ -64,7 +65,7 @@ class Rollout:
     """
 
     def __init__(self, shape, mu, nu, rate_zz, dt, n_steps, precision="f32", checkpoint_every=20,
-                 t0=0.0, w_zz=10.0, Lambda=0.0):
+                 t0=0.0, w_zz=10.0, Lambda=0.0, tuning=None):
         self.shape = tuple(shape)
         self.mu, self.nu = float(mu), float(nu)
         self.rate_zz = None if rate_zz is None else float(rate_zz)
@@ -74,7 +75,7 @@ class Rollout:
         load = None if rate_zz is None else tuple(self.rate_zz * CZZ)
         self.inst = Instance(self.shape, mu=self.mu, nu=self.nu, Lambda=Lambda, cfl=0.25, load_rate=load,
                              load_t0=self.t0)
-        self.plan = Plan([self.inst], precision)
+        self.plan = Plan([self.inst], precision, tuning=tuning)
         self.lib = self.plan.lib
         self.cells = int(np.prod(self.shape))
         self.checkpoints = {}

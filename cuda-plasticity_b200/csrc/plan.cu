@@ -344,12 +344,12 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
     for (int i = 0; tune && i < n_inst; ++i) {
         const cdd_tuning& t = tune[i];
         if ((t.fft_radix && t.fft_radix != 4 && t.fft_radix != 8 && t.fft_radix != 16) ||
-            (t.rows_lines && (!pow2(t.rows_lines) || t.rows_lines > 256)) ||
+            (t.rows_lines && t.rows_lines > 1024) ||
             (t.mid_cols && (!pow2(t.mid_cols) || t.mid_cols > 64)) ||
             (t.green_cols && (!pow2(t.green_cols) || t.green_cols > 64)) || t.stencil_planes < 0 ||
             t.fft_radix < 0 || t.rows_lines < 0 || t.mid_cols < 0 || t.green_cols < 0)
-            return fail(CDD_ERR_ARG, "instance %d: bad tuning (radix 4/8/16, powers of two: lines <= 256, "
-                                     "columns <= 64; planes >= 0)", i);
+            return fail(CDD_ERR_ARG, "instance %d: bad tuning (radix 4/8/16; lines <= 1024; columns: powers of "
+                                     "two <= 64; planes >= 0)", i);
     }
     cdd_plan* p = new cdd_plan();
     p->tune.assign(n_inst, cdd_tuning{0, 0, 0, 0, 0});

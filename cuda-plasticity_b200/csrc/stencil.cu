@@ -644,7 +644,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
                 arrive(k + 5);
             } else {
                 __syncthreads();
-                load_box(k % NS, wrapz(z + 3), true);
+                load_box((k + 5) % NS, wrapz(z + 3), true);   // plane pr = k + 5 lives in slot pr % NS
             }
             __syncthreads();
         }
@@ -941,7 +941,8 @@ size_t stencil_smem_bytes(int precision, bool any3d) {
 }
 
 // Blocks of the stencil: (x, y) tiles times chunks of planes along axis 0. Built-in rule: about
-// 1776 blocks (12 per SM); planes > 0 sets the chunk length instead.
+// 1776 blocks (12 per SM) but at least 8 planes per block (each block first stages a 4-plane
+// halo, so shorter chunks spend most of their time on it); planes > 0 sets the chunk length.
 void stencil_geometry(InstDev& I, int planes) {
     const int nZ = (I.nd == 3) ? I.n0 : 1;
     const int nY = (I.nd == 3) ? I.n1 : I.n0;
@@ -950,6 +951,7 @@ void stencil_geometry(InstDev& I, int planes) {
     int chunks = 1;
     if (I.nd == 3) {
         chunks = (1776 + tiles - 1) / tiles;
+        if (chunks > nZ / 8) chunks = nZ / 8;
         if (planes > 0) chunks = (nZ + planes - 1) / planes;
         if (chunks > nZ) chunks = nZ;
         if (chunks < 1) chunks = 1;

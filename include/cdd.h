@@ -69,12 +69,12 @@ typedef struct cdd_instance {
 typedef struct cdd_plan cdd_plan;
 
 /* Per-instance launch-shape choices (no counterpart in the reference; the autotuner in
- * cdd/autotune.py picks them by timing). 0 in a field keeps the built-in rule. Values that do
- * not fit (not a power of two, shared memory over the device limit) are rejected with CDD_ERR_ARG.
+ * cdd/autotune.py picks them by timing). 0 in a field keeps the built-in rule. Values out of range
+ * (column counts not powers of two, shared memory over the device limit) give CDD_ERR_ARG.
  * None changes the mathematics: results agree with the defaults to rounding. */
 typedef struct cdd_tuning {
     int fft_radix;        /* largest radix of the FFT stage plans: 16 (built-in), 8 or 4 */
-    int rows_lines;       /* R2C / C2R passes: line pairs per block (power of two) */
+    int rows_lines;       /* R2C / C2R passes: line pairs per block (<= 1024) */
     int mid_cols;         /* axis-1 FFT pass (3-D): spectrum columns per block (power of two) */
     int green_cols;       /* fused axis-0 FFT + Green pass: spectrum columns per block (power of two) */
     int stencil_planes;   /* stencil (3-D): planes marched per block along axis 0 */

@@ -98,7 +98,7 @@ def test_tuned_plan_rejects_bad_tuning_before_device_work():
         inst.shape[a] = 16
     inst.mu, inst.nu, inst.cfl = 1.0, 0.3, 0.25
     for bad in [dict(fft_radix=32), dict(fft_radix=2), dict(mid_cols=12), dict(green_cols=128),
-                dict(rows_lines=3), dict(stencil_planes=-1)]:
+                dict(rows_lines=5000), dict(stencil_planes=-1)]:
         t = _lib.cdd_tuning.from_dict(bad)
         h = ctypes.c_void_p()
         rc = lib.cdd_plan_create_tuned(ctypes.byref(inst), 1, _lib.CDD_F64, ctypes.byref(t), ctypes.byref(h))
