@@ -27,8 +27,9 @@ sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
 METRIC = "cell-stage updates/s at 256³: FP32 batched vs FP64 plain (≤1e-5 rel-L2); adj/fwd"
 UNIT = "cell-stage updates/s"
 WORDS_PER_CELL_STAGE = 48      # stress operator: read 9 + write 6; stencil + stage: read 24, write 9
-STRESS_WORDS = 15
-STENCIL_WORDS = 33
+STRESS_WORDS = 15               # stress operator: read beta 9, write sigma 6
+FLUX_WORDS = 24                 # stencil, flux form: read beta 9 + sigma 6, write rhs 9
+FLUX_TRAFFIC_BYTES_PER_CELL = 117.1   # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
 
 
 def parse():
@@ -44,6 +45,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
+    ap.add_argument("--only-flux", action="store_true",
+                    help="run three flux evaluations of the workload and exit (for profiling the stencil)")
     return ap.parse_args()
 
 
@@ -320,6 +323,16 @@ def main():
         barrier()
         return ev0.elapsed_time(ev1) / 1e3
 
+    if args.only_flux:
+        p = cdd.Plan([inst], "f32", tuning=None if args.no_tune else "auto")
+        b = p.empty_field()
+        b.copy_(b0.reshape(-1).to(torch.float32))
+        for _ in range(3):
+            p.flux(b, 0.0, want_speed=False)
+        torch.cuda.synchronize()
+        print(json.dumps({"only_flux": True, "grid": list(shape), "launch_shapes": p.tuning(0)}))
+        return
+
     clocks.start()
     # ---------------- FP32 form (headline) ----------------
     # launch shapes: the autotuner's choice for this GPU and shape (tuned before any timing)
@@ -335,25 +348,27 @@ def main():
     rate32 = world * cells * 3 * K / el32
     ms32 = 1e3 * el32 / K
 
-    # per-operator times (eager launches, CUDA events on the launching stream)
+    # per-operator times (eager launches, CUDA events on the launching stream): the stress solve
+    # (cdd_stress) and the stencil kernel alone (cdd_flux_with_stress on that stress)
     st = torch.cuda.current_stream()
     M = 5
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     s6 = p32.empty_stress()
+    rhs32 = p32.empty_field()
     p32.stress(beta32, out=s6)
-    p32.flux(beta32)
+    p32.flux(beta32, want_speed=False, sigma=s6, out=rhs32)
     torch.cuda.synchronize()
     e0.record(st)
     for _ in range(M):
         p32.stress(beta32, out=s6)
     e1.record(st)
     for _ in range(M):
-        p32.flux(beta32, want_speed=False)
+        p32.flux(beta32, want_speed=False, sigma=s6, out=rhs32)
     e2.record(st)
     torch.cuda.synchronize()
     t_stress = e0.elapsed_time(e1) / 1e3 / M
-    t_flux = e1.elapsed_time(e2) / 1e3 / M
-    t_stencil = max(t_flux - t_stress, 1e-9)
+    t_stencil = e1.elapsed_time(e2) / 1e3 / M
+    del rhs32
 
     # ---------------- FP64 plain form and FP32 error ----------------
     fp64 = None
@@ -441,15 +456,22 @@ def main():
                    "l2": "inputs larger than L2 (FP32 field %.0f MB)" % (9 * cells * 4 / 1e6),
                    "timing": "CUDA graph of whole steps, CUDA events, max over ranks",
                    "launch_shapes": p32_tuning},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "kernel": "one RK3 stage (stress FFT passes + stencil/stage kernel)",
-                     "algorithmic_bytes_per_cell_stage": WORDS_PER_CELL_STAGE * 4,
-                     "traffic": None,
+        # dominant kernel: k_stencil (≈47% of a step in the launch list), timed alone here in its
+        # flux form; algorithmic bytes per launch = 24 words per cell (read beta 9 + stress 6,
+        # write rhs 9); traffic = DRAM bytes per cell from one ncu capture at 192^3, scaled by cells
+        "roofline": {"bound": "hbm", "kernel": "k_stencil (flux evaluation, cdd_flux_with_stress)",
+                     "achieved": FLUX_WORDS * 4 * cells / t_stencil / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": FLUX_WORDS * 4 * cells / t_stencil / 1e9 / peak, "peak_kind": peak_kind,
+                     "launch_ms": 1e3 * t_stencil,
+                     "algorithmic_bytes_per_launch": FLUX_WORDS * 4 * cells,
+                     "traffic": FLUX_TRAFFIC_BYTES_PER_CELL * cells,
+                     "traffic_source": "profiles/k_stencil_flux_192cube_fp32.md (117.1 B/cell at 192^3, scaled)",
+                     "step": {"achieved": achieved, "frac": achieved / peak,
+                              "algorithmic_bytes_per_cell_stage": WORDS_PER_CELL_STAGE * 4},
                      "per_operator": {
                          "stress_fft": {"ms": 1e3 * t_stress, "GBps": STRESS_WORDS * 4 * cells / t_stress / 1e9},
-                         "stencil_stage": {"ms": 1e3 * t_stencil,
-                                           "GBps": STENCIL_WORDS * 4 * cells / t_stencil / 1e9}}},
+                         "stencil_flux": {"ms": 1e3 * t_stencil,
+                                          "GBps": FLUX_WORDS * 4 * cells / t_stencil / 1e9}}},
         "gpu_launches": launches_per_step * K,
         "e2e": e2e,
         "clocks": clk,

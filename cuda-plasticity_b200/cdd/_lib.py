@@ -109,6 +109,8 @@ _PROTOS = {
                                        ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_step_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_flux_with_stress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,

@@ -165,15 +165,23 @@ class Plan:
                                   ctypes.c_void_p(out.data_ptr()), _stream(stream)))
         return out
 
-    def flux(self, beta, t=0.0, want_speed=True, stream=None):
-        """(rhs, speed) of the central-upwind flux at time t; speed is one value per cell."""
+    def flux(self, beta, t=0.0, want_speed=True, stream=None, sigma=None, out=None):
+        """(rhs, speed) of the central-upwind flux at time t; speed is one value per cell.
+        sigma: a packed 6-component internal stress to use instead of computing it (the applied
+        load of time t is still added); out: a packed field to write rhs into."""
         self._check_field(beta)
-        rhs = self.empty_field()
+        rhs = self.empty_field() if out is None else out
         speed = torch.empty(self.total_cells, dtype=self.dtype, device=self.device) if want_speed else None
-        check(self.lib.cdd_flux(self.handle, ctypes.c_void_p(beta.data_ptr()), float(t),
-                                ctypes.c_void_p(rhs.data_ptr()),
-                                ctypes.c_void_p(speed.data_ptr() if speed is not None else 0),
-                                _stream(stream)))
+        sp = ctypes.c_void_p(speed.data_ptr() if speed is not None else 0)
+        if sigma is None:
+            check(self.lib.cdd_flux(self.handle, ctypes.c_void_p(beta.data_ptr()), float(t),
+                                    ctypes.c_void_p(rhs.data_ptr()), sp, _stream(stream)))
+        else:
+            if sigma.numel() != self.stress_elems or sigma.dtype != self.dtype:
+                raise ValueError("sigma must be a packed stress of this plan")
+            check(self.lib.cdd_flux_with_stress(self.handle, ctypes.c_void_p(beta.data_ptr()),
+                                                ctypes.c_void_p(sigma.data_ptr()), float(t),
+                                                ctypes.c_void_p(rhs.data_ptr()), sp, _stream(stream)))
         return rhs, speed
 
     def set_time(self, t=None, t_end=None):

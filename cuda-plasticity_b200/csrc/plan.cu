@@ -571,6 +571,16 @@ int cdd_flux(cdd_plan* p, const void* beta, double t, void* rhs, void* speed, vo
     return CDD_OK;
 }
 
+int cdd_flux_with_stress(cdd_plan* p, const void* beta, const void* sigma6, double t, void* rhs, void* speed,
+                         void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !sigma6 || !rhs) return fail(CDD_ERR_ARG, "null buffer");
+    PlanCore K = p->core;
+    K.d_sigma = const_cast<void*>(sigma6);
+    CDD_CUDA(launch_stencil(K, M_FLUX, beta, beta, rhs, speed, t, user_maps(p, beta), (cudaStream_t)stream));
+    return CDD_OK;
+}
+
 int cdd_set_time(cdd_plan* p, const double* t, const double* t_end) {
     if (int rc = check_plan(p)) return rc;
     const int n = p->core.n_inst;

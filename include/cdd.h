@@ -124,6 +124,13 @@ int cdd_stress(cdd_plan* plan, const void* beta, void* sigma6, void* stream);
  * sum of previous cells), may be NULL. */
 int cdd_flux(cdd_plan* plan, const void* beta, double t, void* rhs, void* speed, void* stream);
 
+/* cdd_flux with the internal stress given by the caller (packed 6-component sigma6, e.g. from
+ * cdd_stress or from another stress model); the applied load of time t is still added. The
+ * reference's dynamics take their stress from an overridable GetSigma (RunPython.py L35-50);
+ * this is that seam. Launches only the stencil kernel. */
+int cdd_flux_with_stress(cdd_plan* plan, const void* beta, const void* sigma6, double t, void* rhs, void* speed,
+                         void* stream);
+
 /* Per-instance clocks: t (current time) and t_end (end of the current Run interval).
  * Host arrays of length n_inst. */
 int cdd_set_time(cdd_plan* plan, const double* t, const double* t_end);

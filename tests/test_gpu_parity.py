@@ -282,3 +282,19 @@ def test_tma_fp32_matches_fp64_and_batch_mixes_paths():
         assert torch.equal(single.field_view(bs, 0), p64.field_view(b64, i))
     p64.check_status()
     p32.check_status()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_flux_with_given_stress_equals_flux(prec):
+    """cdd_flux_with_stress on the plan's own stress reproduces cdd_flux bitwise (load included);
+    a scaled stress gives a different flux."""
+    shape = (16, 24, 48)
+    b0 = cdd.gaussian_random_field(shape, 0.05, 0.05, 9)
+    plan = cdd.Plan([cdd.Instance(shape, load_rate=(-0.025, -0.025, 0.05))], prec)
+    beta = plan.pack([b0])
+    rhs, speed = plan.flux(beta, 0.3)
+    s6 = plan.stress(beta)
+    rhs2, speed2 = plan.flux(beta, 0.3, sigma=s6)
+    assert torch.equal(rhs, rhs2) and torch.equal(speed, speed2)
+    rhs3, _ = plan.flux(beta, 0.3, sigma=2 * s6)
+    assert not torch.equal(rhs, rhs3)
