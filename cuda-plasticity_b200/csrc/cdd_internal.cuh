@@ -80,6 +80,35 @@ inline void append_stage_twiddles(LinePlan& lp, std::vector<double>& re, std::ve
     lp.twspan = (int)re.size() - lp.twst[0];
 }
 
+// ---- asynchronous global -> shared copies (cp.async, 16 bytes, zero fill) ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stage a column tile of complex values: rows x 2^lgw columns of a row-major array (row stride
+// `stride` elements, columns w >= wv are padding: read as zero) into dst[(e << lgw) + w], with
+// 16-byte asynchronous copies. Needs 2^lgw x sizeof(V) >= 16 and 16-byte aligned rows in both
+// spaces. The caller waits (cp_async_wait_all) and synchronises the block before use.
+template <typename V>
+__device__ __forceinline__ void tile_async_load(V* dst, const V* src, long long stride, int rows, int lgw, int wv,
+                                                int tid, int nt) {
+    constexpr int PER = 16 / (int)sizeof(V);   // complex values per copy: 2 (FP32) or 1 (FP64)
+    const int W = 1 << lgw;
+    const int chunks = (rows << lgw) / PER;
+#pragma unroll 4
+    for (int q = tid; q < chunks; q += nt) {
+        const int i = q * PER;
+        const int e = i >> lgw, w = i & (W - 1);
+        int valid = wv - w;
+        valid = valid < 0 ? 0 : (valid > PER ? PER : valid);
+        cp_async16(dst + i, valid ? (const void*)(src + (long long)e * stride + w) : (const void*)src,
+                   valid * (int)sizeof(V));
+    }
+}
+
 // Copy the twiddle rows of lp (global table tw) into shared memory at dst (16-byte aligned);
 // fft_lines then reads them with rebase = lp.twst[0]. The caller synchronises before use.
 template <typename V>

@@ -344,15 +344,20 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int wv = min(W, nh - col0);
     const int tid = threadIdx.x, nt = blockDim.x;
     V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+    if (W * (int)sizeof(V) >= 16) {
+        tile_async_load(s, base, nhp, N, lgw, wv, tid, nt);
+    } else {
 #pragma unroll 8
-    for (int i = tid; i < N * W; i += nt) {
-        const int e = i >> lgw, w = i & (W - 1);
-        V z; z.x = 0; z.y = 0;
-        if (w < wv) z = base[(long long)e * nhp + w];
-        s[i] = z;
+        for (int i = tid; i < N * W; i += nt) {
+            const int e = i >> lgw, w = i & (W - 1);
+            V z; z.x = 0; z.y = 0;
+            if (w < wv) z = base[(long long)e * nhp + w];
+            s[i] = z;
+        }
     }
     V* tws = s + 2 * N * W;
     stage_tw_to_smem(I.lp_mid, tw, tws, tid, nt);
+    cp_async_wait_all();
     __syncthreads();
     ColLayout<1> lay{lgw, 0};
     s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tws, tid, nt, I.lp_mid.twst[0]);
@@ -589,18 +594,24 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     // sym(beta) (1), sym(beta) -> d sigma / d nu (2); all symmetric, 6 components
     constexpr int NIN = 6;
     constexpr int NOUT = 6;
+    if (W * (int)sizeof(V) >= 16) {
 #pragma unroll 1
-    for (int c = 0; c < NIN; ++c) {
+        for (int c = 0; c < NIN; ++c) tile_async_load(s + c * cs, base + c * cstride, estride, N, lgw, wv, tid, nt);
+    } else {
+#pragma unroll 1
+        for (int c = 0; c < NIN; ++c) {
 #pragma unroll 8
-        for (int rem = tid; rem < N * W; rem += nt) {
-            const int e = rem >> lgw, w = rem & (W - 1);
-            V z; z.x = 0; z.y = 0;
-            if (w < wv) z = base[c * cstride + e * estride + w];
-            s[c * cs + rem] = z;
+            for (int rem = tid; rem < N * W; rem += nt) {
+                const int e = rem >> lgw, w = rem & (W - 1);
+                V z; z.x = 0; z.y = 0;
+                if (w < wv) z = base[c * cstride + e * estride + w];
+                s[c * cs + rem] = z;
+            }
         }
     }
     V* tws = s + ((9 * cs + 1) & ~1);   // twiddle rows after the 9 slots
     stage_tw_to_smem(I.lp_first, tw, tws, tid, nt);
+    cp_async_wait_all();
     __syncthreads();
     for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
     // Green contraction, one k point per thread iteration
