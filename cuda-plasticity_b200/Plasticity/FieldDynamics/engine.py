@@ -27,20 +27,20 @@ class FacadePlan(cdd.Plan):
         return t.reshape(-1)
 
 
-def plan_for(gridShape, mu, nu, Lambda=0.0, cfl=0.25, load=None, precision=None):
-    """load: None or (rate[3], initial[3], t0, load_mu, load_nu)."""
+def plan_for(gridShape, mu, nu, Lambda=0.0, cfl=0.25, load=None, precision=None, glide=False):
+    """load: None or (rate[3], initial[3], t0, load_mu, load_nu); glide: glide-only dynamics."""
     precision = precision or _PRECISION
     key = (tuple(gridShape), float(mu), float(nu), float(Lambda), float(cfl),
            None if load is None else (tuple(load[0]), tuple(load[1]), float(load[2]), float(load[3]),
-                                      float(load[4])), precision)
+                                      float(load[4])), precision, bool(glide))
     p = _PLANS.get(key)
     if p is None:
         if load is None:
-            inst = cdd.Instance(tuple(gridShape), mu=mu, nu=nu, Lambda=Lambda, cfl=cfl)
+            inst = cdd.Instance(tuple(gridShape), mu=mu, nu=nu, Lambda=Lambda, cfl=cfl, glide_only=glide)
         else:
             inst = cdd.Instance(tuple(gridShape), mu=mu, nu=nu, Lambda=Lambda, cfl=cfl,
                                 load_rate=tuple(load[0]), load_initial=tuple(load[1]), load_t0=load[2],
-                                load_mu=load[3], load_nu=load[4])
+                                load_mu=load[3], load_nu=load[4], glide_only=glide)
         p = FacadePlan([inst], precision)
         _PLANS[key] = p
     return p

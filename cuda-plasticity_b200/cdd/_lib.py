@@ -38,7 +38,11 @@ class cdd_instance(ctypes.Structure):
         ("load_t0", ctypes.c_double),
         ("load_mu", ctypes.c_double),
         ("load_nu", ctypes.c_double),
+        ("dynamics", ctypes.c_int),
     ]
+
+
+CDD_DYN_GLIDE_CLIMB, CDD_DYN_GLIDE_ONLY = 0, 1
 
 
 class cdd_tuning(ctypes.Structure):

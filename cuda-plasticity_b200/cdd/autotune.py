@@ -86,7 +86,7 @@ def tune(inst, precision, reps=5, sweeps=2, verbose=False):
     from .engine import Instance, Plan
     from .initial import gaussian_random_field_torch
     one = Instance(tuple(inst.shape), mu=inst.mu, nu=inst.nu, Lambda=inst.Lambda, cfl=inst.cfl,
-                   load_rate=inst.load_rate)
+                   load_rate=inst.load_rate, glide_only=inst.glide_only)
     field = gaussian_random_field_torch(tuple(inst.shape), 0.04, 0.05, 7, device="cuda")
     tried = {}
 
@@ -132,7 +132,7 @@ def best(inst, precision, use_cache=True, verbose=False):
     """The tuned launch shapes of inst (a cdd.Instance) at precision, from the cache or by tuning."""
     import torch
     gpu = torch.cuda.get_device_name()
-    key = cache_key(gpu, precision, inst.shape)
+    key = cache_key(gpu, precision + ("-glide" if inst.glide_only else ""), inst.shape)
     cache = load_cache() if use_cache else {}
     if key in cache:
         return dict(cache[key]["tuning"])

@@ -28,6 +28,7 @@ class Instance:
     load_t0: float = 0.0
     load_mu: Optional[float] = None
     load_nu: Optional[float] = None
+    glide_only: bool = False   # the glide-only dynamics (CentralUpwindHJBetaPGlideOnlyDynamics.py)
 
     def to_c(self):
         c = _lib.cdd_instance()
@@ -44,6 +45,7 @@ class Instance:
         c.load_t0 = float(self.load_t0)
         c.load_mu = float(self.mu if self.load_mu is None else self.load_mu)
         c.load_nu = float(self.nu if self.load_nu is None else self.load_nu)
+        c.dynamics = _lib.CDD_DYN_GLIDE_ONLY if self.glide_only else _lib.CDD_DYN_GLIDE_CLIMB
         return c
 
     @property

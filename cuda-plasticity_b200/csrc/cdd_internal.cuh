@@ -158,6 +158,7 @@ struct InstDev {
     double inv_cells;
     int has_load;
     double load_rate[3], load_init[3], load_t0, load_lamb, load_mu;
+    int glide;              // glide-only dynamics (projected velocity)
 };
 
 // Per-instance clock and reduction results kept on the device.
@@ -454,6 +455,7 @@ struct PlanCore {
     int precision = CDD_F64;
     int max_nd = 3;
     bool any3d = false;
+    bool any_glide = false;          // some instance uses the glide-only dynamics
     long long field_elems = 0, stress_elems = 0, cells = 0, spec_elems = 0, rows_total = 0;
     InstDev* d_inst = nullptr;       // device copy of the instance table
     InstClock* d_clock = nullptr;

@@ -389,6 +389,14 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
             free_plan(p);
             return fail(CDD_ERR_ARG, "instance %d: need mu > 0, -1 < nu < 0.5, cfl > 0", i);
         }
+        if (d.dynamics != CDD_DYN_GLIDE_CLIMB && d.dynamics != CDD_DYN_GLIDE_ONLY) {
+            free_plan(p);
+            return fail(CDD_ERR_ARG, "instance %d: unknown dynamics %d", i, d.dynamics);
+        }
+        if (d.dynamics == CDD_DYN_GLIDE_ONLY && d.Lambda != 0.0) {
+            free_plan(p);
+            return fail(CDD_ERR_ARG, "instance %d: the glide-only dynamics takes no Lambda", i);
+        }
         I.nd = d.ndim;
         I.n0 = sh[0]; I.n1 = sh[1]; I.n2 = sh[2];
         if (I.nd == 3) C.any3d = true;
@@ -444,6 +452,8 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
         }
         I.mu = d.mu;
         I.nu = d.nu;
+        I.glide = (d.dynamics == CDD_DYN_GLIDE_ONLY) ? 1 : 0;
+        if (I.glide) C.any_glide = true;
         I.lamb = 2. * d.mu * d.nu / (1. - 2. * d.nu);
         I.Lambda = d.Lambda;
         I.cfl = d.cfl;
@@ -665,6 +675,12 @@ int cdd_observables(cdd_plan* p, const void* beta, double* energy, double* mean_
 }
 
 namespace {
+int check_adjoint_supported(const cdd_plan* p) {
+    for (int i = 0; i < p->core.n_inst; ++i)
+        if (p->inst[i].glide) return fail(CDD_ERR_UNSUPPORTED, "instance %d: no adjoint of the glide-only dynamics", i);
+    return CDD_OK;
+}
+
 int ensure_adjoint_scratch(cdd_plan* p) {
     PlanCore& C = p->core;
     if (C.d_ubar) return CDD_OK;
@@ -711,6 +727,7 @@ RecLayout rec_layout(const PlanCore& C) {
 int cdd_flux_vjp(cdd_plan* p, const void* beta, double t, const void* gbar, void* betabar, void* sigbar6,
                  double* load_bar, void* stream) {
     if (int rc = check_plan(p)) return rc;
+    if (int rc = check_adjoint_supported(p)) return rc;
     if (!beta || !gbar || !betabar || !sigbar6) return fail(CDD_ERR_ARG, "null buffer");
     if (int rc = ensure_adjoint_scratch(p)) return rc;
     CDD_CUDA(launch_flux_vjp(p->core, beta, t, gbar, sigbar6, betabar, load_bar, (cudaStream_t)stream));
@@ -719,6 +736,7 @@ int cdd_flux_vjp(cdd_plan* p, const void* beta, double t, const void* gbar, void
 
 int cdd_flux_branches(cdd_plan* p, const void* beta, double t, uint32_t* flags, void* stream) {
     if (int rc = check_plan(p)) return rc;
+    if (int rc = check_adjoint_supported(p)) return rc;
     if (!beta || !flags) return fail(CDD_ERR_ARG, "null buffer");
     if (int rc = ensure_adjoint_scratch(p)) return rc;
     CDD_CUDA(launch_flux_branches(p->core, beta, t, flags, (cudaStream_t)stream));
@@ -787,6 +805,7 @@ int cdd_step_record(cdd_plan* p, void* beta, double t, double dt, void* rec, voi
 
 int cdd_step_adjoint(cdd_plan* p, const void* rec, double t, double dt, void* ubar, double* pbar, void* stream) {
     if (int rc = check_plan(p)) return rc;
+    if (int rc = check_adjoint_supported(p)) return rc;
     if (!rec || !ubar) return fail(CDD_ERR_ARG, "null buffer");
     if (int rc = ensure_adjoint_scratch(p)) return rc;
     cudaStream_t st = (cudaStream_t)stream;

@@ -186,7 +186,7 @@ __device__ __forceinline__ StageConst stage_const(const InstDev& I, const InstCl
     return k;
 }
 
-template <typename T, int ND, int MODE>
+template <typename T, int ND, int MODE, bool GLIDE>
 __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, bool valid,
                                              const TileView<T, ND>& tv, const T* bn, T* out,
                                              const T* __restrict__ sig, T* __restrict__ speed_out,
@@ -226,6 +226,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
         S[1][2] = S[2][1] = s6[4];
     }
     const bool lam_on = (I.Lambda != 0.0);
+    const bool glide = GLIDE && (I.glide != 0);   // glide-only dynamics (Lambda is 0 then)
     const T str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / (T)3 * (T)I.Lambda : (T)0;
 
     // ---------------- pass 1: A, P, C, trace ----------------
@@ -251,6 +252,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
     // from shared memory (register budget).
     constexpr bool KEEPU = (sizeof(T) == 4);
     T Ukeep[KEEPU ? ND : 1][2][9];
+    T Dv[(KEEPU || !GLIDE) ? 1 : ND][2][3];   // glide-only, FP64: (u_e)_{d e} per axis e and sign
     if constexpr (KEEPU) {
         // all derivatives first (shared memory only), so that the stress loads issued above have
         // the whole derivative evaluation to arrive before the first use
@@ -300,16 +302,25 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
                     Sd[d][s] += v * Sj[l];
                     if (l != d) Pq[d][s] += v * v;
                 }
-                if (lam_on) {
-                    // trace of u_d (components (j, j)) and the -str (u_d)_{l d} terms
+                if (lam_on || glide) {
+                    // trace of u_d (components (j, j))
                     T dj = (j == 0) ? U[d][s][0] : ((j == 1) ? U[d][s][1] : U[d][s][2]);
                     trU[d][s] += dj;
-                    if (j == d) {
+                }
+                if (lam_on && j == d) {
+                    // the -str (u_d)_{l d} terms
 #pragma unroll
-                        for (int l = 0; l < 3; ++l) A[d][s][l] -= str * U[d][s][l];
-                    }
+                    for (int l = 0; l < 3; ++l) A[d][s][l] -= str * U[d][s][l];
                 }
             }
+        if constexpr (!KEEPU && GLIDE) {
+            if (glide && j < ND) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+#pragma unroll
+                    for (int l = 0; l < 3; ++l) Dv[j % ND][s][l] = U[j % ND][s][l];
+            }
+        }
         // pair terms C_de[s_d][s_e] = sum_j (u_d)_ej (u_e)_dj
 #pragma unroll
         for (int a = 0; a < 2; ++a)
@@ -346,12 +357,37 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
         else
             rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] - (T)2 * Cp[0][sx][sy];
         T inv = inv_sqrt(rho2);
+        T av[3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
             T a = A[0][sx][l] + A[1][sy][l];
             if (ND == 3) a += A[2 % ND][sz][l];
-            V[c][l] = a * inv;
+            av[l] = a;
         }
+        if (glide) {
+            // glide-only projection (CentralUpwindHJBetaPGlideOnlyDynamics.py L152-201, 2-D L96-129):
+            // g_d = tr(u_d) - sum_e (u_e)_{d e}, v += g (ME + v.g) / (ME + g.g), then v / |rho|
+            const int sgc[3] = {sx, sy, sz};
+            T gv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                T Dd = (T)0;
+#pragma unroll
+                for (int e = 0; e < ND; ++e) {
+                    if constexpr (KEEPU) Dd += Ukeep[e][sgc[e]][3 * d + e];
+                    else if constexpr (GLIDE) Dd += Dv[e][sgc[e]][d];
+                }
+                const T tr = (d < ND) ? trU[d % ND][sgc[d]] : (T)0;
+                gv[d] = tr - Dd;
+            }
+            const T rr = (T)ME + gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
+            const T rv = (T)ME + av[0] * gv[0] + av[1] * gv[1] + av[2] * gv[2];
+            const T f = fdiv(rv, rr);
+#pragma unroll
+            for (int l = 0; l < 3; ++l) av[l] += gv[l] * f;
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) V[c][l] = av[l] * inv;
     }
     T pp[ND], pm[ND], tot[ND];
     T vsum = 0;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
@@ -520,7 +556,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
 // grid read zeros, and tiles whose box crosses the periodic boundary patch those cells with
 // wrapped loads after the copy lands. FP32 (6 slots) prefetches plane z+3 while computing z;
 // FP64 (5 slots) refills the slot of z-2 after computing z. Otherwise threads load the box.
-template <typename T, int ND, int MODE>
+template <typename T, int ND, int MODE, bool GLIDE>
 __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, double* red, uint64_t* bars,
                                       const StencilMapSet& maps,
                                       const T* __restrict__ bs, const T* bn, T* out,
@@ -629,7 +665,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             tv.so[2] = 0;
         }
         const long long cl = ((long long)z * nY + y) * nX + x;
-        stencil_cell<T, ND, MODE>(I, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, kc, clk[ii], t_flux, vmax,
+        stencil_cell<T, ND, MODE, GLIDE>(I, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, kc, clk[ii], t_flux, vmax,
                                   esum, zsum);
         if (ND == 3 && more) {
             if (use_tma) {
@@ -667,7 +703,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     }
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, bool GLIDE>
 __global__ void __launch_bounds__(ST_THREADS, (sizeof(T) == 4) ? 3 : 2)
 k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre,
           const T* __restrict__ bs, const T* bn, T* out, const T* __restrict__ sig,
@@ -682,10 +718,10 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     if (I.nd == 3)
-        march<T, 3, MODE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+        march<T, 3, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
                           status);
     else
-        march<T, 2, MODE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+        march<T, 2, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
                           status);
 }
 
@@ -806,9 +842,14 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
     const T* n = (const T*)bn;
     T* o = (T*)out;
     const T* s = (const T*)P.d_sigma;
-#define CDD_LAUNCH_ST(M, SP)                                                                       \
-    k_stencil<T, M><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                         P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps)
+    // plans with a glide-only instance run the variant that carries the projection
+#define CDD_LAUNCH_ST(M, SP)                                                                              \
+    if (P.any_glide)                                                                                  \
+        k_stencil<T, M, true><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
+                                                                   P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps); \
+    else                                                                                              \
+        k_stencil<T, M, false><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
+                                                                    P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps)
     switch (mode) {
         case M_FLUX: CDD_LAUNCH_ST(M_FLUX, (T*)speed); break;
         case M_STAGE1: CDD_LAUNCH_ST(M_STAGE1, nullptr); break;
@@ -924,10 +965,14 @@ cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st)
 template <typename T>
 static cudaError_t st_attr(size_t smem) {
     cudaError_t e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2>, smem))) return e;
-    return set_dyn_smem_limit(k_stencil<T, M_STAGE3>, smem);
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE3, false>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX, true>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1, true>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2, true>, smem))) return e;
+    return set_dyn_smem_limit(k_stencil<T, M_STAGE3, true>, smem);
 }
 
 cudaError_t stencil_set_attributes(int precision, size_t smem) {

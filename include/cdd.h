@@ -64,7 +64,14 @@ typedef struct cdd_instance {
     int has_load;          /* nonzero: add the applied-strain stress */
     double load_rate[3], load_initial[3], load_t0;
     double load_mu, load_nu;   /* stiffness the load is converted with */
+    int dynamics;          /* CDD_DYN_GLIDE_CLIMB (0) or CDD_DYN_GLIDE_ONLY (1) */
 } cdd_instance;
+
+/* Dynamics of an instance: BetaPDynamics of CentralUpwindHJBetaPDynamics3D.py (glide and climb,
+ * Lambda optional), or the glide-only BetaPDynamics of CentralUpwindHJBetaPGlideOnlyDynamics.py
+ * (the velocity projected so that it carries no climb, L152-201 / 2-D L96-129; Lambda must be 0).
+ * The adjoint entry points support CDD_DYN_GLIDE_CLIMB only. */
+enum cdd_dynamics { CDD_DYN_GLIDE_CLIMB = 0, CDD_DYN_GLIDE_ONLY = 1 };
 
 typedef struct cdd_plan cdd_plan;
 

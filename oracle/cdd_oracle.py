@@ -236,6 +236,62 @@ def velocity(us, sigma, Lambda):
     return [v / rho for v in V]
 
 
+def velocity_glide(us, sigma):
+    """Glide-only velocity at a corner: the climb velocity projected as in
+    CentralUpwindHJBetaPGlideOnlyDynamics.py BetaP3D_Velocity L152-201 (2-D: BetaP2D_Velocity
+    L96-129), in the reference's operation order; climb velocity L131-150 / L73-94."""
+    shape = us[0].shape[1:]
+    nd = len(us)
+    v = [np.zeros(shape), np.zeros(shape), np.zeros(shape)]
+    for n in range(3):
+        for l in range(3):
+            for d in range(nd):
+                v[l] = v[l] + us[d][ci(l, n)] * sigma[ci(d, n)]
+            for d in range(nd):
+                v[d] = v[d] - us[d][ci(l, n)] * sigma[ci(l, n)]
+    if nd == 3:
+        ux, uy, uz = us
+        rhorho = ME
+        uxTr = ux[0] + ux[4] + ux[8]
+        uyTr = uy[0] + uy[4] + uy[8]
+        uzTr = uz[0] + uz[4] + uz[8]
+        rhorho = rhorho + (uxTr * uxTr + uyTr * uyTr + uzTr * uzTr)
+        rhorho = rhorho - 2 * uxTr * (ux[0] + uy[1] + uz[2])
+        rhorho = rhorho - 2 * uyTr * (ux[3] + uy[4] + uz[5])
+        rhorho = rhorho - 2 * uzTr * (ux[6] + uy[7] + uz[8])
+        for n in range(3):
+            t = ux[ci(n, 0)] + uy[ci(n, 1)] + uz[ci(n, 2)]
+            rhorho = rhorho + t * t
+        rhov = ME
+        rhov = rhov + v[0] * (ux[8] + ux[4] - uy[1] - uz[2])
+        rhov = rhov + v[1] * (uy[0] + uy[8] - ux[3] - uz[5])
+        rhov = rhov + v[2] * (uz[0] + uz[4] - ux[6] - uy[7])
+        factor = rhov / rhorho
+        v[0] = v[0] + (ux[4] + ux[8] - uy[1] - uz[2]) * factor
+        v[1] = v[1] + (uy[0] + uy[8] - ux[3] - uz[5]) * factor
+        v[2] = v[2] + (uz[0] + uz[4] - ux[6] - uy[7]) * factor
+    else:
+        ux, uy = us
+        rhorho = ME
+        uxTr = ux[0] + ux[4] + ux[8]
+        uyTr = uy[0] + uy[4] + uy[8]
+        rhorho = rhorho + (uxTr * uxTr + uyTr * uyTr)
+        rhorho = rhorho - 2 * uxTr * (ux[0] + uy[1])
+        rhorho = rhorho - 2 * uyTr * (ux[3] + uy[4])
+        for n in range(3):
+            t = ux[ci(n, 0)] + uy[ci(n, 1)]
+            rhorho = rhorho + t * t
+        rhov = ME
+        rhov = rhov + v[0] * (ux[8] + ux[4] - uy[1])
+        rhov = rhov + v[1] * (uy[0] + uy[8] - ux[3])
+        rhov = rhov + (-v[2]) * (ux[6] + uy[7])
+        v[0] = v[0] + (ux[4] + ux[8] - uy[1]) * rhov / rhorho
+        v[1] = v[1] + (uy[0] + uy[8] - ux[3]) * rhov / rhorho
+        v[2] = v[2] - (ux[6] + uy[7]) * rhov / rhorho
+    rho = rho_mod(us)
+    return [w / rho for w in v]
+
+
 def hamiltonian(us, V, Lambda):
     """H_ij at a corner (L161-201)."""
     nd = len(us)
@@ -265,8 +321,10 @@ def hamiltonian(us, V, Lambda):
 # ----------------------------------------------------------------------------------------------
 # Central-upwind flux: CentralUpwindHJ3D.CalculateFlux L99-271
 # ----------------------------------------------------------------------------------------------
-def flux(beta, sigma, Lambda=0, Dx=None):
-    """Return (rhs, speed) for plastic distortion ``beta`` under total stress ``sigma``."""
+def flux(beta, sigma, Lambda=0, Dx=None, glide=False):
+    """Return (rhs, speed) for plastic distortion ``beta`` under total stress ``sigma``.
+    glide: the glide-only dynamics (CentralUpwindHJBetaPGlideOnlyDynamics.py: projected velocity,
+    no Lambda term)."""
     shape = beta.shape[1:]
     nd = len(shape)
     if Dx is None:
@@ -280,7 +338,11 @@ def flux(beta, sigma, Lambda=0, Dx=None):
     def us_of(c):
         return [der[a][0] if c[a] else der[a][1] for a in range(nd)]
 
-    Vs = {c: velocity(us_of(c), sigma, Lambda) for c in corners}
+    if glide:
+        Vs = {c: velocity_glide(us_of(c), sigma) for c in corners}
+        Lambda = 0
+    else:
+        Vs = {c: velocity(us_of(c), sigma, Lambda) for c in corners}
     sp, sm, tot = [], [], []
     for a in range(nd):
         vals = [Vs[c][a] for c in corners]
@@ -310,8 +372,9 @@ class Params:
     """Material, loading and integrator parameters of one instance."""
 
     def __init__(self, mu=1.0, nu=0.3, Lambda=0, cfl=0.25, load_rate=None,
-                 load_initial=(0., 0., 0.), load_t0=0., load_mu=None, load_nu=None):
+                 load_initial=(0., 0., 0.), load_t0=0., load_mu=None, load_nu=None, glide=False):
         self.mu, self.nu, self.Lambda, self.cfl = mu, nu, Lambda, cfl
+        self.glide = glide
         self.load_rate = None if load_rate is None else np.asarray(load_rate, float)
         self.load_initial = np.asarray(load_initial, float)
         self.load_t0 = load_t0
@@ -331,7 +394,7 @@ def total_stress(beta, t, p):
 
 def full_flux(beta, t, p):
     """BetaPDynamics.CalculateFlux (CentralUpwindHJBetaPDynamics3D.py L218-221)."""
-    return flux(beta, total_stress(beta, t, p), p.Lambda)
+    return flux(beta, total_stress(beta, t, p), p.Lambda, glide=p.glide)
 
 
 # ----------------------------------------------------------------------------------------------

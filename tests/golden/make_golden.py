@@ -43,6 +43,7 @@ MODULES = [
     "FieldDynamics/CentralUpwindHJ.py", "FieldDynamics/CentralUpwindHJ3D.py",
     "FieldDynamics/CentralUpwindHJBetaPDynamics.py",
     "FieldDynamics/CentralUpwindHJBetaPDynamics3D.py",
+    "FieldDynamics/CentralUpwindHJBetaPGlideOnlyDynamics.py",
     "FieldMovers/__init__.py", "FieldMovers/FieldMover.py",
 ]
 
@@ -84,21 +85,23 @@ def _import_reference():
     from Plasticity.FieldMovers import FieldMover
     from Plasticity.FieldDynamics import CentralUpwindHJBetaPDynamics3D as Dyn3
     from Plasticity.FieldDynamics import CentralUpwindHJBetaPDynamics as Dyn2
-    return PlasticityState, GridArray, FieldMover, Dyn3, Dyn2
+    from Plasticity.FieldDynamics import CentralUpwindHJBetaPGlideOnlyDynamics as Glide
+    return PlasticityState, GridArray, FieldMover, Dyn3, Dyn2, Glide
 
 
 def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.25,
-             load_rate=None, store_fields=True, t_end=1e30):
-    PlasticityState, GridArray, FieldMover, Dyn3, Dyn2 = _import_reference()
+             load_rate=None, store_fields=True, t_end=1e30, glide=False):
+    PlasticityState, GridArray, FieldMover, Dyn3, Dyn2, Glide = _import_reference()
     sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
     from cdd.initial import gaussian_random_field
 
     beta0 = gaussian_random_field(shape, sigma_f, 0.05, seed)
     shape = tuple(shape)
-    mod = Dyn3 if len(shape) == 3 else Dyn2
+    mod = Glide if glide else (Dyn3 if len(shape) == 3 else Dyn2)
+    kw = {} if glide else {"Lambda": Lambda}
 
     if load_rate is None:
-        dynamics = mod.BetaPDynamics(Lambda=Lambda)
+        dynamics = mod.BetaPDynamics(**kw)
     else:
         rate = np.asarray(load_rate, dtype=np.float64)
 
@@ -112,7 +115,7 @@ def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.
                 for i, a in enumerate("xyz"):
                     sigma[a, a] += lamb * tr + 2. * state.mu * eps[i]
                 return sigma
-        dynamics = LoadedDynamics(Lambda=Lambda)
+        dynamics = LoadedDynamics(**kw)
 
     def make_state(arr):
         st = PlasticityState.PlasticityState(shape, mu=mu, nu=nu)
@@ -129,7 +132,7 @@ def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.
         return e, m
 
     out = {"shape": np.array(shape), "sigma_f": sigma_f, "seed": seed, "mu": mu, "nu": nu,
-           "Lambda": Lambda, "cfl": cfl,
+           "Lambda": Lambda, "cfl": cfl, "glide": int(glide),
            "load_rate": np.zeros(3) if load_rate is None else np.asarray(load_rate, float)}
     state = make_state(beta0)
     t0 = time.time()
@@ -186,6 +189,10 @@ CASES = {
                      load_rate=(-0.025, -0.025, 0.05)),
     # 2-D run at mixed-radix size (48 = 16 * 3) and a clamped end time
     "g2d_48_tend": dict(shape=(48, 48), sigma_f=0.05, seed=6, steps=6, t_end=0.004),
+    # glide-only dynamics (CentralUpwindHJBetaPGlideOnlyDynamics.py), 3-D with load and 2-D
+    "g3d_glide": dict(shape=(12, 12, 12), sigma_f=0.06, seed=7, steps=3, glide=True,
+                      load_rate=(-0.025, -0.025, 0.05)),
+    "g2d_glide": dict(shape=(32, 32), sigma_f=0.05, seed=8, steps=5, glide=True),
     # config-1 style curves: 2-D 128^2, sigma 0.05, no load, 100 steps (observables only)
     "c1_2d_128": dict(shape=(128, 128), sigma_f=0.05, seed=11, steps=100, store_fields=False),
     # config-2 style curves at reduced size: 3-D 32^3, sigma 0.04, applied strain rate, 40 steps

@@ -14,6 +14,7 @@ from Plasticity import PlasticitySystem
 from Plasticity.Fields import Fields
 from Plasticity.FieldMovers import FieldMover
 from Plasticity.FieldDynamics import CentralUpwindHJBetaPDynamics3D, CentralUpwindHJBetaPDynamics
+from Plasticity.FieldDynamics import CentralUpwindHJBetaPGlideOnlyDynamics
 from Plasticity.FieldDynamics import engine
 from Plasticity.PlasticityStates import PlasticityState
 from Plasticity.Observers import Observer
@@ -103,3 +104,20 @@ def test_precision_switch_and_energy_observer():
         assert rel(st.betaP.stack(), ref) < 1e-5
     finally:
         engine.set_precision("f64")
+
+
+
+def test_glide_only_system_run_matches_reference():
+    """The glide-only facade (CentralUpwindHJBetaPGlideOnlyDynamics.BetaPDynamics) over a 2-D run,
+    against the reference's own glide-only golden vectors."""
+    g = np.load(golden_path("g2d_glide"))
+    st = state_of(g)
+    dyn = CentralUpwindHJBetaPGlideOnlyDynamics.BetaPDynamics()
+    rhs, speed = dyn.CalculateFlux(0.0, st, CFLCondition=True)
+    assert rel(rhs.stack(), g["rhs"]) < 1e-12
+    assert rel(np.asarray(speed), g["speed"]) < 1e-12
+    recall = Observer.RecallStateObserver()
+    system = PlasticitySystem.PlasticitySystem(st.gridShape, st, FieldMover.TVDRungeKutta_FieldMover(CFLsafeFactor=0.25),
+                                               dyn, [recall])
+    system.Run(startTime=0.0, endTime=float(g["t_final"]) * (1.0 - 1e-12))
+    assert rel(recall.state.betaP.stack(), g["beta_final"]) < 1e-10

@@ -15,7 +15,8 @@ import cdd
 import cdd_oracle as O
 from conftest import golden_path
 
-FIELD_CASES = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_lambda", "g3d_load", "g2d_48_tend"]
+FIELD_CASES = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_lambda", "g3d_load", "g2d_48_tend", "g3d_glide",
+               "g2d_glide"]
 T_END = {"g2d_48_tend": 0.004}
 
 
@@ -29,13 +30,17 @@ def inst_of(g):
     lr = g["load_rate"]
     return cdd.Instance(shape=tuple(int(v) for v in g["shape"]), mu=float(g["mu"]), nu=float(g["nu"]),
                         Lambda=float(g["Lambda"]), cfl=float(g["cfl"]),
-                        load_rate=tuple(lr) if np.any(lr) else None)
+                        load_rate=tuple(lr) if np.any(lr) else None, glide_only=glide_of(g))
+
+
+def glide_of(g):
+    return bool(int(g["glide"])) if "glide" in g.files else False
 
 
 def params_of(g):
     lr = g["load_rate"]
     return O.Params(mu=float(g["mu"]), nu=float(g["nu"]), Lambda=float(g["Lambda"]),
-                    cfl=float(g["cfl"]), load_rate=lr if np.any(lr) else None)
+                    cfl=float(g["cfl"]), load_rate=lr if np.any(lr) else None, glide=glide_of(g))
 
 
 SYM = [0, 1, 2, 4, 5, 8]   # xx xy xz yy yz zz in the 9-component order
@@ -298,3 +303,54 @@ def test_flux_with_given_stress_equals_flux(prec):
     assert torch.equal(rhs, rhs2) and torch.equal(speed, speed2)
     rhs3, _ = plan.flux(beta, 0.3, sigma=2 * s6)
     assert not torch.equal(rhs, rhs3)
+
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 64), (64, 64)])
+def test_glide_only_fp32_form_and_batched_with_glide_climb(shape):
+    """Glide-only dynamics: FP32 form within 1e-5 of FP64 after 10 steps; a plan mixing a
+    glide-only and a glide-and-climb instance gives each its single-plan result: bitwise for the
+    glide-only one (same kernel variant), to rounding for the other (the mixed plan runs it in the
+    variant compiled with the projection, whose instruction scheduling may contract differently)."""
+    b0 = cdd.gaussian_random_field(shape, 0.05, 0.05, 13)
+    glide = cdd.Instance(shape, load_rate=(-0.025, -0.025, 0.05), glide_only=True)
+    out = {}
+    for prec in ("f64", "f32"):
+        plan = cdd.Plan([glide], prec)
+        b = plan.pack([b0])
+        plan.set_time(0.0, 1e30)
+        plan.run(b, 10, graph=True)
+        plan.check_status()
+        out[prec] = plan.field_view(b, 0).double().cpu().numpy()
+    for c in range(9):
+        assert rel(out["f32"][c], out["f64"][c]) < 1e-5, c
+    climb = cdd.Instance(shape, load_rate=(-0.025, -0.025, 0.05))
+    mixed = cdd.Plan([glide, climb], "f64")
+    bm = mixed.pack([b0, b0])
+    mixed.set_time(0.0, 1e30)
+    mixed.run(bm, 2, graph=False)
+    for i, inst in enumerate((glide, climb)):
+        single = cdd.Plan([inst], "f64")
+        bs = single.pack([b0])
+        single.set_time(0.0, 1e30)
+        single.run(bs, 2, graph=False)
+        if i == 0:
+            assert torch.equal(mixed.field_view(bm, i), single.field_view(bs, 0))
+        else:
+            assert rel(mixed.field_view(bm, i).cpu().numpy(), single.field_view(bs, 0).cpu().numpy()) < 1e-13
+    assert not torch.equal(mixed.field_view(bm, 0), mixed.field_view(bm, 1))
+
+
+def test_adjoint_rejects_glide_only():
+    import ctypes
+    from cdd import _lib
+    shape = (16, 16, 16)
+    plan = cdd.Plan([cdd.Instance(shape, glide_only=True)], "f64")
+    b = plan.pack([cdd.gaussian_random_field(shape, 0.05, 0.05, 1)])
+    g = torch.zeros_like(b)
+    vb, sb = plan.empty_field(), plan.empty_stress()
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = plan.lib.cdd_flux_vjp(plan.handle, P(b), ctypes.c_double(0.0), P(g), P(vb), P(sb), None, None)
+    assert rc == _lib.CDD_ERR_UNSUPPORTED
+    with pytest.raises(cdd.CDDError):
+        cdd.Plan([cdd.Instance(shape, Lambda=1.0, glide_only=True)], "f64")

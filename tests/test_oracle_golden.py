@@ -11,7 +11,8 @@ import cdd_oracle as O
 from conftest import golden_path
 
 TOL = 1e-13
-FIELD_CASES = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_lambda", "g3d_load", "g2d_48_tend"]
+FIELD_CASES = ["g3d_16", "g2d_32", "g3d_aniso", "g3d_lambda", "g3d_load", "g2d_48_tend", "g3d_glide",
+               "g2d_glide"]
 T_END = {"g2d_48_tend": 0.004}
 
 
@@ -22,7 +23,8 @@ def rel(a, b):
 def params_of(g):
     lr = g["load_rate"]
     return O.Params(mu=float(g["mu"]), nu=float(g["nu"]), Lambda=int(g["Lambda"]),
-                    cfl=float(g["cfl"]), load_rate=lr if np.any(lr) else None)
+                    cfl=float(g["cfl"]), load_rate=lr if np.any(lr) else None,
+                    glide=bool(int(g["glide"])) if "glide" in g.files else False)
 
 
 @pytest.mark.parametrize("name", FIELD_CASES)
