@@ -350,6 +350,24 @@ struct RowLayout {   // lines are rows of length n, padded every 16 elements
         l = fdiv_q(nr, g);
         j = g - l * nr.d;
     }
+    template <int NR> __device__ __forceinline__ void split_c(int g, int& l, int& j) const {
+        l = g / NR;
+        j = g - l * NR;
+    }
+    // Offsets of elements i0 + r STEP of line l, r = 0, 1, ...  LIN: the padding splits,
+    // row_pad(i0 + r STEP) = row_pad(i0) + row_pad(r STEP), so each offset is the line base plus a
+    // constant (the caller guarantees it: see fft_stage_c).
+    template <int STEP, bool LIN> struct Walk {
+        int b, i0;
+        __device__ __forceinline__ int operator()(int r) const {
+            if constexpr (LIN) return b + r * STEP + ((r * STEP) >> 4);
+            else return b + row_pad(i0 + r * STEP);
+        }
+    };
+    template <int STEP, bool LIN> __device__ __forceinline__ Walk<STEP, LIN> walk(int l, int i0) const {
+        if constexpr (LIN) return {l * ld + row_pad(i0), 0};
+        else return {l * ld, i0};
+    }
 };
 
 // K groups of 2^lgw columns: element i of line l = (c, w) at c * cs + (i << lgw) + w; consecutive
@@ -366,6 +384,16 @@ struct ColLayout {
     __device__ __forceinline__ void split(int g, const FDiv&, int& l, int& j) const {
         j = (K == 1) ? (g >> lgw) : (g >> lgw) / K;
         l = g - j * (K << lgw);
+    }
+    template <int NR> __device__ __forceinline__ void split_c(int g, int& l, int& j) const {
+        split(g, FDiv{}, l, j);
+    }
+    template <int STEP, bool LIN> struct Walk {   // elements i0 + r STEP of one line: a fixed stride
+        int b, stride;
+        __device__ __forceinline__ int operator()(int r) const { return b + r * stride; }
+    };
+    template <int STEP, bool LIN> __device__ __forceinline__ Walk<STEP, LIN> walk(int l, int i0) const {
+        return {addr(l, i0), STEP << lgw};
     }
 };
 
@@ -405,11 +433,90 @@ __device__ __forceinline__ void fft_stage(const V* __restrict__ src, V* __restri
     __syncthreads();
 }
 
+// One stage with radix R, span NS and NR = n / R butterflies per line known at compile time: the
+// butterfly split, the twiddle row index jm = j mod NS and the element strides fold to constants.
+// Same codelets, twiddle rows and operation order as fft_stage (bitwise-identical results).
+// Row-layout offsets split into base + constant when the padding period 16 and the stride divide
+// one another: loads walk j + r NR with j < NR; stores walk jd + r NS with jd = (j - jm) R + jm, whose
+// first term is a multiple of NS R (a multiple of 16 when 16 divides NS R).
+template <int R, int NS, int NR, typename V, bool INV, typename Lay>
+__device__ __forceinline__ void fft_stage_c(const V* __restrict__ src, V* __restrict__ dst, const Lay& lay,
+                                            const V* __restrict__ twrows, int tid, int nt) {
+    constexpr bool LIN_LD = (NR % 16 == 0) || (16 % NR == 0);
+    constexpr bool LIN_ST = (NS % 16 == 0) || (16 % NS == 0 && (NS * R) % 16 == 0);
+    const int total = lay_lines(lay) * NR;
+#pragma unroll 1
+    for (int g = tid; g < total; g += nt) {
+        int l, j;
+        lay.template split_c<NR>(g, l, j);
+        const int jm = (NS == 1) ? 0 : j % NS;
+        const auto ld = lay.template walk<NR, LIN_LD>(l, j);
+        V v[R];
+        if constexpr (NS == 1) {   // first stage: all twiddles are 1
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = src[ld(r)];
+        } else {
+            V w[R];
+            load_tw_row<R>(twrows + jm * tw_row(R), w);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const V a = src[ld(r)];
+                v[r] = (r == 0) ? a : (INV ? vmulc(a, w[r]) : vmul(a, w[r]));
+            }
+        }
+        dft<R, V, INV>(v);
+        const auto sw = lay.template walk<NS, LIN_ST>(l, (j - jm) * R + jm);
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[sw(r)] = v[r];
+    }
+    __syncthreads();
+}
+
+template <int... Rs> struct RadixProd;
+template <> struct RadixProd<> { static constexpr int v = 1; };
+template <int R, int... Rs> struct RadixProd<R, Rs...> { static constexpr int v = R * RadixProd<Rs...>::v; };
+
+// Stages st, st+1, ... of a plan whose remaining radices are R, Rs... (span NS so far).
+template <typename V, bool INV, typename Lay, int NS, int R, int... Rs>
+__device__ __forceinline__ V* fft_lines_c(V* src, V* dst, const Lay& lay, const LinePlan& lp,
+                                          const V* __restrict__ twbase, int tid, int nt, int rebase, int st) {
+    constexpr int N = NS * RadixProd<R, Rs...>::v;
+    fft_stage_c<R, NS, N / R, V, INV>(src, dst, lay, twbase + (lp.twst[st] - rebase), tid, nt);
+    if constexpr (sizeof...(Rs) == 0) return dst;
+    else return fft_lines_c<V, INV, Lay, NS * R, Rs...>(dst, src, lay, lp, twbase, tid, nt, rebase, st + 1);
+}
+
 // Run all stages of `lp` on the lines of `lay`, starting in buffer a (b is scratch of the same
 // layout). Returns the buffer that holds the result. Every thread of the block must call this.
+// The radix sequences that make_line_plan gives the usual lengths (16 to 512, and 24, 48, 96, 192
+// with the default largest radix 16) run the compile-time stages; others the general engine.
+template <typename V, bool INV, typename Lay>
+__device__ __forceinline__ V* fft_lines_g(V* a, V* b, const Lay& lay, const LinePlan& lp,
+                                          const V* __restrict__ twbase, int tid, int nt, int rebase);
+
 template <typename V, bool INV, typename Lay>
 __device__ __forceinline__ V* fft_lines(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
-                        int tid, int nt, int rebase = 0) {
+                                        int tid, int nt, int rebase = 0) {
+    const int nst = lp.nst, r0 = lp.radix[0], r1 = lp.radix[1], r2 = lp.radix[2];
+#define CDD_SEQ(COND, ...) \
+    if (COND) return fft_lines_c<V, INV, Lay, 1, __VA_ARGS__>(a, b, lay, lp, twbase, tid, nt, rebase, 0);
+    CDD_SEQ(nst == 2 && r0 == 16 && r1 == 16, 16, 16)
+    CDD_SEQ(nst == 2 && r0 == 16 && r1 == 8, 16, 8)
+    CDD_SEQ(nst == 2 && r0 == 16 && r1 == 4, 16, 4)
+    CDD_SEQ(nst == 2 && r0 == 8 && r1 == 4, 8, 4)
+    CDD_SEQ(nst == 3 && r0 == 16 && r1 == 8 && r2 == 4, 16, 8, 4)
+    CDD_SEQ(nst == 1 && r0 == 16, 16)
+    CDD_SEQ(nst == 2 && r0 == 16 && r1 == 3, 16, 3)
+    CDD_SEQ(nst == 2 && r0 == 8 && r1 == 3, 8, 3)
+    CDD_SEQ(nst == 3 && r0 == 8 && r1 == 4 && r2 == 3, 8, 4, 3)
+    CDD_SEQ(nst == 3 && r0 == 16 && r1 == 4 && r2 == 3, 16, 4, 3)
+#undef CDD_SEQ
+    return fft_lines_g<V, INV>(a, b, lay, lp, twbase, tid, nt, rebase);
+}
+
+template <typename V, bool INV, typename Lay>
+__device__ __forceinline__ V* fft_lines_g(V* a, V* b, const Lay& lay, const LinePlan& lp, const V* __restrict__ twbase,
+                        int tid, int nt, int rebase) {
     V* src = a;
     V* dst = b;
     for (int st = 0; st < lp.nst; ++st) {
