@@ -90,22 +90,56 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Stage a column tile of complex values: rows x 2^lgw columns of a row-major array (row stride
 // `stride` elements, columns w >= wv are padding: read as zero) into dst[(e << lgw) + w], with
-// 16-byte asynchronous copies. Needs 2^lgw x sizeof(V) >= 16 and 16-byte aligned rows in both
-// spaces. The caller waits (cp_async_wait_all) and synchronises the block before use.
+// 16-byte asynchronous copies. Each thread keeps one 16-byte chunk column and walks the rows with
+// pointer increments. Needs 2^lgw x sizeof(V) >= 16, nt a multiple of the chunks per row and
+// 16-byte aligned rows in both spaces. The caller waits (cp_async_wait_all) and synchronises the
+// block before use.
 template <typename V>
 __device__ __forceinline__ void tile_async_load(V* dst, const V* src, long long stride, int rows, int lgw, int wv,
                                                 int tid, int nt) {
-    constexpr int PER = 16 / (int)sizeof(V);   // complex values per copy: 2 (FP32) or 1 (FP64)
-    const int W = 1 << lgw;
-    const int chunks = (rows << lgw) / PER;
+    constexpr int PER = 16 / (int)sizeof(V);       // complex values per copy: 2 (FP32) or 1 (FP64)
+    constexpr int LPER = (PER == 2) ? 1 : 0;
+    const int cl = lgw - LPER;                     // log2 chunks per row
+    const int w = (tid & ((1 << cl) - 1)) * PER;
+    int valid = wv - w;
+    valid = valid < 0 ? 0 : (valid > PER ? PER : valid);
+    const int rstep = nt >> cl;
+    if (rstep <= 0) return;   // launches use 256 threads and at most 64 columns: never taken
+    int e = tid >> cl;
+    const V* g = valid ? src + (long long)e * stride + w : src;
+    const long long gstep = valid ? (long long)rstep * stride : 0;
+    V* d = dst + (e << lgw) + w;
+    const int dstep = rstep << lgw;
 #pragma unroll 4
-    for (int q = tid; q < chunks; q += nt) {
-        const int i = q * PER;
-        const int e = i >> lgw, w = i & (W - 1);
-        int valid = wv - w;
-        valid = valid < 0 ? 0 : (valid > PER ? PER : valid);
-        cp_async16(dst + i, valid ? (const void*)(src + (long long)e * stride + w) : (const void*)src,
-                   valid * (int)sizeof(V));
+    for (; e < rows; e += rstep, g += gstep, d += dstep) cp_async16(d, g, valid * (int)sizeof(V));
+}
+
+// The inverse: a column tile in shared memory (layout as above) back to the row-major array, only
+// the columns w < wv, with 16-byte stores (a partial chunk of an FP32 tile stores its one valid
+// value). Same requirements; the caller synchronises before.
+template <typename V>
+__device__ __forceinline__ void tile_store(V* dst, const V* src, long long stride, int rows, int lgw, int wv,
+                                           int tid, int nt) {
+    constexpr int PER = 16 / (int)sizeof(V);
+    constexpr int LPER = (PER == 2) ? 1 : 0;
+    const int cl = lgw - LPER;
+    const int w = (tid & ((1 << cl) - 1)) * PER;
+    const int valid = wv - w;
+    if (valid <= 0) return;
+    const int rstep = nt >> cl;
+    if (rstep <= 0) return;
+    int e = tid >> cl;
+    V* g = dst + (long long)e * stride + w;
+    const long long gstep = (long long)rstep * stride;
+    const V* d = src + (e << lgw) + w;
+    const int dstep = rstep << lgw;
+    if (valid >= PER) {
+#pragma unroll 4
+        for (; e < rows; e += rstep, g += gstep, d += dstep)
+            *reinterpret_cast<float4*>(g) = *reinterpret_cast<const float4*>(d);
+    } else {
+#pragma unroll 4
+        for (; e < rows; e += rstep, g += gstep, d += dstep) *g = *d;
     }
 }
 
@@ -116,6 +150,18 @@ __device__ __forceinline__ void stage_tw_to_smem(const LinePlan& lp, const V* __
                                                  int nt) {
     const V* src = tw + lp.twst[0];
     for (int i = tid; i < lp.twspan; i += nt) dst[i] = __ldg(src + i);
+}
+
+// Row kernels (R2C / C2R): per-block table of the 2P rows a block reads or writes, after the
+// twiddle rows in shared memory: element offsets of the two rows (p, q; -1: past the end) and the
+// FP64 mean stress added to the row (C2R of FP32 plans).
+struct RowPtr {
+    long long p, q;
+};
+__host__ __device__ constexpr size_t rows_table_bytes(int P) { return 16 + (size_t)2 * P * (sizeof(RowPtr) + sizeof(double)); }
+// The table starts 16-byte aligned after the twiddle rows (tws: twspan complex values).
+template <typename V> __device__ __forceinline__ RowPtr* rows_table(V* tws, int twspan) {
+    return reinterpret_cast<RowPtr*>(tws + ((twspan + 1) & ~1));
 }
 
 // Per-pass tiling of one instance (host-chosen, read by the kernels).
@@ -484,6 +530,148 @@ __device__ __forceinline__ V* fft_lines_c(V* src, V* dst, const Lay& lay, const 
     fft_stage_c<R, NS, N / R, V, INV>(src, dst, lay, twbase + (lp.twst[st] - rebase), tid, nt);
     if constexpr (sizeof...(Rs) == 0) return dst;
     else return fft_lines_c<V, INV, Lay, NS * R, Rs...>(dst, src, lay, lp, twbase, tid, nt, rebase, st + 1);
+}
+
+// ---- column tiles with the first and last stage in global memory ----
+// The lines are the columns of a tile: K components of 2^lgw columns, line l = (c, w) with
+// c = l >> lgw. The first stage reads its butterflies straight from global memory into registers
+// and the last stage writes its outputs straight back, so a tile passes through shared memory only
+// between stages (one buffer for two-stage plans). Same codelets, twiddle rows and operation order
+// as fft_stage.
+template <int K> __device__ __forceinline__ void col_split(int g, int lgw, int& l, int& j) {
+    j = (K == 1) ? (g >> lgw) : (g >> lgw) / K;
+    l = g - j * (K << lgw);
+}
+
+// Shared tile: element i of line (c, w) at base[c * cs + (i << lgw) + w].
+template <typename V, int K> struct SColT {
+    V* base;
+    int lgw, cs;
+    struct Walk {
+        V* p;
+        int stride;
+        __device__ __forceinline__ V ld(int r) const { return p[r * stride]; }
+        __device__ __forceinline__ void st(int r, V v) const { p[r * stride] = v; }
+    };
+    __device__ __forceinline__ Walk walk(int l, int i0, int step) const {
+        const int c = (K == 1) ? 0 : (l >> lgw), w = l & ((1 << lgw) - 1);
+        return {base + c * cs + (i0 << lgw) + w, step << lgw};
+    }
+};
+
+// Global tile: element i of line (c, w) at base[c * cstride + i * stride + w]; columns w >= wv are
+// padding: they read as zero and are not written.
+template <typename V, int K> struct GColT {
+    V* base;
+    long long stride, cstride;
+    int lgw, wv;
+    struct Walk {
+        V* p;
+        long long stride;
+        bool valid;
+        __device__ __forceinline__ V ld(int r) const {
+            V z;
+            z.x = 0;
+            z.y = 0;
+            return valid ? p[r * stride] : z;
+        }
+        __device__ __forceinline__ void st(int r, V v) const {
+            if (valid) p[r * stride] = v;
+        }
+    };
+    __device__ __forceinline__ Walk walk(int l, int i0, int step) const {
+        const int c = (K == 1) ? 0 : (l >> lgw), w = l & ((1 << lgw) - 1);
+        return {base + c * cstride + (long long)i0 * stride + w, (long long)step * stride, w < wv};
+    }
+};
+
+template <int R, int NS, int NR, typename V, bool INV, int K, class LS, class LD>
+__device__ __forceinline__ void fft_stage_io(const LS& src, const LD& dst, int lgw, const V* __restrict__ twrows,
+                                             int tid, int nt) {
+    const int total = (K << lgw) * NR;
+#pragma unroll 1
+    for (int g = tid; g < total; g += nt) {
+        int l, j;
+        col_split<K>(g, lgw, l, j);
+        const int jm = (NS == 1) ? 0 : j % NS;
+        const auto a = src.walk(l, j, NR);
+        V v[R];
+        if constexpr (NS == 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = a.ld(r);
+        } else {
+            V w[R];
+            load_tw_row<R>(twrows + jm * tw_row(R), w);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const V x = a.ld(r);
+                v[r] = (r == 0) ? x : (INV ? vmulc(x, w[r]) : vmul(x, w[r]));
+            }
+        }
+        dft<R, V, INV>(v);
+        const auto b = dst.walk(l, (j - jm) * R + jm, NS);
+#pragma unroll
+        for (int r = 0; r < R; ++r) b.st(r, v[r]);
+    }
+    __syncthreads();
+}
+
+// Stages st, st+1, ... (remaining radices R, Rs..., span NS so far) from `in` to `out`; stage k
+// writes the shared tile x when k is even and y when odd, the last stage writes `out`.
+template <typename V, bool INV, int K, class LIn, class LOut, int NS, int R, int... Rs>
+__device__ __forceinline__ void fft_io_c(const LIn& in, const SColT<V, K>& x, const SColT<V, K>& y, const LOut& out,
+                                         int lgw, const LinePlan& lp, const V* __restrict__ twbase, int tid, int nt,
+                                         int rebase, int st) {
+    constexpr int N = NS * RadixProd<R, Rs...>::v;
+    const V* tw = twbase + (lp.twst[st] - rebase);
+    if constexpr (sizeof...(Rs) == 0) {
+        fft_stage_io<R, NS, N / R, V, INV, K>(in, out, lgw, tw, tid, nt);
+    } else {
+        fft_stage_io<R, NS, N / R, V, INV, K>(in, x, lgw, tw, tid, nt);
+        fft_io_c<V, INV, K, SColT<V, K>, LOut, NS * R, Rs...>(x, y, x, out, lgw, lp, twbase, tid, nt, rebase, st + 1);
+    }
+}
+
+// The compile-time radix sequences of at least two stages (make_line_plan with the default largest
+// radix 16 for 32..512 and 48, 96, 192, 24).
+#define CDD_IO_SEQS(X)                                  \
+    X(nst == 2 && r0 == 16 && r1 == 16, 16, 16)         \
+    X(nst == 2 && r0 == 16 && r1 == 8, 16, 8)           \
+    X(nst == 2 && r0 == 16 && r1 == 4, 16, 4)           \
+    X(nst == 2 && r0 == 8 && r1 == 4, 8, 4)             \
+    X(nst == 3 && r0 == 16 && r1 == 8 && r2 == 4, 16, 8, 4) \
+    X(nst == 2 && r0 == 16 && r1 == 3, 16, 3)           \
+    X(nst == 2 && r0 == 8 && r1 == 3, 8, 3)             \
+    X(nst == 3 && r0 == 8 && r1 == 4 && r2 == 3, 8, 4, 3)   \
+    X(nst == 3 && r0 == 16 && r1 == 4 && r2 == 3, 16, 4, 3)
+
+// True when lp runs through fft_io (the host sizes shared memory with this).
+__host__ __device__ inline bool line_plan_io(const LinePlan& lp) {
+    const int nst = lp.nst, r0 = lp.radix[0], r1 = lp.radix[1], r2 = lp.radix[2];
+    (void)r2;
+#define CDD_IO_TEST(COND, ...) if (COND) return true;
+    CDD_IO_SEQS(CDD_IO_TEST)
+#undef CDD_IO_TEST
+    return false;
+}
+
+// All stages of lp from `in` to `out` through the shared tiles x, y (y unused by two-stage plans).
+// Returns false, doing nothing, when lp has no compile-time sequence. Every thread of the block
+// must call this; it ends synchronised.
+template <typename V, bool INV, int K, class LIn, class LOut>
+__device__ __forceinline__ bool fft_io(const LIn& in, const SColT<V, K>& x, const SColT<V, K>& y, const LOut& out,
+                                       int lgw, const LinePlan& lp, const V* __restrict__ twbase, int tid, int nt,
+                                       int rebase) {
+    const int nst = lp.nst, r0 = lp.radix[0], r1 = lp.radix[1], r2 = lp.radix[2];
+    (void)r2;
+#define CDD_IO_RUN(COND, ...)                                                                               \
+    if (COND) {                                                                                             \
+        fft_io_c<V, INV, K, LIn, LOut, 1, __VA_ARGS__>(in, x, y, out, lgw, lp, twbase, tid, nt, rebase, 0); \
+        return true;                                                                                        \
+    }
+    CDD_IO_SEQS(CDD_IO_RUN)
+#undef CDD_IO_RUN
+    return false;
 }
 
 // Run all stages of `lp` on the lines of `lay`, starting in buffer a (b is scratch of the same

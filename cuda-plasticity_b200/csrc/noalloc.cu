@@ -203,7 +203,7 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.tiles_a = 1;
         P.pass[k].threads = t.threads;
         P.pass[k].smem = ((2 * (size_t)Pl * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
-                         (size_t)I.lp_last.twspan * velt;
+                         (size_t)I.lp_last.twspan * velt + rows_table_bytes(Pl);
     }
     for (int k : {PASS_MID_F, PASS_MID_I}) {
         PassTile& t = I.tile[k];
@@ -217,7 +217,8 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         t.threads = 256;
         t.tiles_a = (I.nh + W - 1) / W;
         t.blocks = comps * I.n0 * t.tiles_a;
-        P.pass[k].smem = 2 * (size_t)W * I.n1 * velt + (size_t)I.lp_mid.twspan * velt;
+        P.pass[k].smem = ((line_plan_io(I.lp_mid) && I.lp_mid.nst == 2) ? 1 : 2) * (size_t)W * I.n1 * velt +
+                         (size_t)I.lp_mid.twspan * velt;
     }
     {
         PassTile& t = I.tile[PASS_GREEN];

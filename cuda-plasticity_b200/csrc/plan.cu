@@ -183,7 +183,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.blocks = (int)((npairs + P - 1) / P);
             t.tiles_a = 1;
             size_t sm = ((2 * (size_t)P * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
-                        (size_t)I.lp_last.twspan * velt;   // buffers + twiddle rows
+                        (size_t)I.lp_last.twspan * velt + rows_table_bytes(P);   // buffers + twiddle rows + row table
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;
         }
@@ -201,7 +201,9 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = 256;
             t.tiles_a = (I.nh + W - 1) / W;
             t.blocks = comps * I.n0 * t.tiles_a;
-            size_t sm = 2 * (size_t)W * I.n1 * velt + (size_t)I.lp_mid.twspan * velt;
+            // one shared tile for two-stage plans run with the first and last stage in global memory
+            const int bufs = (line_plan_io(I.lp_mid) && I.lp_mid.nst == 2) ? 1 : 2;
+            size_t sm = bufs * (size_t)W * I.n1 * velt + (size_t)I.lp_mid.twspan * velt;
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;
         }

@@ -105,6 +105,23 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const int tid = threadIdx.x, nt = blockDim.x;
     const T half = (T)0.5;
 
+    // row table: the two source rows of each of the block's 2P rows (-1: past the last row)
+    V* tws = s + ((2 * P * ld + 1) & ~1);   // twiddle rows, 16-byte aligned after the buffers
+    RowPtr* rt = rows_table(tws, I.lp_last.twspan);
+    for (int r = tid; r < 2 * P; r += nt) {
+        const long long ra = 2LL * lb * P + r;
+        RowPtr e;
+        e.p = e.q = -1;
+        if (ra < nrows) {
+            const T *pa, *qa;
+            src_rows(I, beta, mode, ra, pa, qa);
+            e.p = pa - beta;
+            e.q = qa - beta;
+        }
+        rt[r] = e;
+    }
+    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
+    __syncthreads();
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(beta + I.foff)) & 15) == 0) &&
                      ((((uintptr_t)(beta + I.soff)) & 15) == 0) && ((I.cells & 3) == 0);
     if (vec) {
@@ -112,24 +129,21 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
             const int i = i4 << 2;
             const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
-            const long long p = (long long)lb * P + pl;
+            const RowPtr ea = rt[2 * pl], eb = rt[2 * pl + 1];
             T a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
-            if (p < npairs) {
-                const long long ra = 2 * p;
-                const T *pa, *qa;
+            if (ea.p >= 0) {
                 T u[4], v[4];
-                src_rows(I, beta, mode, ra, pa, qa);
-                load4(pa + idx, u);
-                load4(qa + idx, v);
+                load4(beta + ea.p + idx, u);
+                load4(beta + ea.q + idx, v);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) a[q] = half * (u[q] + v[q]);
-                if (ra + 1 < nrows) {
-                    src_rows(I, beta, mode, ra + 1, pa, qa);
-                    load4(pa + idx, u);
-                    load4(qa + idx, v);
+            }
+            if (eb.p >= 0) {
+                T u[4], v[4];
+                load4(beta + eb.p + idx, u);
+                load4(beta + eb.q + idx, v);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) b[q] = half * (u[q] + v[q]);
-                }
+                for (int q = 0; q < 4; ++q) b[q] = half * (u[q] + v[q]);
             }
             V* d = s + pl * ld + row_pad(idx);
 #pragma unroll
@@ -138,24 +152,14 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     } else {
 #pragma unroll 2
         for (int i = tid; i < P * N; i += nt) {
-            int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
-            long long p = (long long)lb * P + pl;
+            const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
+            const RowPtr ea = rt[2 * pl], eb = rt[2 * pl + 1];
             V z; z.x = 0; z.y = 0;
-            if (p < npairs) {
-                long long ra = 2 * p;
-                const T *pa, *qa;
-                src_rows(I, beta, mode, ra, pa, qa);
-                z.x = half * (pa[idx] + qa[idx]);
-                if (ra + 1 < nrows) {
-                    src_rows(I, beta, mode, ra + 1, pa, qa);
-                    z.y = half * (pa[idx] + qa[idx]);
-                }
-            }
+            if (ea.p >= 0) z.x = half * (beta[ea.p + idx] + beta[ea.q + idx]);
+            if (eb.p >= 0) z.y = half * (beta[eb.p + idx] + beta[eb.q + idx]);
             s[pl * ld + row_pad(idx)] = z;
         }
     }
-    V* tws = s + ((2 * P * ld + 1) & ~1);   // twiddle rows, 16-byte aligned after the buffers
-    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     __syncthreads();
     if (MEAN64) {
         const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -260,6 +264,24 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     }
     V* tws = s + ((2 * P * ld + 1) & ~1);
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
+    // row table: the destination rows of each of the block's 2P rows and their FP64 mean stress
+    RowPtr* rt = rows_table(tws, I.lp_last.twspan);
+    double* rmean = reinterpret_cast<double*>(rt + 2 * P);
+    for (int r = tid; r < 2 * P; r += nt) {
+        const long long ra = 2LL * lb * P + r;
+        RowPtr e;
+        e.p = e.q = -1;
+        double m = 0.0;
+        if (ra < nrows) {
+            T *pd, *qd;
+            dst_rows(I, out, mode, ra, pd, qd);
+            e.p = pd - out;
+            e.q = qd - out;
+            if (MEAN64) m = mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
+        }
+        rt[r] = e;
+        rmean[r] = m;
+    }
     __syncthreads();
     RowLayout lay{P, ld};
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tws, tid, nt, I.lp_last.twst[0]);
@@ -270,49 +292,40 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
             const int i = i4 << 2;
             const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
-            const long long p = (long long)lb * P + pl;
-            if (p >= npairs) continue;
-            const long long ra = 2 * p;
+            const RowPtr ea = rt[2 * pl], eb = rt[2 * pl + 1];
+            if (ea.p < 0) continue;
             T va[4], vb[4];
             const V* sr = s + pl * ld + row_pad(idx);
 #pragma unroll
             for (int q = 0; q < 4; ++q) { V z = sr[q]; va[q] = z.x; vb[q] = z.y; }
             if (MEAN64) {
-                const T ma = (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
-                const T mb = (ra + 1 < nrows) ? (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)(ra + 1))) : (T)0;
+                const T ma = (T)rmean[2 * pl], mb = (T)rmean[2 * pl + 1];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) { va[q] += ma; vb[q] += mb; }
             }
-            T *pd, *qd;
-            dst_rows(I, out, mode, ra, pd, qd);
-            store4(pd + idx, va);
-            if (qd != pd) store4(qd + idx, va);
-            if (ra + 1 < nrows) {
-                dst_rows(I, out, mode, ra + 1, pd, qd);
-                store4(pd + idx, vb);
-                if (qd != pd) store4(qd + idx, vb);
+            store4(out + ea.p + idx, va);
+            if (ea.q != ea.p) store4(out + ea.q + idx, va);
+            if (eb.p >= 0) {
+                store4(out + eb.p + idx, vb);
+                if (eb.q != eb.p) store4(out + eb.q + idx, vb);
             }
         }
     } else {
         for (int i = tid; i < P * N; i += nt) {
-            int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
-            long long p = (long long)lb * P + pl;
-            if (p >= npairs) continue;
+            const int pl = fdiv_q(I.fd_nl, i), idx = i - pl * N;
+            const RowPtr ea = rt[2 * pl], eb = rt[2 * pl + 1];
+            if (ea.p < 0) continue;
             V z = s[pl * ld + row_pad(idx)];
-            long long ra = 2 * p;
             T va = z.x, vb = z.y;
             if (MEAN64) {
-                va += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
-                if (ra + 1 < nrows) vb += (T)mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)(ra + 1)));
+                va += (T)rmean[2 * pl];
+                vb += (T)rmean[2 * pl + 1];
             }
-            T *pd, *qd;
-            dst_rows(I, out, mode, ra, pd, qd);
-            pd[idx] = va;
-            if (qd != pd) qd[idx] = va;
-            if (ra + 1 < nrows) {
-                dst_rows(I, out, mode, ra + 1, pd, qd);
-                pd[idx] = vb;
-                if (qd != pd) qd[idx] = vb;
+            out[ea.p + idx] = va;
+            if (ea.q != ea.p) out[ea.q + idx] = va;
+            if (eb.p >= 0) {
+                out[eb.p + idx] = vb;
+                if (eb.q != eb.p) out[eb.q + idx] = vb;
             }
         }
     }
@@ -344,6 +357,15 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int wv = min(W, nh - col0);
     const int tid = threadIdx.x, nt = blockDim.x;
     V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+    if (line_plan_io(I.lp_mid)) {
+        // first and last stage in global memory; one shared tile for two-stage plans
+        V* tws = s + (I.lp_mid.nst == 2 ? 1 : 2) * N * W;
+        stage_tw_to_smem(I.lp_mid, tw, tws, tid, nt);
+        const GColT<V, 1> g{base, nhp, 0, lgw, wv};
+        const SColT<V, 1> x{s, lgw, 0}, y{s + N * W, lgw, 0};
+        fft_io<V, INV, 1>(g, x, y, g, lgw, I.lp_mid, tws, tid, nt, I.lp_mid.twst[0]);
+        return;
+    }
     if (W * (int)sizeof(V) >= 16) {
         tile_async_load(s, base, nhp, N, lgw, wv, tid, nt);
     } else {
@@ -361,10 +383,14 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     __syncthreads();
     ColLayout<1> lay{lgw, 0};
     s = fft_lines<V, INV>(s, s + N * W, lay, I.lp_mid, tws, tid, nt, I.lp_mid.twst[0]);
+    if (W * (int)sizeof(V) >= 16) {
+        tile_store(base, s, nhp, N, lgw, wv, tid, nt);
+    } else {
 #pragma unroll 4
-    for (int i = tid; i < N * W; i += nt) {
-        const int e = i >> lgw, w = i & (W - 1);
-        if (w < wv) base[(long long)e * nhp + w] = s[i];
+        for (int i = tid; i < N * W; i += nt) {
+            const int e = i >> lgw, w = i & (W - 1);
+            if (w < wv) base[(long long)e * nhp + w] = s[i];
+        }
     }
 }
 
@@ -594,6 +620,9 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     // sym(beta) (1), sym(beta) -> d sigma / d nu (2); all symmetric, 6 components
     constexpr int NIN = 6;
     constexpr int NOUT = 6;
+    V* tws = s + ((9 * cs + 1) & ~1);   // twiddle rows after the 9 slots
+    // forward: all six component tiles staged at once (16-byte asynchronous copies keep the whole
+    // tile in flight), then the axis-0 transforms in shared memory
     if (W * (int)sizeof(V) >= 16) {
 #pragma unroll 1
         for (int c = 0; c < NIN; ++c) tile_async_load(s + c * cs, base + c * cstride, estride, N, lgw, wv, tid, nt);
@@ -609,7 +638,6 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
             }
         }
     }
-    V* tws = s + ((9 * cs + 1) & ~1);   // twiddle rows after the 9 slots
     stage_tw_to_smem(I.lp_first, tw, tws, tid, nt);
     cp_async_wait_all();
     __syncthreads();
@@ -693,13 +721,29 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         }
     }
     __syncthreads();
-    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
+    if (line_plan_io(I.lp_first)) {
+        // inverse transforms from the component slots straight to global memory
+        const SColT<V, 3> scratch{s + 6 * cs, lgw, cs};
 #pragma unroll 1
-    for (int c = 0; c < NOUT; ++c) {
+        for (int g = 0; g < NOUT / 3; ++g) {
+            const SColT<V, 3> slots{s + 3 * g * cs, lgw, cs};
+            const GColT<V, 3> gout{base + 3 * g * cstride, estride, cstride, lgw, wv};
+            fft_io<V, true, 3>(slots, scratch, slots, gout, lgw, I.lp_first, tws, tid, nt, I.lp_first.twst[0]);
+        }
+        return;
+    }
+    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
+    if (W * (int)sizeof(V) >= 16) {
+#pragma unroll 1
+        for (int c = 0; c < NOUT; ++c) tile_store(base + c * cstride, s + c * cs, estride, N, lgw, wv, tid, nt);
+    } else {
+#pragma unroll 1
+        for (int c = 0; c < NOUT; ++c) {
 #pragma unroll 4
-        for (int rem = tid; rem < N * W; rem += nt) {
-            const int e = rem >> lgw, w = rem & (W - 1);
-            if (w < wv) base[c * cstride + e * estride + w] = s[c * cs + rem];
+            for (int rem = tid; rem < N * W; rem += nt) {
+                const int e = rem >> lgw, w = rem & (W - 1);
+                if (w < wv) base[c * cstride + e * estride + w] = s[c * cs + rem];
+            }
         }
     }
 }
