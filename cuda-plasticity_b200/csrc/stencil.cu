@@ -32,12 +32,18 @@ namespace cdd {
 // with D2_i = (D1_i + D1_{i-1}) / 2: the middle argument is the mean of the outer two. It has the
 // sign of both when they agree and its magnitude is never below the smaller of theirs (also after
 // rounding: fl(a + c) / 2 >= min(a, c) for a, c > 0), so the 3-way minmod equals the 2-way one:
-// min(|a|, |c|) with their common sign, 0 when the signs differ or one is zero.
-template <typename T> __device__ __forceinline__ T minmod2(T a, T c) {
-    const T m = fmin(fabs(a), fabs(c));
-    const bool pos = (a > (T)0) & (c > (T)0);
-    const bool neg = (a < (T)0) & (c < (T)0);
-    return pos ? m : (neg ? -m : (T)0);
+// min(|a|, |c|) with their common sign, 0 when the signs differ or one is zero. That is the median
+// of (a, c, 0); FP32 forms it with four min/max operations and no compares or selects:
+// max(min(a, c), min(max(a, c), 0)) (both positive: min(a, c); both negative: max(a, c); else 0).
+// FP64 keeps the compare-and-select form.
+__device__ __forceinline__ float minmod2(float a, float c) {
+    return fmaxf(fminf(a, c), fminf(fmaxf(a, c), 0.0f));
+}
+__device__ __forceinline__ double minmod2(double a, double c) {
+    const double m = fmin(fabs(a), fabs(c));
+    const bool pos = (a > 0.0) & (c > 0.0);
+    const bool neg = (a < 0.0) & (c < 0.0);
+    return pos ? m : (neg ? -m : 0.0);
 }
 
 // 1/sqrt and division: FP32 uses the hardware approximations (<= 2 ulp), FP64 exact ones.
