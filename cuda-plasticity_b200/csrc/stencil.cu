@@ -192,14 +192,27 @@ __device__ __forceinline__ StageConst stage_const(const InstDev& I, const InstCl
     return k;
 }
 
+// Per-thread pointers to the current cell (component 0; components are `cells` apart) and the
+// instance scalars the cell update needs, formed once per block before the march: the march only
+// advances the pointers by one plane, and nothing per cell re-reads the instance table (global
+// stores through `out` would otherwise force those reloads).
+template <typename T> struct CellCtx {
+    const T* sig;   // internal stress (6 components)
+    const T* bn;    // beta_n of the stage updates
+    T* out;         // rhs (flux, stage 1) or the updated state (stages 2, 3)
+    T* spd;         // CFL speed (flux mode, optional)
+    long long cells;
+    T ih;           // 1 / Dx
+    bool has_load, lam_on, glide;
+};
+
 template <typename T, int ND, int MODE, bool GLIDE>
-__device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, bool valid,
-                                             const TileView<T, ND>& tv, const T* bn, T* out,
-                                             const T* __restrict__ sig, T* __restrict__ speed_out,
+__device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>& cx, bool valid,
+                                             const TileView<T, ND>& tv,
                                              const StageConst& kc_block, const InstClock& ck, double t_flux,
                                              double& vmax, double& esum, double& zsum) {
-    const T ih = (T)I.inv_h;
-    const long long cells = I.cells;
+    const T ih = cx.ih;
+    const long long cells = cx.cells;
     // FP32 reads the block's stage constants from shared memory; FP64 (no registers to spare across
     // the march) re-derives them per cell
     StageConst kc_cell;
@@ -211,13 +224,13 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
     constexpr bool PRE = UPD && (sizeof(T) == 4);
     T vn[UPD ? 9 : 1];
     if constexpr (PRE) {
-        const T* un = bn + I.foff + cl;
+        const T* un = cx.bn;
 #pragma unroll
         for (int c = 0; c < 9; ++c) vn[c] = (valid && kc.active) ? un[c * cells] : (T)0;
     }
     const double* ld = kc.ld;
     // total stress at the cell: internal + applied load (FP64), symmetric
-    const T* sp = sig + I.soff + cl;
+    const T* sp = cx.sig;
     T S[3][3];
     {
         T s6[6];
@@ -226,13 +239,13 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
         S[0][0] = (T)((double)s6[0] + ld[0]);
         S[1][1] = (T)((double)s6[3] + ld[1]);
         S[2][2] = (T)((double)s6[5] + ld[2]);
-        if (!I.has_load) { S[0][0] = s6[0]; S[1][1] = s6[3]; S[2][2] = s6[5]; }
+        if (!cx.has_load) { S[0][0] = s6[0]; S[1][1] = s6[3]; S[2][2] = s6[5]; }
         S[0][1] = S[1][0] = s6[1];
         S[0][2] = S[2][0] = s6[2];
         S[1][2] = S[2][1] = s6[4];
     }
-    const bool lam_on = (I.Lambda != 0.0);
-    const bool glide = GLIDE && (I.glide != 0);   // glide-only dynamics (Lambda is 0 then)
+    const bool lam_on = cx.lam_on;
+    const bool glide = GLIDE && cx.glide;   // glide-only dynamics (Lambda is 0 then)
     const T str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / (T)3 * (T)I.Lambda : (T)0;
 
     // ---------------- pass 1: A, P, C, trace ----------------
@@ -513,14 +526,14 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
     // ---------------- outputs ----------------
     if (MODE == M_FLUX) {
         if (valid) {
-            T* o = out + I.foff + cl;
+            T* o = cx.out;
 #pragma unroll
             for (int c = 0; c < 9; ++c) o[c * cells] = rhs[c];
-            if (speed_out) speed_out[I.coff + cl] = spd;
+            if (cx.spd) *cx.spd = spd;
         }
     } else if (MODE == M_STAGE1) {
         if (valid) {
-            T* o = out + I.foff + cl;
+            T* o = cx.out;
 #pragma unroll
             for (int c = 0; c < 9; ++c) o[c * cells] = rhs[c];
             double v = (double)spd;
@@ -537,9 +550,9 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, long long cl, boo
     } else if constexpr (UPD) {
         if (valid && kc.active) {
             const T dt = (T)kc.dt;
-            T* o = out + I.foff + cl;
+            T* o = cx.out;
             if constexpr (!PRE) {
-                const T* un = bn + I.foff + cl;
+                const T* un = cx.bn;
 #pragma unroll
                 for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
             }
@@ -653,6 +666,21 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     if (sizeof(T) == 4 && tid == 0) kc = stage_const<MODE>(I, clk[ii], t_flux);
     __syncthreads();
     double vmax = 0.0, esum = 0.0, zsum = 0.0;
+    // this thread's cell in plane z0 (cell (z0, 0, 0) for threads outside the grid: in-bounds
+    // loads, no stores)
+    CellCtx<T> cx;
+    {
+        const long long cl0 = vxy ? ((long long)z0 * nY + y) * nX + x : (long long)z0 * plane;
+        cx.sig = sig + I.soff + cl0;
+        cx.bn = bn ? bn + I.foff + cl0 : nullptr;   // stage updates only
+        cx.out = out + I.foff + cl0;
+        cx.spd = speed_out ? speed_out + I.coff + cl0 : nullptr;
+        cx.cells = cells;
+        cx.ih = (T)I.inv_h;
+        cx.has_load = I.has_load != 0;
+        cx.lam_on = (I.Lambda != 0.0);
+        cx.glide = (I.glide != 0);
+    }
     TileView<T, ND> tv;
     tv.sm = sm;
     tv.idx = (ty + 2) * RX + tx + OX;
@@ -670,9 +698,11 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         } else {
             tv.so[2] = 0;
         }
-        const long long cl = ((long long)z * nY + y) * nX + x;
-        stencil_cell<T, ND, MODE, GLIDE>(I, vxy ? cl : 0, vxy, tv, bn, out, sig, speed_out, kc, clk[ii], t_flux, vmax,
-                                  esum, zsum);
+        stencil_cell<T, ND, MODE, GLIDE>(I, cx, vxy, tv, kc, clk[ii], t_flux, vmax, esum, zsum);
+        cx.sig += plane;
+        if (cx.bn) cx.bn += plane;
+        cx.out += plane;
+        if (cx.spd) cx.spd += plane;
         if (ND == 3 && more) {
             if (use_tma) {
                 if (NS == 5) {
