@@ -17,6 +17,7 @@ CDD_ERR_NONFINITE = 4
 CDD_ERR_TIMEOUT = 5
 CDD_ERR_UNSUPPORTED = 6
 CDD_ERR_ALLOC = 7
+CDD_ERR_IO = 8
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_SHAPE", 3: "ERR_CUDA", 4: "ERR_NONFINITE",
                 5: "ERR_TIMEOUT", 6: "ERR_UNSUPPORTED", 7: "ERR_ALLOC"}
 
@@ -119,6 +120,21 @@ _PROTOS = {
     "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_field_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_field_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_void_p]),
+    "cdd_ics_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
+                                    ctypes.c_void_p]),
+    "cdd_ics_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "cdd_plas_append": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
+                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "cdd_plas_frames": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+    "cdd_plas_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                     ctypes.c_longlong, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
+                                     ctypes.c_void_p]),
     "cdd_last_error": (ctypes.c_char_p, []),
     "cdd_version": (ctypes.c_char_p, []),
 }

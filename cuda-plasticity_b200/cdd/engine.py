@@ -5,6 +5,7 @@ is a 1-D tensor of ``plan.field_elems`` elements (FP64 or FP32 by plan precision
 occupies ``field_view(t, i)``, shaped ``(9,) + shape`` with the last grid axis contiguous.
 """
 import ctypes
+import os
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -233,6 +234,88 @@ class Plan:
     def check_status(self):
         torch.cuda.current_stream().synchronize()
         check(self.lib.cdd_check_status(self.handle))
+
+    # ------------------------------------------------------------------ reference file formats
+    # The CUDA solver's files keep each of the 9 components with grid axis 0 fastest; see
+    # include/cdd.h (cdd_field_export ... cdd_plas_read) for the .ics and .plas layouts.
+    def _file_prec(self, precision):
+        if precision is None:
+            return _lib.CDD_F64 if self.dtype == torch.float64 else _lib.CDD_F32
+        return {"f64": _lib.CDD_F64, "f32": _lib.CDD_F32}[precision]
+
+    def export_field(self, beta, i=0, precision="f64", stream=None):
+        """Instance i of beta in the files' layout: a device tensor of shape (9,) + the grid
+        reversed (element [c, i2, i1, i0] = component c at (i0, i1, i2))."""
+        self._check_field(beta)
+        code = self._file_prec(precision)
+        out = torch.empty((9,) + tuple(reversed(self.instances[i].shape)),
+                          dtype=torch.float64 if code == _lib.CDD_F64 else torch.float32, device=self.device)
+        check(self.lib.cdd_field_export(self.handle, int(i), ctypes.c_void_p(beta.data_ptr()),
+                                        ctypes.c_void_p(out.data_ptr()), code, _stream(stream)))
+        return out
+
+    def import_field(self, src, beta, i=0, stream=None):
+        """Write a contiguous CUDA tensor in the files' layout (9 * cells FP64 or FP32 values) into
+        instance i of beta."""
+        self._check_field(beta)
+        if not src.is_cuda or not src.is_contiguous() or src.numel() != 9 * self.cells[i] \
+                or src.dtype not in (torch.float64, torch.float32):
+            raise ValueError("src must be a contiguous FP64/FP32 CUDA tensor of 9 * cells values")
+        code = _lib.CDD_F64 if src.dtype == torch.float64 else _lib.CDD_F32
+        check(self.lib.cdd_field_import(self.handle, int(i), ctypes.c_void_p(src.data_ptr()), code,
+                                        ctypes.c_void_p(beta.data_ptr()), _stream(stream)))
+        return beta
+
+    def read_ics(self, path, beta=None, i=0, stream=None):
+        """Load an .ics initial condition (float64) into instance i of beta (a new zero field when
+        None); returns beta."""
+        if beta is None:
+            beta = torch.zeros(self.field_elems, dtype=self.dtype, device=self.device)
+        self._check_field(beta)
+        check(self.lib.cdd_ics_read(self.handle, int(i), os.fsencode(path), ctypes.c_void_p(beta.data_ptr()),
+                                    _stream(stream)))
+        return beta
+
+    def write_ics(self, path, beta, i=0, stream=None):
+        self._check_field(beta)
+        check(self.lib.cdd_ics_write(self.handle, int(i), os.fsencode(path), ctypes.c_void_p(beta.data_ptr()),
+                                     _stream(stream)))
+
+    def append_plas(self, path, t, beta, i=0, precision=None, stream=None):
+        """Append the frame (t, instance i of beta) to a .plas file in `precision` ("f64" or "f32";
+        default: the plan's)."""
+        self._check_field(beta)
+        check(self.lib.cdd_plas_append(self.handle, int(i), os.fsencode(path), float(t),
+                                       ctypes.c_void_p(beta.data_ptr()), self._file_prec(precision),
+                                       _stream(stream)))
+
+    def plas_frames(self, path, i=0, precision=None):
+        n = ctypes.c_longlong(0)
+        check(self.lib.cdd_plas_frames(self.handle, int(i), os.fsencode(path), self._file_prec(precision),
+                                       ctypes.byref(n)))
+        return int(n.value)
+
+    def read_plas(self, path, beta=None, i=0, frame=-1, precision=None, stream=None):
+        """Frame `frame` (negative: from the end) of a .plas file into instance i of beta (a new
+        zero field when None); returns (t, beta)."""
+        if beta is None:
+            beta = torch.zeros(self.field_elems, dtype=self.dtype, device=self.device)
+        self._check_field(beta)
+        t = ctypes.c_double(0.0)
+        check(self.lib.cdd_plas_read(self.handle, int(i), os.fsencode(path), self._file_prec(precision),
+                                     int(frame), ctypes.byref(t), ctypes.c_void_p(beta.data_ptr()),
+                                     _stream(stream)))
+        return float(t.value), beta
+
+    def restart_from_plas(self, path, beta=None, i=0, precision=None, stream=None):
+        """Continue from the last frame of a .plas file, as the CUDA solver's restart does
+        (plasticity.cu L107-123): instance i's field and clock are set from the frame. Returns
+        (t, beta)."""
+        t, beta = self.read_plas(path, beta, i, -1, precision, stream)
+        tt, _, _ = self.get_time()
+        tt[i] = t
+        self.set_time(tt)
+        return t, beta
 
 
 def stress_to_tensor9(s6):

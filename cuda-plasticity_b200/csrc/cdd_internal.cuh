@@ -813,6 +813,10 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
 bool stencil_tma_eligible(const InstDev& I, int precision);
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
 cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st);
+// Convert 9 components between the plan layout (last axis contiguous) and the reference files'
+// layout (axis 0 fastest) of an n0 x n1 x n2 grid (2-D: n0 x 1 x n1); to_file selects the direction.
+cudaError_t launch_field_xpose(bool to_file, const void* src, int src_prec, void* dst, int dst_prec, int n0, int n1,
+                               int n2, cudaStream_t st);
 cudaError_t launch_axpy_f0(const PlanCore& P, const void* u, void* rhs_f0, cudaStream_t st);
 cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st);
 cudaError_t stencil_set_attributes(int precision, size_t smem);

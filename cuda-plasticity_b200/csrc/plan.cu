@@ -1,4 +1,5 @@
 // Plan construction and the C ABI of libcdd (see include/cdd.h).
+#include <cerrno>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -591,6 +592,187 @@ int cdd_flux_with_stress(cdd_plan* p, const void* beta, const void* sigma6, doub
     K.d_sigma = const_cast<void*>(sigma6);
     CDD_CUDA(launch_stencil(K, M_FLUX, beta, beta, rhs, speed, t, user_maps(p, beta), (cudaStream_t)stream));
     return CDD_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// The reference CUDA solver's file formats (.ics, .plas)
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// Grid of instance i as the transpose kernel sees it (2-D (n0, n1) -> (n0, 1, n1)).
+void xpose_dims(const InstDev& I, int& n0, int& n1, int& n2) {
+    if (I.nd == 3) { n0 = I.n0; n1 = I.n1; n2 = I.n2; }
+    else { n0 = I.n0; n1 = 1; n2 = I.n1; }
+}
+
+int check_inst_prec(const cdd_plan* p, int i, int prec) {
+    if (int rc = check_plan(p)) return rc;
+    if (i < 0 || i >= p->core.n_inst) return fail(CDD_ERR_ARG, "instance %d out of range", i);
+    if (prec != CDD_F64 && prec != CDD_F32) return fail(CDD_ERR_ARG, "bad file precision %d", prec);
+    return CDD_OK;
+}
+
+size_t prec_bytes(int prec) { return prec == CDD_F64 ? 8 : 4; }
+
+// Device staging buffer released on scope exit.
+struct StageBuf {
+    void* ptr = nullptr;
+    ~StageBuf() { if (ptr) cudaFree(ptr); }
+};
+
+struct File {
+    FILE* f = nullptr;
+    ~File() { if (f) fclose(f); }
+};
+
+int io_fail(const char* what, const char* path) {
+    return fail(CDD_ERR_IO, "%s '%s': %s", what, path ? path : "(null)", strerror(errno));
+}
+
+// Export instance i to host memory in the file layout and precision.
+int export_to_host(cdd_plan* p, int i, const void* beta, int prec, std::vector<char>& host, cudaStream_t st) {
+    const InstDev& I = p->inst[i];
+    const size_t bytes = 9 * (size_t)I.cells * prec_bytes(prec);
+    StageBuf d;
+    CDD_CUDA(cudaMalloc(&d.ptr, bytes));
+    int n0, n1, n2;
+    xpose_dims(I, n0, n1, n2);
+    const size_t el = prec_bytes(p->core.precision);
+    CDD_CUDA(launch_field_xpose(true, (const char*)beta + I.foff * el, p->core.precision, d.ptr, prec, n0, n1, n2, st));
+    host.resize(bytes);
+    CDD_CUDA(cudaMemcpyAsync(host.data(), d.ptr, bytes, cudaMemcpyDeviceToHost, st));
+    CDD_CUDA(cudaStreamSynchronize(st));
+    return CDD_OK;
+}
+
+// Import a host buffer in the file layout and precision into instance i.
+int import_from_host(cdd_plan* p, int i, const std::vector<char>& host, int prec, void* beta, cudaStream_t st) {
+    const InstDev& I = p->inst[i];
+    const size_t bytes = 9 * (size_t)I.cells * prec_bytes(prec);
+    StageBuf d;
+    CDD_CUDA(cudaMalloc(&d.ptr, bytes));
+    CDD_CUDA(cudaMemcpyAsync(d.ptr, host.data(), bytes, cudaMemcpyHostToDevice, st));
+    int n0, n1, n2;
+    xpose_dims(I, n0, n1, n2);
+    const size_t el = prec_bytes(p->core.precision);
+    CDD_CUDA(launch_field_xpose(false, d.ptr, prec, (char*)beta + I.foff * el, p->core.precision, n0, n1, n2, st));
+    CDD_CUDA(cudaStreamSynchronize(st));
+    return CDD_OK;
+}
+
+long long file_size(FILE* f) {
+    if (fseeko(f, 0, SEEK_END) != 0) return -1;
+    const long long n = (long long)ftello(f);
+    fseeko(f, 0, SEEK_SET);
+    return n;
+}
+
+}  // namespace
+
+int cdd_field_import(cdd_plan* p, int i, const void* src, int src_precision, void* beta, void* stream) {
+    if (int rc = check_inst_prec(p, i, src_precision)) return rc;
+    if (!src || !beta) return fail(CDD_ERR_ARG, "null buffer");
+    const InstDev& I = p->inst[i];
+    int n0, n1, n2;
+    xpose_dims(I, n0, n1, n2);
+    const size_t el = prec_bytes(p->core.precision);
+    CDD_CUDA(launch_field_xpose(false, src, src_precision, (char*)beta + I.foff * el, p->core.precision, n0, n1, n2,
+                                (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_field_export(cdd_plan* p, int i, const void* beta, void* dst, int dst_precision, void* stream) {
+    if (int rc = check_inst_prec(p, i, dst_precision)) return rc;
+    if (!dst || !beta) return fail(CDD_ERR_ARG, "null buffer");
+    const InstDev& I = p->inst[i];
+    int n0, n1, n2;
+    xpose_dims(I, n0, n1, n2);
+    const size_t el = prec_bytes(p->core.precision);
+    CDD_CUDA(launch_field_xpose(true, (const char*)beta + I.foff * el, p->core.precision, dst, dst_precision, n0, n1,
+                                n2, (cudaStream_t)stream));
+    return CDD_OK;
+}
+
+int cdd_ics_read(cdd_plan* p, int i, const char* path, void* beta, void* stream) {
+    if (int rc = check_inst_prec(p, i, CDD_F64)) return rc;
+    if (!path || !beta) return fail(CDD_ERR_ARG, "null argument");
+    File f;
+    f.f = fopen(path, "rb");
+    if (!f.f) return io_fail("cannot open", path);
+    const size_t bytes = 9 * (size_t)p->inst[i].cells * 8;
+    std::vector<char> host(bytes);
+    if (fread(host.data(), 1, bytes, f.f) != bytes)
+        return fail(CDD_ERR_IO, "'%s' holds fewer than the %zu bytes of a 9-component float64 field", path, bytes);
+    return import_from_host(p, i, host, CDD_F64, beta, (cudaStream_t)stream);
+}
+
+int cdd_ics_write(cdd_plan* p, int i, const char* path, const void* beta, void* stream) {
+    if (int rc = check_inst_prec(p, i, CDD_F64)) return rc;
+    if (!path || !beta) return fail(CDD_ERR_ARG, "null argument");
+    std::vector<char> host;
+    if (int rc = export_to_host(p, i, beta, CDD_F64, host, (cudaStream_t)stream)) return rc;
+    File f;
+    f.f = fopen(path, "wb");
+    if (!f.f) return io_fail("cannot create", path);
+    if (fwrite(host.data(), 1, host.size(), f.f) != host.size()) return io_fail("cannot write", path);
+    return CDD_OK;
+}
+
+int cdd_plas_append(cdd_plan* p, int i, const char* path, double t, const void* beta, int file_precision,
+                    void* stream) {
+    if (int rc = check_inst_prec(p, i, file_precision)) return rc;
+    if (!path || !beta) return fail(CDD_ERR_ARG, "null argument");
+    std::vector<char> host;
+    if (int rc = export_to_host(p, i, beta, file_precision, host, (cudaStream_t)stream)) return rc;
+    File f;
+    f.f = fopen(path, "ab");
+    if (!f.f) return io_fail("cannot open", path);
+    const double t64 = t;
+    const float t32 = (float)t;
+    const void* tag = (file_precision == CDD_F64) ? (const void*)&t64 : (const void*)&t32;
+    if (fwrite(tag, 1, prec_bytes(file_precision), f.f) != prec_bytes(file_precision) ||
+        fwrite(host.data(), 1, host.size(), f.f) != host.size() || fflush(f.f) != 0)
+        return io_fail("cannot append to", path);
+    return CDD_OK;
+}
+
+int cdd_plas_frames(cdd_plan* p, int i, const char* path, int file_precision, long long* frames) {
+    if (int rc = check_inst_prec(p, i, file_precision)) return rc;
+    if (!path || !frames) return fail(CDD_ERR_ARG, "null argument");
+    File f;
+    f.f = fopen(path, "rb");
+    if (!f.f) return io_fail("cannot open", path);
+    const long long size = file_size(f.f);
+    if (size < 0) return io_fail("cannot size", path);
+    const long long frame_bytes = (9 * p->inst[i].cells + 1) * (long long)prec_bytes(file_precision);
+    *frames = size / frame_bytes;
+    return CDD_OK;
+}
+
+int cdd_plas_read(cdd_plan* p, int i, const char* path, int file_precision, long long frame, double* t, void* beta,
+                  void* stream) {
+    if (int rc = check_inst_prec(p, i, file_precision)) return rc;
+    if (!path || !beta) return fail(CDD_ERR_ARG, "null argument");
+    File f;
+    f.f = fopen(path, "rb");
+    if (!f.f) return io_fail("cannot open", path);
+    const long long size = file_size(f.f);
+    if (size < 0) return io_fail("cannot size", path);
+    const size_t el = prec_bytes(file_precision);
+    const long long frame_bytes = (9 * p->inst[i].cells + 1) * (long long)el;
+    const long long count = size / frame_bytes;
+    const long long k = frame < 0 ? count + frame : frame;
+    if (k < 0 || k >= count)
+        return fail(CDD_ERR_IO, "'%s' has %lld whole frames; frame %lld does not exist", path, count, frame);
+    if (fseeko(f.f, (off_t)(k * frame_bytes), SEEK_SET) != 0) return io_fail("cannot seek in", path);
+    double t64 = 0.0;
+    float t32 = 0.0f;
+    if (fread(file_precision == CDD_F64 ? (void*)&t64 : (void*)&t32, 1, el, f.f) != el)
+        return io_fail("cannot read", path);
+    std::vector<char> host((size_t)(frame_bytes - (long long)el));
+    if (fread(host.data(), 1, host.size(), f.f) != host.size()) return io_fail("cannot read", path);
+    if (t) *t = (file_precision == CDD_F64) ? t64 : (double)t32;
+    return import_from_host(p, i, host, file_precision, beta, (cudaStream_t)stream);
 }
 
 int cdd_set_time(cdd_plan* p, const double* t, const double* t_end) {

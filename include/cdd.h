@@ -42,7 +42,8 @@ enum cdd_status {
     CDD_ERR_NONFINITE = 4,    /* a wave-speed maximum was NaN/Inf: the step was not applied */
     CDD_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
     CDD_ERR_UNSUPPORTED = 6,  /* option not supported by this build */
-    CDD_ERR_ALLOC = 7         /* device allocation failed */
+    CDD_ERR_ALLOC = 7,        /* device allocation failed */
+    CDD_ERR_IO = 8            /* a file could not be opened, read or written, or is too short */
 };
 
 enum cdd_precision { CDD_F64 = 0, CDD_F32 = 1 };
@@ -257,6 +258,39 @@ int cdd_stress_noalloc(const cdd_instance* inst, int precision, const void* beta
                        void* stream);
 
 /* Message for the calling thread's last failing call ("" if none). */
+/* ---- The reference CUDA solver's on-disk formats ----
+ * File layout of one field: the 9 components in the order xx xy xz yx yy yz zx zy zz, each with
+ * grid axis 0 fastest (element (i0, i1, i2) at i0 + n0 (i1 + n1 i2); 2-D: i0 + n0 i1): the
+ * reference writes every component transposed (Plasticity/RunCUDA.py L9-22, convertStateToCUDA)
+ * and reads it back transposed (Plasticity/FieldInitializers/FieldInitializer.py L61-103,
+ * LoadStateRaw). A plan stores each component with the last axis contiguous.
+ *  .ics : one field in float64, no time (read by plasticity.cu L126-140 with ReadDoubleMatrixFile,
+ *         assist.h L65-97; written by convertStateToCUDA).
+ *  .plas: frames [t][field], t and the field in the file's precision (the solver's data_type:
+ *         float64 or float32), appended by ContinueWriteMatrix (assist.h L164-192,
+ *         plasticity.cu L153-159); a restart continues from the last frame (plasticity.cu L107-123).
+ * `beta` is always the plan's packed field; i selects the instance whose part is converted.
+ * The file functions synchronise `stream` and stage through a temporary device buffer. */
+
+/* Device conversion between instance i's part of beta and a device buffer in the file layout
+ * (9 * cells elements of src_precision / dst_precision; FP64 -> FP32 rounds to nearest). */
+int cdd_field_import(cdd_plan* plan, int i, const void* src, int src_precision, void* beta, void* stream);
+int cdd_field_export(cdd_plan* plan, int i, const void* beta, void* dst, int dst_precision, void* stream);
+
+/* .ics: read the first 9 * cells float64 values of `path` into instance i; write instance i. */
+int cdd_ics_read(cdd_plan* plan, int i, const char* path, void* beta, void* stream);
+int cdd_ics_write(cdd_plan* plan, int i, const char* path, const void* beta, void* stream);
+
+/* .plas: append the frame (t, instance i) in file_precision (creating the file); count the whole
+ * frames of a file (a trailing partial frame is ignored, as LoadStateRaw does); read frame
+ * `frame` (0-based; negative counts from the end, -1 = the last frame, the restart state) into
+ * instance i and its time into *t. */
+int cdd_plas_append(cdd_plan* plan, int i, const char* path, double t, const void* beta, int file_precision,
+                    void* stream);
+int cdd_plas_frames(cdd_plan* plan, int i, const char* path, int file_precision, long long* frames);
+int cdd_plas_read(cdd_plan* plan, int i, const char* path, int file_precision, long long frame, double* t,
+                  void* beta, void* stream);
+
 const char* cdd_last_error(void);
 
 /* Library version string. */

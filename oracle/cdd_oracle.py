@@ -434,3 +434,48 @@ def run(beta, t0, t_end, p, max_steps=None, observer=None):
             observer(t, beta)
         if t >= t_end or (max_steps is not None and n >= max_steps):
             return beta, t
+
+
+# ----------------------------------------------------------------------------------------------
+# The reference CUDA solver's on-disk formats: convertStateToCUDA (Plasticity/RunCUDA.py L9-22)
+# writes every component transposed (grid axis 0 fastest); ContinueWriteMatrix (assist.h
+# L164-192) appends frames [t][field] in the solver's data_type; LoadStateRaw
+# (Plasticity/FieldInitializers/FieldInitializer.py L61-103) reads them back.
+# ----------------------------------------------------------------------------------------------
+def to_file_layout(field):
+    """(9,) + grid -> (9,) + reversed grid: component c transposed (all axes reversed)."""
+    return np.stack([np.ascontiguousarray(np.asarray(c).transpose()) for c in field])
+
+
+def from_file_layout(data, shape):
+    """Inverse of to_file_layout for a flat array of 9 * prod(shape) values."""
+    d = np.asarray(data).reshape((9,) + tuple(reversed(shape)))
+    return np.stack([np.ascontiguousarray(c.transpose()) for c in d])
+
+
+def ics_bytes(field):
+    """An .ics initial condition: the field in the file layout as float64, no time."""
+    return to_file_layout(np.asarray(field, dtype=np.float64)).tobytes()
+
+
+def plas_frame_bytes(t, field, dtype=np.float64):
+    """One .plas frame: the time, then the field in the file layout, both in `dtype`."""
+    dtype = np.dtype(dtype)
+    return np.array([t], dtype=dtype).tobytes() + to_file_layout(np.asarray(field).astype(dtype)).tobytes()
+
+
+def read_plas(raw, shape, dtype=np.float64, time=None):
+    """(t, field) of the frame LoadStateRaw selects: the last one (time None) or the first with
+    t >= time (the last read when none is), from the bytes of a .plas file."""
+    dtype = np.dtype(dtype)
+    n = 9 * int(np.prod(shape))
+    frame = (n + 1) * dtype.itemsize
+    count = len(raw) // frame
+    k = count - 1
+    if time is not None:
+        for k in range(count):
+            if np.frombuffer(raw, dtype, 1, k * frame)[0] >= time:
+                break
+    t = np.frombuffer(raw, dtype, 1, k * frame)[0]
+    data = np.frombuffer(raw, dtype, n, k * frame + dtype.itemsize)
+    return float(t), from_file_layout(data, shape)

@@ -17,6 +17,9 @@ CentralUpwindHJBetaPDynamics.py (2-D, the module RunPython.py imports), and
 ``TVDRungeKutta_FieldMover.CalculateOneAdaptiveTimeStep`` -- on seeded inputs from
 ``cdd.initial.gaussian_random_field`` and writes ``*.npz`` fixtures next to this file.
 
+``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
+LoadStateRaw run from their source text (``run_io_case``).
+
 Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only NAME]``.
 Only this script reads the reference tree; tests read the committed ``.npz`` files.
 """
@@ -175,6 +178,73 @@ def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.
           % (name, shape, steps, out["wall_s"], os.path.relpath(path, REPO)))
 
 
+# ---- the CUDA solver's file formats: the reference's own writer and reader, run from their source
+# text (their modules do not import under Python 3: RunCUDA.py needs simplejson and Configure,
+# FieldInitializer.py state classes and scipy names that are gone), with two more mechanical
+# patches: (vii) ``numpy.fromstring(`` -> ``numpy.frombuffer(`` (binary fromstring is removed in
+# numpy 2) and (viii) ``tp = range(dim)`` -> ``tp = list(range(dim))`` (a Python-3 range has no
+# reverse()).
+IO_PATCHES = [("numpy.fromstring(", "numpy.frombuffer("), ("tp = range(dim)", "tp = list(range(dim))")]
+
+
+def _reference_function(reference, rel, name, patches=()):
+    with open(os.path.join(reference, "Plasticity", rel)) as f:
+        src = f.read().expandtabs(8)
+    m = re.search(r"^def %s\(.*?(?=^\S)" % name, src, flags=re.M | re.S)
+    text = _patch(m.group(0))
+    for a, b in patches:
+        text = text.replace(a, b)
+    return text
+
+
+def run_io_case(reference, name="io_formats"):
+    """convertStateToCUDA (RunCUDA.py L9-22) writes .ics bytes of seeded states; .plas files of
+    three frames [t][field] are framed as ContinueWriteMatrix does (assist.h L164-192: the time in
+    the data type, then the field in the .ics layout); LoadStateRaw (FieldInitializer.py L61-103)
+    reads them back (last frame, and the first frame with t >= 0.15), in float64 and float32."""
+    import tempfile
+    PlasticityState, GridArray = _import_reference()[:2]
+    ns = {"numpy": np, "PlasticityState": PlasticityState, "GridArray": GridArray}
+    exec(_reference_function(reference, "RunCUDA.py", "convertStateToCUDA"), ns)
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "ReformatState"), ns)
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "LoadStateRaw", IO_PATCHES), ns)
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for dim, N, seed in ((3, 8, 21), (2, 12, 22)):
+            shape = (N,) * dim
+            rng = np.random.default_rng(seed)
+            fields = [rng.standard_normal((9,) + shape) for _ in range(3)]
+            times = [0.1, 0.2, 0.3]
+            ics = []
+            for k, f in enumerate(fields):
+                st = PlasticityState.PlasticityState(shape)
+                for c, comp in enumerate(COMPONENTS):
+                    st.betaP[comp] = GridArray.GridArray(f[c].copy())
+                path = os.path.join(tmp, "s%d.ics" % k)
+                ns["convertStateToCUDA"](st, path)
+                with open(path, "rb") as fh:
+                    ics.append(fh.read())
+            key = "%dd" % dim
+            out["fields_" + key] = np.stack(fields)
+            out["times_" + key] = np.array(times)
+            out["ics_" + key] = np.frombuffer(ics[0], np.uint8)
+            for dt in ("float64", "float32"):
+                raw = b"".join(np.array([t], dt).tobytes() + np.frombuffer(b, np.float64).astype(dt).tobytes()
+                               for t, b in zip(times, ics))
+                path = os.path.join(tmp, "run_%s.plas" % dt)
+                with open(path, "wb") as fh:
+                    fh.write(raw)
+                out["plas_%s_%s" % (key, dt)] = np.frombuffer(raw, np.uint8)
+                for tag, tsel in (("last", None), ("t015", 0.15)):
+                    t, st = ns["LoadStateRaw"](path, N, dim, time=tsel, dtype=dt)
+                    out["load_%s_%s_%s_t" % (key, dt, tag)] = np.asarray(t, dtype=np.float64).reshape(-1)
+                    out["load_%s_%s_%s" % (key, dt, tag)] = np.stack(
+                        [np.asarray(st.betaP[comp]) for comp in COMPONENTS])
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
+
+
 CASES = {
     # one flux, one step and 10 steps of 3-D glide+climb dynamics
     "g3d_16": dict(shape=(16, 16, 16), sigma_f=0.05, seed=1, steps=10),
@@ -207,6 +277,8 @@ def main():
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     build_patched_copy(args.reference)
+    if args.only in (None, "io_formats"):
+        run_io_case(args.reference)
     for name, kw in CASES.items():
         if args.only and name != args.only:
             continue
