@@ -116,50 +116,47 @@ class PlasticityState:
         e = (sq - self.nu / (1.0 + self.nu) * tr * tr) / (4.0 * self.mu)
         return GridArray.GridArray(e.cpu().numpy())
 
-    def CalculateBetaElastic(self, type='k'):
-        """beta^E = IFFT(kmask T beta^P) - beta^P on the host (PlasticityState.py L357-390).
+    def _observe(self, kind):
+        """A k-space observable of this state's beta^P on the GPU (cdd.Plan.observe), as host FP64."""
+        plan = self._engine()
+        out = plan.observe(kind, plan.pack_state(self))
+        return plan.observable_view(out, 0, kind).detach().to('cpu').double().numpy()
 
-        T contracted with beta^P^ is k_i g_j with g_j = k_j (A s / kSq - B r / kSqSq)
-        + (p_j + q_j) / kSq (s = trace, p_j = k_m b_mj, q_j = b_jn k_n, r = k_m q_m).
-        """
-        K = FourierSpaceTools.FourierSpaceTools(self.gridShape)
-        k = [numpy.asarray(K.kx), numpy.asarray(K.ky), numpy.asarray(K.kz)]
-        kSq = numpy.asarray(K.kSq) + ME
-        kSqSq = numpy.asarray(K.kSqSq) + ME
-        lamb = 2. * self.mu * self.nu / (1. - 2. * self.nu)
-        A = lamb / (lamb + 2. * self.mu)
-        B = 2. * (lamb + self.mu) / (lamb + 2. * self.mu)
-        bh = numpy.fft.rfftn(self.betaP.stack(), axes=tuple(range(1, self.dimension + 1)))
-        b = lambda i, j: bh[3 * i + j]
-        s = b(0, 0) + b(1, 1) + b(2, 2)
-        p = [k[0] * b(0, j) + k[1] * b(1, j) + k[2] * b(2, j) for j in range(3)]
-        q = [b(j, 0) * k[0] + b(j, 1) * k[1] + b(j, 2) * k[2] for j in range(3)]
-        r = k[0] * q[0] + k[1] * q[1] + k[2] * q[2]
-        c = A * s / kSq - B * r / kSqSq
-        g = [k[j] * c + (p[j] + q[j]) / kSq for j in range(3)]
-        mask = numpy.asarray(K.kmask)
-        out = numpy.stack([mask * k[i] * g[j] for i in range(3) for j in range(3)])
-        be = numpy.fft.irfftn(out, s=self.gridShape, axes=tuple(range(1, self.dimension + 1)))
-        return Fields.from_stack(self.gridShape, be - self.betaP.stack())
+    def CalculateBetaElastic(self, type='k'):
+        """beta^E = IFFT(kmask T beta^P^) - beta^P (PlasticityState.py L357-390), on the GPU."""
+        if type != 'k':
+            raise NotImplementedError("CalculateBetaElastic supports type='k' on the GPU")
+        return Fields.from_stack(self.gridShape, self._observe("beta_elastic"))
+
+    def CalculateRotationField(self, type='k'):
+        """rotE_ij = (beta^E_ij - beta^E_ji) / 2 (PlasticityState.py L435-446), on the GPU."""
+        if type != 'k':
+            raise NotImplementedError("CalculateRotationField supports type='k' on the GPU")
+        w = self._observe("rotation")   # xy, xz, yz
+        full = numpy.zeros((9,) + tuple(self.gridShape))
+        for c, (i, j) in enumerate(((0, 1), (0, 2), (1, 2))):
+            full[3 * i + j] = w[c]
+            full[3 * j + i] = -w[c]
+        return Fields.from_stack(self.gridShape, full)
+
+    def CalculateRotationRodrigues(self, type='k', source='betaP'):
+        """Rodrigues rotation vector (PlasticityState.py L447-494), on the GPU: source 'betaP' (the
+        reference's default) from beta^P's transform, 'betaE' from the rotation field."""
+        if type != 'k' or source not in ('betaP', 'betaE'):
+            raise NotImplementedError("CalculateRotationRodrigues supports type='k', source='betaP'/'betaE'")
+        if source == 'betaP':
+            rod = self._observe("rodrigues")
+        else:
+            w = self._observe("rotation")
+            rod = numpy.stack([w[2], -w[1], w[0]])
+        return Fields.from_stack(self.gridShape, rod, components=[x, y, z])
 
     def CalculateRhoFourier(self, type='k'):
         """Nye dislocation density rho_ij = -eps_ikl d_k betaP_lj by Fourier derivatives
-        (PlasticityState.py L264-304), on the host."""
-        K = FourierSpaceTools.FourierSpaceTools(self.gridShape)
-        Kb = self.betaP.FFT()
-        ks = [K.kx, K.ky, K.kz]
-        D = [Kb * (1.0j * ks[d]) for d in range(self.dimension if self.dimension > 1 else 1)]
-        Kr = Fields.TensorField(self.gridShape, kspace=True)
-        for i in (x, y, z):
-            if self.dimension == 3:
-                Kr[x, i] = D[2][y, i] - D[1][z, i]
-                Kr[y, i] = D[0][z, i] - D[2][x, i]
-                Kr[z, i] = D[1][x, i] - D[0][y, i]
-            elif self.dimension == 2:
-                Kr[x, i] = -D[1][z, i]
-                Kr[y, i] = D[0][z, i]
-                Kr[z, i] = D[1][x, i] - D[0][y, i]
-        return Kr.IFFT()
+        (PlasticityState.py L264-304), on the GPU."""
+        if type != 'k':
+            raise NotImplementedError("CalculateRhoFourier supports type='k' on the GPU")
+        return Fields.from_stack(self.gridShape, self._observe("rho"))
 
     # ---------------------------------------------------------------- state algebra
     def _combine(self, other, op):

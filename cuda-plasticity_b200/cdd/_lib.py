@@ -18,6 +18,10 @@ CDD_ERR_TIMEOUT = 5
 CDD_ERR_UNSUPPORTED = 6
 CDD_ERR_ALLOC = 7
 CDD_ERR_IO = 8
+CDD_OBS_BETA_ELASTIC = 0
+CDD_OBS_ROTATION = 1
+CDD_OBS_RODRIGUES = 2
+CDD_OBS_RHO = 3
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_SHAPE", 3: "ERR_CUDA", 4: "ERR_NONFINITE",
                 5: "ERR_TIMEOUT", 6: "ERR_UNSUPPORTED", 7: "ERR_ALLOC"}
 
@@ -120,6 +124,8 @@ _PROTOS = {
     "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_observe_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
     "cdd_field_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_field_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

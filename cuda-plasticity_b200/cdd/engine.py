@@ -235,6 +235,32 @@ class Plan:
         torch.cuda.current_stream().synchronize()
         check(self.lib.cdd_check_status(self.handle))
 
+    # ------------------------------------------------------------------ field observables
+    # name -> (cdd_observable, components); see cdd_observe_field in include/cdd.h
+    OBSERVABLES = {"beta_elastic": (_lib.CDD_OBS_BETA_ELASTIC, 9), "rotation": (_lib.CDD_OBS_ROTATION, 3),
+                   "rodrigues": (_lib.CDD_OBS_RODRIGUES, 3), "rho": (_lib.CDD_OBS_RHO, 9)}
+
+    def observe(self, kind, beta, out=None, stream=None):
+        """A k-space field observable of every instance of beta: "beta_elastic" (9 components),
+        "rotation" (3: xy, xz, yz of the antisymmetric part of beta^E), "rodrigues" (3: x, y, z,
+        from beta^P) or "rho" (9: the Nye density). Returns a packed buffer; ``observable_view``
+        gives instance i."""
+        self._check_field(beta)
+        code, nc = self.OBSERVABLES[kind]
+        n = self.field_elems if nc == 9 else self.field_elems // 3
+        if out is None:
+            out = torch.empty(n, dtype=self.dtype, device=self.device)
+        elif out.numel() != n or out.dtype != self.dtype or not out.is_contiguous():
+            raise ValueError("out must be a contiguous %s tensor of %d elements" % (self.dtype, n))
+        check(self.lib.cdd_observe_field(self.handle, code, ctypes.c_void_p(beta.data_ptr()),
+                                         ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+        return out
+
+    def observable_view(self, buf, i, kind):
+        nc = self.OBSERVABLES[kind][1]
+        o = self.field_offsets[i] * nc // 9
+        return buf[o:o + nc * self.cells[i]].view((nc,) + tuple(self.instances[i].shape))
+
     # ------------------------------------------------------------------ reference file formats
     # The CUDA solver's files keep each of the 9 components with grid axis 0 fastest; see
     # include/cdd.h (cdd_field_export ... cdd_plas_read) for the .ics and .plas layouts.

@@ -158,7 +158,10 @@ __device__ __forceinline__ void stage_tw_to_smem(const LinePlan& lp, const V* __
 struct RowPtr {
     long long p, q;
 };
-__host__ __device__ constexpr size_t rows_table_bytes(int P) { return 16 + (size_t)2 * P * (sizeof(RowPtr) + sizeof(double)); }
+// (C2R also keeps a second table of epilogue source rows; the R2C pass uses the first part only.)
+__host__ __device__ constexpr size_t rows_table_bytes(int P) {
+    return 16 + (size_t)2 * P * (2 * sizeof(RowPtr) + sizeof(double));
+}
 // The table starts 16-byte aligned after the twiddle rows (tws: twspan complex values).
 template <typename V> __device__ __forceinline__ RowPtr* rows_table(V* tws, int twspan) {
     return reinterpret_cast<RowPtr*>(tws + ((twspan + 1) & ~1));
@@ -767,6 +770,8 @@ struct PlanCore {
     double* d_obs = nullptr;         // per-instance energy, mean zz (2 per instance)
     int* d_status = nullptr;
     LaunchShape pass[NUM_PASSES];
+    LaunchShape pass9[NUM_PASSES];   // the k-space observables: 9-component row / axis-1 passes, 12-slot k-space pass
+    bool obs_ok = false;             // pass9 fits the device (shared memory of the 12-slot k-space pass)
     LaunchShape stencil;
     LaunchShape cellwise;            // elementwise kernels over cells
     LaunchShape obs;                 // observables: one thread per cell
@@ -813,6 +818,8 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
 bool stencil_tma_eligible(const InstDev& I, int precision);
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
 cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st);
+// k-space observables of beta (kind: cdd_observable); out in the packed 9- or 3-component layout.
+cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st);
 // Convert 9 components between the plan layout (last axis contiguous) and the reference files'
 // layout (axis 0 fastest) of an n0 x n1 x n2 grid (2-D: n0 x 1 x n1); to_file selects the direction.
 cudaError_t launch_field_xpose(bool to_file, const void* src, int src_prec, void* dst, int dst_prec, int n0, int n1,

@@ -165,6 +165,9 @@ int build_shapes(cdd_plan* p, size_t elt) {
     size_t smem_max[NUM_PASSES] = {0, 0, 0, 0, 0};
     int n_tma = 0;
     int thr_max[NUM_PASSES] = {0, 0, 0, 0, 0};
+    std::vector<int> pre9[NUM_PASSES];   // the observables' launch shapes (9 components)
+    for (int k = 0; k < NUM_PASSES; ++k) pre9[k].push_back(0);
+    size_t smem_green12 = 0;
     for (int i = 0; i < n; ++i) {
         InstDev& I = p->inst[i];
         // rows kernels (R2C: 9 components, C2R: 6); ping-pong buffers of P padded rows
@@ -230,6 +233,19 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (t.threads > thr_max[PASS_GREEN]) thr_max[PASS_GREEN] = t.threads;
         }
         for (int k = 0; k < NUM_PASSES; ++k) pre[k].push_back(pre[k].back() + I.tile[k].blocks);
+        {
+            // the observables carry up to 9 components through the row and axis-1 passes and keep
+            // 9 + 3 component slots in the k-space pass
+            const long long np9 = (9LL * I.rows + 1) / 2;
+            const int P = I.tile[PASS_R2C].lines;
+            const int b_rows = (int)((np9 + P - 1) / P);
+            const int b_mid = (I.nd == 3) ? 9 * I.n0 * I.tile[PASS_MID_F].tiles_a : 0;
+            const int b9[NUM_PASSES] = {b_rows, b_mid, I.tile[PASS_GREEN].blocks, b_mid, b_rows};
+            for (int k = 0; k < NUM_PASSES; ++k) pre9[k].push_back(pre9[k].back() + b9[k]);
+            const int W = I.tile[PASS_GREEN].lines;
+            const size_t sm = ((size_t)12 * (I.n0 * W + W) + 1) / 2 * 2 * velt + (size_t)I.lp_first.twspan * velt;
+            if (sm > smem_green12) smem_green12 = sm;
+        }
         stencil_geometry(I, p->tune[i].stencil_planes);
         // effective launch shapes of this instance
         p->tune[i].rows_lines = I.tile[PASS_R2C].lines;
@@ -260,6 +276,21 @@ int build_shapes(cdd_plan* p, size_t elt) {
         if (L.smem > smem_all) smem_all = L.smem;
         CDD_CUDA(dalloc(p, (void**)&L.d_pre, sizeof(int) * (n + 1)));
         CDD_CUDA(cudaMemcpy(L.d_pre, pre[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        LaunchShape& L9 = C.pass9[k];
+        L9.blocks = pre9[k].back();
+        L9.threads = L.threads;
+        L9.smem = (k == PASS_GREEN) ? smem_green12 : L.smem;
+        if (L9.smem > smem_all) smem_all = L9.smem;
+        CDD_CUDA(dalloc(p, (void**)&L9.d_pre, sizeof(int) * (n + 1)));
+        CDD_CUDA(cudaMemcpy(L9.d_pre, pre9[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
+    {
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        C.obs_ok = !(optin > 0 && smem_green12 + 1024 > (size_t)optin);
+        if (!C.obs_ok) C.pass9[PASS_GREEN].smem = C.pass[PASS_GREEN].smem;   // never launched
+        if (C.pass9[PASS_GREEN].smem > smem_all) smem_all = C.pass9[PASS_GREEN].smem;
     }
     C.stencil.blocks = pre_st.back();
     C.stencil.threads = 256;
@@ -773,6 +804,17 @@ int cdd_plas_read(cdd_plan* p, int i, const char* path, int file_precision, long
     if (fread(host.data(), 1, host.size(), f.f) != host.size()) return io_fail("cannot read", path);
     if (t) *t = (file_precision == CDD_F64) ? t64 : (double)t32;
     return import_from_host(p, i, host, file_precision, beta, (cudaStream_t)stream);
+}
+
+int cdd_observe_field(cdd_plan* p, int kind, const void* beta, void* out, void* stream) {
+    if (int rc = check_plan(p)) return rc;
+    if (!beta || !out) return fail(CDD_ERR_ARG, "null buffer");
+    if (kind < CDD_OBS_BETA_ELASTIC || kind > CDD_OBS_RHO) return fail(CDD_ERR_ARG, "bad observable %d", kind);
+    if (!p->core.obs_ok)
+        return fail(CDD_ERR_SHAPE, "the k-space observables need more shared memory than the device has for this "
+                                   "axis-0 length");
+    CDD_CUDA(launch_observable(p->core, kind, beta, out, (cudaStream_t)stream));
+    return CDD_OK;
 }
 
 int cdd_set_time(cdd_plan* p, const double* t, const double* t_end) {

@@ -62,17 +62,22 @@ __device__ __forceinline__ double mean_stress(const InstDev& I, const double* m,
 
 // The stress depends on beta only through its symmetric part s = (beta + beta^T) / 2 (every term of
 // the Green contraction and of sigma is symmetric in beta), so the transforms carry 6 components.
-// Source rows of the 6-component R2C input, row ra = component o * rows + r:
+// Source rows of the R2C input, row ra = component o * rows + r:
 //   RS_STRESS: row ra of a 6-component stress-layout array (p == q);
-//   RS_SYM:    rows of beta_ij and beta_ji (p == q on the diagonal).
+//   RS_SYM:    rows of beta_ij and beta_ji (p == q on the diagonal), 6 components;
+//   RS_FULL:   row ra of a 9-component field (p == q), all 9 components.
 // The value is (p + q) / 2, exact when p == q.
-enum RowSource { RS_STRESS = 1, RS_SYM = 2 };
+enum RowSource { RS_STRESS = 1, RS_SYM = 2, RS_FULL = 3 };
 
 template <typename T>
 __device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mode, long long ra, const T*& p,
                                          const T*& q) {
     if (mode == RS_STRESS) {
         p = q = base + I.soff + ra * I.nl;
+        return;
+    }
+    if (mode == RS_FULL) {
+        p = q = base + I.foff + ra * I.nl;
         return;
     }
     const int o = fdiv_q(I.fd_rows, (int)ra);
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
                                                   const T* __restrict__ beta,
                                                   typename VecOf<T>::type* __restrict__ spec,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  double* __restrict__ rowsum, int mode) {
+                                                  double* __restrict__ rowsum, int mode, int ncomp) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -100,7 +105,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_R2C].lines, ld = rows_ld(N);
-    const long long nrows = 6LL * I.rows;
+    const long long nrows = (long long)ncomp * I.rows;
+    if (2LL * lb * P >= nrows) return;   // launch sized for more components than this pass carries
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const T half = (T)0.5;
@@ -206,12 +212,33 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
 //                 that of its symmetric part: d/d beta_ij = d/d beta_ji = the symmetric entry).
 // The imaginary parts of the k = 0 and Nyquist bins are dropped (numpy irfft semantics).
 // ------------------------------------------------------------------------------------------
-enum RowDest { RD_STRESS = 0, RD_SYM_FIELD = 1 };
+//   RD_FIELD9 / RD_FIELD3: row ra of a packed 9- / 3-component array (instance offsets foff and
+//                 foff / 3), with an optional epilogue (RowEpilogue).
+enum RowDest { RD_STRESS = 0, RD_SYM_FIELD = 1, RD_FIELD9 = 2, RD_FIELD3 = 3 };
+
+// Real-space terms the observables subtract from the inverse transform of output component c:
+// out_c -= coef (beta[EPI_P[c]] - beta[EPI_Q[c]]) (EPI_Q < 0: no second term). beta^E: -beta^P;
+// rotation (xy, xz, yz) and Rodrigues vector (x, y, z): minus the antisymmetric part of beta^P
+// (PlasticityState.py L357-390, L435-446, L447-475).
+enum RowEpilogue { EPI_NONE = 0, EPI_BETA_E = 1, EPI_ROTATION = 2, EPI_RODRIGUES = 3 };
+__device__ __constant__ int EPI_P[4][9] = {{-1, -1, -1, -1, -1, -1, -1, -1, -1},
+                                           {0, 1, 2, 3, 4, 5, 6, 7, 8},
+                                           {1, 2, 5, -1, -1, -1, -1, -1, -1},
+                                           {5, 6, 1, -1, -1, -1, -1, -1, -1}};
+__device__ __constant__ int EPI_Q[4][9] = {{-1, -1, -1, -1, -1, -1, -1, -1, -1},
+                                           {-1, -1, -1, -1, -1, -1, -1, -1, -1},
+                                           {3, 6, 7, -1, -1, -1, -1, -1, -1},
+                                           {7, 2, 3, -1, -1, -1, -1, -1, -1}};
+__device__ __constant__ double EPI_COEF[4] = {0.0, 1.0, 0.5, 0.5};
 
 template <typename T>
 __device__ __forceinline__ void dst_rows(const InstDev& I, T* base, int mode, long long ra, T*& p, T*& q) {
     if (mode == RD_STRESS) {
         p = q = base + I.soff + ra * I.nl;
+        return;
+    }
+    if (mode == RD_FIELD9 || mode == RD_FIELD3) {
+        p = q = base + (mode == RD_FIELD9 ? I.foff : I.foff / 3) + ra * I.nl;
         return;
     }
     const int o = fdiv_q(I.fd_rows, (int)ra);
@@ -221,13 +248,37 @@ __device__ __forceinline__ void dst_rows(const InstDev& I, T* base, int mode, lo
     q = base + I.foff + (long long)(3 * j + i) * I.cells + r * I.nl;
 }
 
+// out -= coef (beta[e.p + idx ..] - beta[e.q + idx ..]) for four (epilogue4) or one value.
+__device__ __forceinline__ void load4c(const float* p, float* v) {
+    float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void load4c(const double* p, double* v) {
+    double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+template <typename T>
+__device__ __forceinline__ void epilogue4(const T* beta, const RowPtr& e, T coef, int idx, T* v) {
+    T a[4], b[4] = {0, 0, 0, 0};
+    load4c(beta + e.p + idx, a);
+    if (e.q >= 0) load4c(beta + e.q + idx, b);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] -= coef * (a[q] - b[q]);
+}
+template <typename T>
+__device__ __forceinline__ T epilogue1(const T* beta, const RowPtr& e, T coef, int idx, T v) {
+    const T b = e.q >= 0 ? beta[e.q + idx] : (T)0;
+    return v - coef * (beta[e.p + idx] - b);
+}
+
 template <typename T, bool MEAN64>
 __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restrict__ insts, int n_inst,
                                                   const int* __restrict__ pre,
                                                   const typename VecOf<T>::type* __restrict__ spec,
                                                   T* __restrict__ out,
                                                   const typename VecOf<T>::type* __restrict__ tw,
-                                                  const double* __restrict__ sbar, int mode) {
+                                                  const double* __restrict__ sbar, int mode, int ncomp,
+                                                  const T* __restrict__ beta, int epi) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -235,7 +286,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     const int N = I.nl, P = I.tile[PASS_C2R].lines, ld = rows_ld(N), nh = I.nh;
-    const long long nrows = 6LL * I.rows;
+    const long long nrows = (long long)ncomp * I.rows;
+    if (2LL * lb * P >= nrows) return;   // launch sized for more components than this pass carries
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
@@ -266,11 +318,13 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     // row table: the destination rows of each of the block's 2P rows and their FP64 mean stress
     RowPtr* rt = rows_table(tws, I.lp_last.twspan);
-    double* rmean = reinterpret_cast<double*>(rt + 2 * P);
+    RowPtr* re = rt + 2 * P;                                        // epilogue source rows
+    double* rmean = reinterpret_cast<double*>(re + 2 * P);          // mean stress or epilogue coefficient
     for (int r = tid; r < 2 * P; r += nt) {
         const long long ra = 2LL * lb * P + r;
-        RowPtr e;
+        RowPtr e, ep;
         e.p = e.q = -1;
+        ep.p = ep.q = -1;
         double m = 0.0;
         if (ra < nrows) {
             T *pd, *qd;
@@ -278,15 +332,25 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
             e.p = pd - out;
             e.q = qd - out;
             if (MEAN64) m = mean_stress(I, sbar + 9 * ii, fdiv_q(I.fd_rows, (int)ra));
+            if (epi != EPI_NONE) {
+                const int o = fdiv_q(I.fd_rows, (int)ra);
+                const long long rr = ra - (long long)o * I.rows;
+                const int cp = EPI_P[epi][o], cq = EPI_Q[epi][o];
+                ep.p = I.foff + (long long)cp * I.cells + rr * I.nl;
+                ep.q = cq >= 0 ? I.foff + (long long)cq * I.cells + rr * I.nl : -1;
+                m = EPI_COEF[epi];
+            }
         }
         rt[r] = e;
+        re[r] = ep;
         rmean[r] = m;
     }
     __syncthreads();
     RowLayout lay{P, ld};
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tws, tid, nt, I.lp_last.twst[0]);
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(out + I.soff)) & 15) == 0) &&
-                     ((((uintptr_t)(out + I.foff)) & 15) == 0) && ((I.cells & 3) == 0);
+                     ((((uintptr_t)(out + I.foff)) & 15) == 0) && ((((uintptr_t)(out + I.foff / 3)) & 15) == 0) &&
+                     (epi == EPI_NONE || ((((uintptr_t)(beta + I.foff)) & 15) == 0)) && ((I.cells & 3) == 0);
     if (vec) {
 #pragma unroll 2
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
@@ -302,6 +366,10 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
                 const T ma = (T)rmean[2 * pl], mb = (T)rmean[2 * pl + 1];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) { va[q] += ma; vb[q] += mb; }
+            }
+            if (epi != EPI_NONE) {
+                epilogue4(beta, re[2 * pl], (T)rmean[2 * pl], idx, va);
+                if (eb.p >= 0) epilogue4(beta, re[2 * pl + 1], (T)rmean[2 * pl + 1], idx, vb);
             }
             store4(out + ea.p + idx, va);
             if (ea.q != ea.p) store4(out + ea.q + idx, va);
@@ -320,6 +388,10 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
             if (MEAN64) {
                 va += (T)rmean[2 * pl];
                 vb += (T)rmean[2 * pl + 1];
+            }
+            if (epi != EPI_NONE) {
+                va = epilogue1(beta, re[2 * pl], (T)rmean[2 * pl], idx, va);
+                if (eb.p >= 0) vb = epilogue1(beta, re[2 * pl + 1], (T)rmean[2 * pl + 1], idx, vb);
             }
             out[ea.p + idx] = va;
             if (ea.q != ea.p) out[ea.q + idx] = va;
@@ -340,7 +412,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
                                                  const int* __restrict__ pre,
                                                  typename VecOf<T>::type* __restrict__ spec,
                                                  const typename VecOf<T>::type* __restrict__ tw,
-                                                 int pass) {
+                                                 int pass, int ncomp) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -352,6 +424,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int ta = lb % ta_n; lb /= ta_n;
     const int i0 = lb % I.n0;
     const int c = lb / I.n0;
+    if (c >= ncomp) return;   // launch sized for more components than this pass carries
     const int N = I.n1, nhp = I.nhp, nh = I.nh;
     const int col0 = ta * W;
     const int wv = min(W, nh - col0);
@@ -567,14 +640,106 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
     }
 }
 
-// Shared memory: 9 component slots of N x W (+W pad): slots 0..5 hold the 6 components, 6..8
-// are the ping-pong scratch. The transforms run three components at a time against the scratch;
-// when the stage count is odd the result is copied back to the component slots.
+// ---- k-space observables (PlasticityState.py) ----
+// Component counts of the k-space pass per mode (see k_green) and its shared-memory slots (inputs
+// or outputs, whichever are more, plus three scratch slots).
+__host__ __device__ constexpr int green_nin(int gmode) { return gmode == 6 ? 9 : 6; }
+__host__ __device__ constexpr int green_nout(int gmode) {
+    return (gmode == 3 || gmode == 6) ? 9 : ((gmode == 4 || gmode == 5) ? 3 : 6);
+}
+__host__ __device__ constexpr int green_slots(int gmode) {
+    return (green_nin(gmode) > green_nout(gmode) ? green_nin(gmode) : green_nout(gmode)) + 3;
+}
+
+// One k point of an observable, scaled by 1 / cells for the inverse transform:
+//  3: beta^E before the real-space -beta^P term (CalculateBetaElastic L357-390):
+//     kmask sum_mn T_ijmn b_mn = kmask k_i g_j with g as in green_point and, b entering through
+//     its symmetric part, p = q = sym(b) k;
+//  4: its antisymmetric part (k_i g_j - k_j g_i) / 2 for (xy, xz, yz) (CalculateRotationField
+//     L435-446);
+//  5: the Rodrigues vector from beta^P (CalculateRotationRodrigues L447-475, source 'betaP'):
+//     kmask sum_jst k_j (e_ijt k_s + e_ijs k_t) b_st / (2 kSq) = kmask (k x q)_i / kSq;
+//  6: the Nye density rho_ai = -e_akl d_k b_li by Fourier derivatives (CalculateRhoFourier
+//     L264-304): rho_xi = i (kz b_yi - ky b_zi), rho_yi = i (kx b_zi - kz b_xi),
+//     rho_zi = i (ky b_xi - kx b_yi) (kz = 0 in 2-D), no mask.
+// Inputs: 6 symmetric components xx xy xz yy yz zz (3-5) or all 9 (6).
+template <typename T, typename V, int GMODE>
+__device__ __forceinline__ void obs_point(const V* b, V* o, T kx, T ky, T kz, bool kzero, T A, T B, T scale) {
+    const T k[3] = {kx, ky, kz};
+    if constexpr (GMODE == 6) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const V bx = b[i], by = b[3 + i], bz = b[6 + i];
+            V u[3];
+            u[0].x = kz * by.x - ky * bz.x; u[0].y = kz * by.y - ky * bz.y;
+            u[1].x = kx * bz.x - kz * bx.x; u[1].y = kx * bz.y - kz * bx.y;
+            u[2].x = ky * bx.x - kx * by.x; u[2].y = ky * bx.y - kx * by.y;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {   // multiply by i
+                o[3 * a + i].x = -u[a].y * scale;
+                o[3 * a + i].y = u[a].x * scale;
+            }
+        }
+        return;
+    } else {
+        const V b9[9] = {b[0], b[1], b[2], b[1], b[3], b[4], b[2], b[4], b[5]};
+        const T ksq = kx * kx + ky * ky + kz * kz;
+        const T ikse = (T)1 / (ksq + (T)ME);
+        const T mask = kzero ? (T)0 : (T)1;
+        V q[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            q[j].x = b9[3 * j].x * k[0] + b9[3 * j + 1].x * k[1] + b9[3 * j + 2].x * k[2];
+            q[j].y = b9[3 * j].y * k[0] + b9[3 * j + 1].y * k[1] + b9[3 * j + 2].y * k[2];
+        }
+        if constexpr (GMODE == 5) {
+            const T f = mask * ikse * scale;
+            o[0].x = f * (k[1] * q[2].x - k[2] * q[1].x); o[0].y = f * (k[1] * q[2].y - k[2] * q[1].y);
+            o[1].x = f * (k[2] * q[0].x - k[0] * q[2].x); o[1].y = f * (k[2] * q[0].y - k[0] * q[2].y);
+            o[2].x = f * (k[0] * q[1].x - k[1] * q[0].x); o[2].y = f * (k[0] * q[1].y - k[1] * q[0].y);
+            return;
+        } else {
+            const T ikqe = (T)1 / (ksq * ksq + (T)ME);
+            V s1 = vadd(vadd(b9[0], b9[4]), b9[8]);
+            V r;
+            r.x = k[0] * q[0].x + k[1] * q[1].x + k[2] * q[2].x;
+            r.y = k[0] * q[0].y + k[1] * q[1].y + k[2] * q[2].y;
+            V cc;
+            cc.x = A * s1.x * ikse - B * r.x * ikqe;
+            cc.y = A * s1.y * ikse - B * r.y * ikqe;
+            V g[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                g[j].x = mask * scale * (k[j] * cc.x + (q[j].x + q[j].x) * ikse);
+                g[j].y = mask * scale * (k[j] * cc.y + (q[j].y + q[j].y) * ikse);
+            }
+            if constexpr (GMODE == 3) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) { o[3 * i + j].x = k[i] * g[j].x; o[3 * i + j].y = k[i] * g[j].y; }
+            } else {
+                const int ia[3] = {0, 0, 1}, ja[3] = {1, 2, 2};
+                const T hf = (T)0.5;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int i = ia[c], j = ja[c];
+                    o[c].x = hf * (k[i] * g[j].x - k[j] * g[i].x);
+                    o[c].y = hf * (k[i] * g[j].y - k[j] * g[i].y);
+                }
+            }
+        }
+    }
+}
+
+// Shared memory: component slots of N x W (+W pad), the last three being the ping-pong scratch
+// (slot `scr` on). The transforms run three components at a time against the scratch; when the
+// stage count is odd the result is copied back to the component slots.
 template <typename V, bool INV>
 __device__ __forceinline__ void fft_group3(V* s, int g, int lgw, int cs, const LinePlan& lp,
-                                           const V* __restrict__ tws, int tid, int nt) {
+                                           const V* __restrict__ tws, int tid, int nt, int scr) {
     V* a = s + 3 * g * cs;
-    V* b = s + 6 * cs;   // slots 6..8: scratch
+    V* b = s + scr * cs;   // scratch slots
     ColLayout<3> lay{lgw, cs};
     V* r = fft_lines<V, INV>(a, b, lay, lp, tws, tid, nt, lp.twst[0]);
     if (r != a) {
@@ -617,10 +782,13 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     V* base = spec + I.spoff + (I.nd == 3 ? (long long)i1 * nhp : 0) + col0;
 
     // components in / out of the k-space pass: sym(beta) -> sigma (0), sigma cotangent -> cotangent of
-    // sym(beta) (1), sym(beta) -> d sigma / d nu (2); all symmetric, 6 components
-    constexpr int NIN = 6;
-    constexpr int NOUT = 6;
-    V* tws = s + ((9 * cs + 1) & ~1);   // twiddle rows after the 9 slots
+    // sym(beta) (1), sym(beta) -> d sigma / d nu (2), all 6 -> 6; the observables sym(beta) ->
+    // beta^E (3, 6 -> 9), -> rotation (4, 6 -> 3), -> Rodrigues vector (5, 6 -> 3), beta -> Nye
+    // density (6, 9 -> 9)
+    constexpr int NIN = green_nin(GMODE);
+    constexpr int NOUT = green_nout(GMODE);
+    constexpr int SCR = green_slots(GMODE) - 3;   // first scratch slot
+    V* tws = s + ((green_slots(GMODE) * cs + 1) & ~1);   // twiddle rows after the slots
     // forward: all six component tiles staged at once (16-byte asynchronous copies keep the whole
     // tile in flight), then the axis-0 transforms in shared memory
     if (W * (int)sizeof(V) >= 16) {
@@ -641,7 +809,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     stage_tw_to_smem(I.lp_first, tw, tws, tid, nt);
     cp_async_wait_all();
     __syncthreads();
-    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
+    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -669,9 +837,11 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         V b[NIN], o[NOUT];
 #pragma unroll
         for (int c = 0; c < NIN; ++c) b[c] = s[c * cs + i];
-        // the symmetric 3 x 3 matrix of the six components (row-major, b9[3i + j])
-        const V b9[9] = {b[0], b[1], b[2], b[1], b[3], b[4], b[2], b[4], b[5]};
-        if constexpr (GMODE == 0) {
+        if constexpr (GMODE >= 3) {
+            obs_point<T, V, GMODE>(b, o, kx, ky, kz, kzero, A, B, scale);
+        } else if constexpr (GMODE == 0) {
+            // the symmetric 3 x 3 matrix of the six components (row-major, b9[3i + j])
+            const V b9[9] = {b[0], b[1], b[2], b[1], b[3], b[4], b[2], b[4], b[5]};
             V ph;
             green_point<T, V>(b9, o, kx, ky, kz, kzero, lam, mu, A, B, scale, MEAN64, phib ? &ph : nullptr);
             if (phib) phib[e * estride + w] = ph;
@@ -702,6 +872,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
             o[4].x = hf * (bb[5].x + bb[7].x); o[4].y = hf * (bb[5].y + bb[7].y);
             o[5] = bb[8];
         } else {
+            const V b9[9] = {b[0], b[1], b[2], b[1], b[3], b[4], b[2], b[4], b[5]};
             green_point_dnu<T, V>(b9, o, kx, ky, kz, kzero, lam, mu, A, B, scale, (T)I.nu);
         }
 #pragma unroll
@@ -723,7 +894,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     __syncthreads();
     if (line_plan_io(I.lp_first)) {
         // inverse transforms from the component slots straight to global memory
-        const SColT<V, 3> scratch{s + 6 * cs, lgw, cs};
+        const SColT<V, 3> scratch{s + SCR * cs, lgw, cs};
 #pragma unroll 1
         for (int g = 0; g < NOUT / 3; ++g) {
             const SColT<V, 3> slots{s + 3 * g * cs, lgw, cs};
@@ -732,7 +903,7 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         }
         return;
     }
-    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt);
+    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
     if (W * (int)sizeof(V) >= 16) {
 #pragma unroll 1
         for (int c = 0; c < NOUT; ++c) tile_store(base + c * cstride, s + c * cs, estride, N, lgw, wv, tid, nt);
@@ -796,15 +967,15 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     const LaunchShape* L = P.pass;
     if (f32) {
         k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM, 6);
         k_mean_beta<<<dim3(P.n_inst, 6), 1024, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, RS_SYM);
+            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, RS_SYM, 6);
     }
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6);
     if (f32)
         k_green<T, true, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
@@ -813,13 +984,13 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6);
     if (f32)
         k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS, 6, nullptr, EPI_NONE);
     else
         k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS, 6, nullptr, EPI_NONE);
     return cudaGetLastError();
 }
 
@@ -834,17 +1005,17 @@ static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* o
     const V* tw = (const V*)P.d_tw;
     const LaunchShape* L = P.pass;
     k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, GMODE == 1 ? RS_STRESS : RS_SYM);
+        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, GMODE == 1 ? RS_STRESS : RS_SYM, 6);
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F);
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6);
     k_green<T, false, GMODE><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
         P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, part);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I);
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6);
     k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, GMODE == 1 ? RD_SYM_FIELD : RD_STRESS);
+        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, GMODE == 1 ? RD_SYM_FIELD : RD_STRESS, 6, nullptr, EPI_NONE);
     return cudaGetLastError();
 }
 
@@ -857,6 +1028,52 @@ cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* 
 cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st) {
     if (P.precision == CDD_F32) return run_stress_variant<float, 2>(P, beta, out6, nullptr, nullptr, st);
     return run_stress_variant<double, 2>(P, beta, out6, nullptr, nullptr, st);
+}
+
+// k-space observables: forward transforms of sym(beta) (6 components, the stress passes' launch
+// shapes) or of all 9 components (the 9-component shapes), the observable's k-space operator in the
+// fused axis-0 pass, inverse transforms of its 9 or 3 components with the real-space epilogue.
+// No FP64 mean path: every operator's k = 0 mode is zero (kmask, or a factor k).
+template <typename T, int GMODE>
+static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out, cudaStream_t st) {
+    typedef typename VecOf<T>::type V;
+    V* spec = (V*)P.d_spec;
+    const V* tw = (const V*)P.d_tw;
+    constexpr int NIN = green_nin(GMODE), NOUT = green_nout(GMODE);
+    constexpr int EPI = GMODE == 3 ? EPI_BETA_E : (GMODE == 4 ? EPI_ROTATION : (GMODE == 5 ? EPI_RODRIGUES : EPI_NONE));
+    const LaunchShape* LI = (NIN == 9) ? P.pass9 : P.pass;
+    const LaunchShape* LO = (NOUT == 9) ? P.pass9 : P.pass;
+    const LaunchShape& LG = P.pass9[PASS_GREEN];
+    k_r2c_rows<T, false><<<LI[PASS_R2C].blocks, LI[PASS_R2C].threads, LI[PASS_R2C].smem, st>>>(
+        P.d_inst, P.n_inst, LI[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, NIN == 9 ? RS_FULL : RS_SYM, NIN);
+    if (LI[PASS_MID_F].blocks > 0)
+        k_fft_mid<T, false><<<LI[PASS_MID_F].blocks, LI[PASS_MID_F].threads, LI[PASS_MID_F].smem, st>>>(
+            P.d_inst, P.n_inst, LI[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, NIN);
+    k_green<T, false, GMODE><<<LG.blocks, LG.threads, LG.smem, st>>>(P.d_inst, P.n_inst, LG.d_pre, spec, tw,
+                                                                      (const T*)P.d_k, nullptr, nullptr);
+    if (LO[PASS_MID_I].blocks > 0)
+        k_fft_mid<T, true><<<LO[PASS_MID_I].blocks, LO[PASS_MID_I].threads, LO[PASS_MID_I].smem, st>>>(
+            P.d_inst, P.n_inst, LO[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, NOUT);
+    k_c2r_rows<T, false><<<LO[PASS_C2R].blocks, LO[PASS_C2R].threads, LO[PASS_C2R].smem, st>>>(
+        P.d_inst, P.n_inst, LO[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, NOUT == 9 ? RD_FIELD9 : RD_FIELD3, NOUT,
+        (const T*)beta, EPI);
+    return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t run_observable_t(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st) {
+    switch (kind) {
+        case CDD_OBS_BETA_ELASTIC: return run_observable<T, 3>(P, beta, out, st);
+        case CDD_OBS_ROTATION: return run_observable<T, 4>(P, beta, out, st);
+        case CDD_OBS_RODRIGUES: return run_observable<T, 5>(P, beta, out, st);
+        case CDD_OBS_RHO: return run_observable<T, 6>(P, beta, out, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st) {
+    if (P.precision == CDD_F32) return run_observable_t<float>(P, kind, beta, out, st);
+    return run_observable_t<double>(P, kind, beta, out, st);
 }
 
 cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st, void* phi) {
@@ -877,6 +1094,10 @@ static cudaError_t set_attr_t(size_t smem) {
     if ((e = set_dyn_smem_limit(k_green<T, false, 0>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 1>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 2>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 3>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 4>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 5>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 6>, smem))) return e;
     return cudaSuccess;
 }
 

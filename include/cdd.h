@@ -258,6 +258,23 @@ int cdd_stress_noalloc(const cdd_instance* inst, int precision, const void* beta
                        void* stream);
 
 /* Message for the calling thread's last failing call ("" if none). */
+/* ---- Field observables in k space (PlasticityState.py) ----
+ * out: a packed field buffer of the plan's precision. 9-component observables are written in the
+ * field layout (instance i at cdd_plan_field_offset(i)); 3-component ones in a packed 3-component
+ * layout (instance i at cdd_plan_field_offset(i) / 3, components back to back, cells apart).
+ *  CDD_OBS_BETA_ELASTIC: beta^E = IFFT(kmask T beta^P^) - beta^P, 9 components
+ *                        (CalculateBetaElastic L357-390);
+ *  CDD_OBS_ROTATION:     (beta^E_ij - beta^E_ji) / 2 for (xy, xz, yz), 3 components
+ *                        (CalculateRotationField L435-446: the other entries follow by antisymmetry);
+ *  CDD_OBS_RODRIGUES:    the Rodrigues rotation vector (x, y, z) from beta^P, 3 components
+ *                        (CalculateRotationRodrigues L447-475, source 'betaP');
+ *  CDD_OBS_RHO:          the Nye dislocation density rho_ij = -eps_ikl d_k beta^P_lj by Fourier
+ *                        derivatives, 9 components (CalculateRhoFourier L264-304).
+ * Uses the plan's spectrum scratch (stream-ordered with the other entry points). CDD_ERR_SHAPE when
+ * the k-space pass of 12 component slots does not fit the device's shared memory. */
+enum cdd_observable { CDD_OBS_BETA_ELASTIC = 0, CDD_OBS_ROTATION = 1, CDD_OBS_RODRIGUES = 2, CDD_OBS_RHO = 3 };
+int cdd_observe_field(cdd_plan* plan, int kind, const void* beta, void* out, void* stream);
+
 /* ---- The reference CUDA solver's on-disk formats ----
  * File layout of one field: the 9 components in the order xx xy xz yx yy yz zx zy zz, each with
  * grid axis 0 fastest (element (i0, i1, i2) at i0 + n0 (i1 + n1 i2); 2-D: i0 + n0 i1): the

@@ -479,3 +479,61 @@ def read_plas(raw, shape, dtype=np.float64, time=None):
     t = np.frombuffer(raw, dtype, 1, k * frame)[0]
     data = np.frombuffer(raw, dtype, n, k * frame + dtype.itemsize)
     return float(t), from_file_layout(data, shape)
+
+
+# ----------------------------------------------------------------------------------------------
+# Field observables: PlasticityState.CalculateRhoFourier L264-304, CalculateRotationField
+# L435-446, CalculateRotationRodrigues L447-475 (source 'betaP'); beta_elastic above is
+# CalculateBetaElastic L357-390.
+# ----------------------------------------------------------------------------------------------
+PERM = np.zeros((3, 3, 3))                        # Constants.py L16-22
+PERM[0, 1, 2] = PERM[1, 2, 0] = PERM[2, 0, 1] = 1.
+PERM[0, 2, 1] = PERM[2, 1, 0] = PERM[1, 0, 2] = -1.
+
+
+def rho_fourier(beta):
+    """Nye density rho_ij = -eps_ikl d_k beta_lj with Fourier derivatives d_k -> i k_k (no kmask)."""
+    shape = beta.shape[1:]
+    axes = tuple(range(-len(shape), 0))
+    Kb = np.fft.rfftn(beta, axes=axes)
+    k = k_tables(shape)[0]
+    D = [Kb * (1.0j * k[d]) for d in range(len(shape))]
+    Kr = np.zeros_like(Kb)
+    for i in range(3):
+        if len(shape) == 3:
+            Kr[ci(0, i)] = D[2][ci(1, i)] - D[1][ci(2, i)]
+            Kr[ci(1, i)] = D[0][ci(2, i)] - D[2][ci(0, i)]
+            Kr[ci(2, i)] = D[1][ci(0, i)] - D[0][ci(1, i)]
+        else:
+            Kr[ci(0, i)] = -D[1][ci(2, i)]
+            Kr[ci(1, i)] = D[0][ci(2, i)]
+            Kr[ci(2, i)] = D[1][ci(0, i)] - D[0][ci(1, i)]
+    return np.fft.irfftn(Kr, s=shape, axes=axes)
+
+
+def rotation_field(beta, mu, nu):
+    """rotE_ij = (betaE_ij - betaE_ji) / 2, 9 components."""
+    be = beta_elastic(beta, mu, nu)
+    return np.stack([(be[ci(i, j)] - be[ci(j, i)]) / 2. for i in range(3) for j in range(3)])
+
+
+def rodrigues(beta):
+    """Rodrigues vector (x, y, z) from beta^P: IFFT(kmask sum k_j (e_ijt k_s + e_ijs k_t) b_st /
+    kSq / 2) minus the antisymmetric part of beta^P."""
+    shape = beta.shape[1:]
+    axes = tuple(range(-len(shape), 0))
+    Kb = np.fft.rfftn(beta, axes=axes)
+    k, kSq0, _, kmask = k_tables(shape)
+    kSq = kSq0 + ME
+    Kr = np.zeros((3,) + Kb.shape[1:], dtype=complex)
+    for i in range(3):
+        for s in range(3):
+            for t in range(3):
+                for j in range(3):
+                    Kr[i] += k[j] * (PERM[i, j, t] * k[s] + PERM[i, j, s] * k[t]) * Kb[ci(s, t)] / kSq / 2.
+        Kr[i] *= kmask
+    rod = np.fft.irfftn(Kr, s=shape, axes=axes)
+    rod[0] -= (beta[ci(1, 2)] - beta[ci(2, 1)]) / 2.
+    rod[1] -= (beta[ci(2, 0)] - beta[ci(0, 2)]) / 2.
+    rod[2] -= (beta[ci(0, 1)] - beta[ci(1, 0)]) / 2.
+    return rod

@@ -17,7 +17,8 @@ CentralUpwindHJBetaPDynamics.py (2-D, the module RunPython.py imports), and
 ``TVDRungeKutta_FieldMover.CalculateOneAdaptiveTimeStep`` -- on seeded inputs from
 ``cdd.initial.gaussian_random_field`` and writes ``*.npz`` fixtures next to this file.
 
-``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
+``observables.npz`` holds the field observables of PlasticityState (beta^E, rotation, Rodrigues
+vector, Nye density) of seeded fields. ``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
 LoadStateRaw run from their source text (``run_io_case``).
 
 Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only NAME]``.
@@ -245,6 +246,31 @@ def run_io_case(reference, name="io_formats"):
     print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
 
 
+def run_observables_case(name="observables"):
+    """The field observables of PlasticityState (CalculateBetaElastic L357-390, CalculateRotationField
+    L435-446, CalculateRotationRodrigues L447-475 with source 'betaP', CalculateRhoFourier L264-304)
+    of seeded fields: a cubic and a non-cubic 3-D grid and a 2-D grid."""
+    PlasticityState, GridArray = _import_reference()[:2]
+    sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
+    from cdd.initial import gaussian_random_field
+    out = {}
+    for key, shape, seed in (("c", (8, 8, 8), 41), ("a", (6, 8, 12), 42), ("2d", (16, 16), 43)):
+        beta = gaussian_random_field(shape, 0.06, 0.05, seed)
+        st = PlasticityState.PlasticityState(shape, mu=1.0, nu=0.3)
+        for c, comp in enumerate(COMPONENTS):
+            st.betaP[comp] = GridArray.GridArray(beta[c].copy())
+        stack9 = lambda f: np.stack([np.asarray(f[comp]) for comp in COMPONENTS])
+        out["beta_" + key] = beta
+        out["betaE_" + key] = stack9(st.CalculateBetaElastic())
+        out["rot_" + key] = stack9(st.CalculateRotationField())
+        rod = st.CalculateRotationRodrigues()
+        out["rod_" + key] = np.stack([np.asarray(rod[a]) for a in "xyz"])
+        out["rho_" + key] = stack9(st.CalculateRhoFourier())
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
+
+
 CASES = {
     # one flux, one step and 10 steps of 3-D glide+climb dynamics
     "g3d_16": dict(shape=(16, 16, 16), sigma_f=0.05, seed=1, steps=10),
@@ -279,6 +305,8 @@ def main():
     build_patched_copy(args.reference)
     if args.only in (None, "io_formats"):
         run_io_case(args.reference)
+    if args.only in (None, "observables"):
+        run_observables_case()
     for name, kw in CASES.items():
         if args.only and name != args.only:
             continue
