@@ -30,6 +30,11 @@ WORDS_PER_CELL_STAGE = 48      # stress operator: read 9 + write 6; stencil + st
 STRESS_WORDS = 15               # stress operator: read beta 9, write sigma 6
 FLUX_WORDS = 24                 # stencil, flux form: read beta 9 + sigma 6, write rhs 9
 FLUX_TRAFFIC_BYTES_PER_CELL = 117.1   # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
+# executed FP32 operations (add + mul + 2 fma) and thread instructions per cell of the FP32 flux-form
+# stencil, from ncu's instruction counters at 192^3
+FLUX_FLOP_PER_CELL = 1312.4
+FLUX_INST_PER_CELL = 1967.0
+FLUX_COUNTS_SOURCE = "profiles/k_stencil_flux_flops_192cube.md"
 
 
 def parse():
@@ -45,8 +50,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
-    ap.add_argument("--only-flux", action="store_true",
-                    help="run three flux evaluations of the workload and exit (for profiling the stencil)")
+    ap.add_argument("--only-flux", nargs="?", const="f32", default=None, choices=["f32", "f64"],
+                    help="run three flux evaluations of the workload at the given precision and exit "
+                         "(for profiling the stencil)")
     return ap.parse_args()
 
 
@@ -142,6 +148,33 @@ def workload(size, seed):
     inst = cdd.Instance(shape, mu=1.0, nu=0.3, Lambda=0.0, cfl=0.25,
                         load_rate=(-0.025, -0.025, 0.05))
     return shape, inst
+
+
+def gemm_peak_tflops(dev, dtype, n=8192, reps=5):
+    """Dense GEMM throughput of cuBLAS (through torch, TF32 off) on this GPU: the measured
+    CUDA-core (FP32) or FP64 peak the stencil's FLOP rate is compared with."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(n, n, device=dev, dtype=dtype)
+        b = torch.randn(n, n, device=dev, dtype=dtype)
+        c = torch.empty(n, n, device=dev, dtype=dtype)
+        for _ in range(2):
+            torch.mm(a, b, out=c)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            torch.mm(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        s = e0.elapsed_time(e1) / 1e3 / reps
+        del a, b, c
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / s / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
 
 
 def peaks():
@@ -324,13 +357,13 @@ def main():
         return ev0.elapsed_time(ev1) / 1e3
 
     if args.only_flux:
-        p = cdd.Plan([inst], "f32", tuning=None if args.no_tune else "auto")
+        p = cdd.Plan([inst], args.only_flux, tuning=None if args.no_tune else "auto")
         b = p.empty_field()
-        b.copy_(b0.reshape(-1).to(torch.float32))
+        b.copy_(b0.reshape(-1).to(p.dtype))
         for _ in range(3):
             p.flux(b, 0.0, want_speed=False)
         torch.cuda.synchronize()
-        print(json.dumps({"only_flux": True, "grid": list(shape), "launch_shapes": p.tuning(0)}))
+        print(json.dumps({"only_flux": args.only_flux, "grid": list(shape), "launch_shapes": p.tuning(0)}))
         return
 
     clocks.start()
@@ -442,6 +475,10 @@ def main():
         return
 
     peak, peak_kind = peaks()
+    fp32_peak = gemm_peak_tflops(dev, torch.float32)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    issue_peak = nsm * 4 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e9   # warp instructions per ns
+    issue_ach = FLUX_INST_PER_CELL / 32 * cells / t_stencil / 1e9
     stage_s = el32 / K / 3
     achieved = WORDS_PER_CELL_STAGE * 4 * cells / stage_s / 1e9
     launches_per_step = 3 * 6 + 3 + 2
@@ -466,6 +503,14 @@ def main():
                      "algorithmic_bytes_per_launch": FLUX_WORDS * 4 * cells,
                      "traffic": FLUX_TRAFFIC_BYTES_PER_CELL * cells,
                      "traffic_source": "profiles/k_stencil_flux_192cube_fp32.md (117.1 B/cell at 192^3, scaled)",
+                     "flop": {"bound": "fp32", "flop_per_cell": FLUX_FLOP_PER_CELL,
+                              "achieved": FLUX_FLOP_PER_CELL * cells / t_stencil / 1e12, "peak": fp32_peak,
+                              "unit": "TFLOP/s", "frac": FLUX_FLOP_PER_CELL * cells / t_stencil / 1e12 / fp32_peak,
+                              "peak_kind": "measured: cuBLAS FP32 GEMM (TF32 off), 8192^3, this run",
+                              "counts_source": FLUX_COUNTS_SOURCE},
+                     "issue": {"thread_inst_per_cell": FLUX_INST_PER_CELL, "achieved_ginst_s": issue_ach,
+                               "peak_ginst_s": issue_peak, "frac": issue_ach / issue_peak,
+                               "peak_kind": "4 warp instructions per cycle per SM at the median SM clock of the run"},
                      "step": {"achieved": achieved, "frac": achieved / peak,
                               "algorithmic_bytes_per_cell_stage": WORDS_PER_CELL_STAGE * 4},
                      "per_operator": {
