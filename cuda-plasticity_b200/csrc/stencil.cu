@@ -129,12 +129,24 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
 // u+ and u- from the five values u_{-2} .. u_{+2} along one axis. The limiter arguments D1, D2
 // of FindDerivatives all carry 1/h^2; minmod is positively homogeneous, so the kernel limits the
 // undivided second differences and applies 1/h once: u+ = (d_0 - mm/2) / h, u- = (d_-1 + mm_-1/2) / h.
+// The two limiters of one axis share their middle argument em1: minmod(a, em1) is the median of
+// (a, em1, 0), i.e. a clamped to [min(em1, 0), max(em1, 0)], so FP32 forms those bounds once.
+__device__ __forceinline__ void minmod_pair(float e0, float em1, float em2, float& dd0, float& ddm) {
+    const float lo = fminf(em1, 0.0f), hi = fmaxf(em1, 0.0f);
+    dd0 = fminf(fmaxf(e0, lo), hi);
+    ddm = fminf(fmaxf(em2, lo), hi);
+}
+__device__ __forceinline__ void minmod_pair(double e0, double em1, double em2, double& dd0, double& ddm) {
+    dd0 = minmod2(e0, em1);
+    ddm = minmod2(em1, em2);
+}
+
 template <typename T>
 __device__ __forceinline__ void derivs5(const T* v, T ih, T& up, T& um) {
     const T dm2 = v[1] - v[0], dm1 = v[2] - v[1], d0 = v[3] - v[2], d1 = v[4] - v[3];
     const T e0 = d1 - d0, em1 = d0 - dm1, em2 = dm1 - dm2;
-    const T dd0 = minmod2(e0, em1);
-    const T ddm = minmod2(em1, em2);
+    T dd0, ddm;
+    minmod_pair(e0, em1, em2, dd0, ddm);
     up = (d0 - (T)0.5 * dd0) * ih;
     um = (dm1 + (T)0.5 * ddm) * ih;
 }
@@ -693,8 +705,15 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         }
         if (use_tma && NS == 6 && more) issued = k + 5;
         if (ND == 3) {
+            // ring planes z-2 .. z+2 live in slots (k + q) mod NS: rotate by one plane per step
+            if (k == 0) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) tv.so[q] = ((k + q) % NS) * 9 * PP;
+                for (int q = 0; q < 5; ++q) tv.so[q] = q * 9 * PP;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) tv.so[q] = tv.so[q + 1];
+                tv.so[4] = (tv.so[3] + 9 * PP == NS * 9 * PP) ? 0 : tv.so[3] + 9 * PP;
+            }
         } else {
             tv.so[2] = 0;
         }
