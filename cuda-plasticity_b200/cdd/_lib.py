@@ -44,6 +44,11 @@ class cdd_instance(ctypes.Structure):
         ("load_mu", ctypes.c_double),
         ("load_nu", ctypes.c_double),
         ("dynamics", ctypes.c_int),
+        ("vacancy", ctypes.c_int),
+        ("vac_alpha", ctypes.c_double),
+        ("vac_beta", ctypes.c_double),
+        ("vac_gamma", ctypes.c_double),
+        ("dt_max", ctypes.c_double),
     ]
 
 
@@ -124,6 +129,7 @@ _PROTOS = {
     "cdd_stress_dnu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_stress_noalloc": (ctypes.c_int, [ctypes.POINTER(cdd_instance), ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "cdd_set_vacancy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "cdd_observe_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "cdd_field_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,

@@ -30,6 +30,10 @@ class Instance:
     load_mu: Optional[float] = None
     load_nu: Optional[float] = None
     glide_only: bool = False   # the glide-only dynamics (CentralUpwindHJBetaPGlideOnlyDynamics.py)
+    # vacancy coupling (VacancyDynamics.py): (alpha, beta, gamma) of sigma_ii -= alpha c,
+    # c += beta d tr(beta^P), diffusion constant gamma; None: no vacancies
+    vacancy: Optional[Sequence[float]] = None
+    dt_max: float = 0.0        # > 0: upper bound of the adaptive step (the splitting mover's dtBound)
 
     def to_c(self):
         c = _lib.cdd_instance()
@@ -47,6 +51,10 @@ class Instance:
         c.load_mu = float(self.mu if self.load_mu is None else self.load_mu)
         c.load_nu = float(self.nu if self.load_nu is None else self.load_nu)
         c.dynamics = _lib.CDD_DYN_GLIDE_ONLY if self.glide_only else _lib.CDD_DYN_GLIDE_CLIMB
+        c.vacancy = 0 if self.vacancy is None else 1
+        if self.vacancy is not None:
+            c.vac_alpha, c.vac_beta, c.vac_gamma = (float(v) for v in self.vacancy)
+        c.dt_max = float(self.dt_max)
         return c
 
     @property
@@ -234,6 +242,24 @@ class Plan:
     def check_status(self):
         torch.cuda.current_stream().synchronize()
         check(self.lib.cdd_check_status(self.handle))
+
+    # ------------------------------------------------------------------ vacancy coupling
+    def empty_vacancy(self):
+        """A zeroed buffer of vacancy concentrations (one value per cell of every instance)."""
+        return torch.zeros(self.field_elems // 9, dtype=self.dtype, device=self.device)
+
+    def vacancy_view(self, buf, i):
+        o = self.field_offsets[i] // 9
+        return buf[o:o + self.cells[i]].view(tuple(self.instances[i].shape))
+
+    def set_vacancy(self, c):
+        """Register the vacancy-concentration buffer that later steps and fluxes read and update
+        (None clears it)."""
+        if c is not None and (not c.is_cuda or c.dtype != self.dtype or not c.is_contiguous()
+                              or c.numel() != self.field_elems // 9):
+            raise ValueError("c must be a contiguous %s CUDA tensor of %d elements" % (self.dtype, self.field_elems // 9))
+        self._vacancy = c
+        check(self.lib.cdd_set_vacancy(self.handle, ctypes.c_void_p(0 if c is None else c.data_ptr())))
 
     # ------------------------------------------------------------------ field observables
     # name -> (cdd_observable, components); see cdd_observe_field in include/cdd.h

@@ -208,6 +208,9 @@ struct InstDev {
     int has_load;
     double load_rate[3], load_init[3], load_t0, load_lamb, load_mu;
     int glide;              // glide-only dynamics (projected velocity)
+    int vacancy;            // vacancy coupling: sigma_ii -= vac_alpha c, c update + diffusion per step
+    double vac_alpha, vac_beta, vac_gamma;
+    double dt_max;          // > 0: upper bound of the adaptive step
 };
 
 // Per-instance clock and reduction results kept on the device.
@@ -754,6 +757,9 @@ struct PlanCore {
     int max_nd = 3;
     bool any3d = false;
     bool any_glide = false;          // some instance uses the glide-only dynamics
+    bool any_vac = false;            // some instance has vacancy coupling
+    void* d_vac = nullptr;           // caller's vacancy concentrations (cdd_set_vacancy), field_elems / 9
+    void* d_vtr = nullptr;           // trace of beta^P at the step start (vacancy instances), field_elems / 9
     long long field_elems = 0, stress_elems = 0, cells = 0, spec_elems = 0, rows_total = 0;
     InstDev* d_inst = nullptr;       // device copy of the instance table
     InstClock* d_clock = nullptr;
@@ -818,6 +824,11 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
 bool stencil_tma_eligible(const InstDev& I, int precision);
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st);
 cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st);
+// Vacancy coupling around a step: save tr(beta^P) before it; after it, c += vac_beta d tr and the
+// diffusion c^ *= exp(-vac_gamma dt k^2) (FFT passes over one component).
+cudaError_t launch_vacancy_pre(const PlanCore& P, const void* beta, cudaStream_t st);
+cudaError_t launch_vacancy_post(const PlanCore& P, const void* beta, cudaStream_t st);
+cudaError_t launch_vacancy_diffusion(const PlanCore& P, cudaStream_t st);
 // k-space observables of beta (kind: cdd_observable); out in the packed 9- or 3-component layout.
 cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st);
 // Convert 9 components between the plan layout (last axis contiguous) and the reference files'

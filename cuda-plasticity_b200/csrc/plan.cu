@@ -126,6 +126,7 @@ struct cdd_plan {
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     const void* graph_beta = nullptr;
+    const void* graph_vac = nullptr;
     int device = 0;
     StencilMapSet maps_f0, maps_f1, maps_user;   // tensor maps of the stage inputs
     const void* maps_user_ptr = nullptr;
@@ -334,7 +335,9 @@ const StencilMapSet& user_maps(cdd_plan* p, const void* beta) {
 
 int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_fixed) {
     PlanCore& C = p->core;
+    if (C.any_vac && !C.d_vac) return fail(CDD_ERR_ARG, "the plan has vacancy instances: call cdd_set_vacancy first");
     const StencilMapSet& mu = user_maps(p, beta);
+    if (C.any_vac) CDD_CUDA(launch_vacancy_pre(C, beta, st));
     CDD_CUDA(launch_stress(C, beta, C.d_sigma, st));
     CDD_CUDA(launch_stencil(C, M_STAGE1, beta, beta, C.d_f0, nullptr, 0.0, mu, st));
     CDD_CUDA(launch_dt(C, fixed, dt_fixed, st));
@@ -343,6 +346,7 @@ int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_f
     CDD_CUDA(launch_stencil(C, M_STAGE2, C.d_f0, beta, C.d_f1, nullptr, 0.0, p->maps_f0, st));
     CDD_CUDA(launch_stress(C, C.d_f1, C.d_sigma, st));
     CDD_CUDA(launch_stencil(C, M_STAGE3, C.d_f1, beta, beta, nullptr, 0.0, p->maps_f1, st));
+    if (C.any_vac) CDD_CUDA(launch_vacancy_post(C, beta, st));
     return CDD_OK;
 }
 
@@ -431,6 +435,16 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
             free_plan(p);
             return fail(CDD_ERR_ARG, "instance %d: the glide-only dynamics takes no Lambda", i);
         }
+        if (d.vacancy && (d.dynamics != CDD_DYN_GLIDE_CLIMB || !(d.vac_gamma >= 0) || !std::isfinite(d.vac_alpha) ||
+                          !std::isfinite(d.vac_beta))) {
+            free_plan(p);
+            return fail(CDD_ERR_ARG, "instance %d: vacancy coupling needs the glide-and-climb dynamics, finite "
+                        "vac_alpha, vac_beta and vac_gamma >= 0", i);
+        }
+        if (!(d.dt_max >= 0)) {
+            free_plan(p);
+            return fail(CDD_ERR_ARG, "instance %d: dt_max must be >= 0", i);
+        }
         I.nd = d.ndim;
         I.n0 = sh[0]; I.n1 = sh[1]; I.n2 = sh[2];
         if (I.nd == 3) C.any3d = true;
@@ -488,6 +502,12 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
         I.nu = d.nu;
         I.glide = (d.dynamics == CDD_DYN_GLIDE_ONLY) ? 1 : 0;
         if (I.glide) C.any_glide = true;
+        I.vacancy = d.vacancy ? 1 : 0;
+        I.vac_alpha = d.vac_alpha;
+        I.vac_beta = d.vac_beta;
+        I.vac_gamma = d.vac_gamma;
+        I.dt_max = d.dt_max;
+        if (I.vacancy) C.any_vac = true;
         I.lamb = 2. * d.mu * d.nu / (1. - 2. * d.nu);
         I.Lambda = d.Lambda;
         I.cfl = d.cfl;
@@ -559,6 +579,7 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
     ALLOC_OR_FAIL(C.d_sigma, elt * (size_t)C.stress_elems);
     ALLOC_OR_FAIL(C.d_f0, elt * (size_t)C.field_elems);
     ALLOC_OR_FAIL(C.d_f1, elt * (size_t)C.field_elems);
+    if (C.any_vac) ALLOC_OR_FAIL(C.d_vtr, elt * (size_t)(C.field_elems / 9));
     if (precision == CDD_F32) ALLOC_OR_FAIL(C.d_rowsum, sizeof(double) * (size_t)C.rows_total);
     ALLOC_OR_FAIL(C.d_sbar, sizeof(double) * 9 * n_inst);
     ALLOC_OR_FAIL(C.d_bmax, sizeof(double) * (size_t)C.stencil.blocks);
@@ -609,6 +630,7 @@ int cdd_stress(cdd_plan* p, const void* beta, void* sigma6, void* stream) {
 int cdd_flux(cdd_plan* p, const void* beta, double t, void* rhs, void* speed, void* stream) {
     if (int rc = check_plan(p)) return rc;
     if (!beta || !rhs) return fail(CDD_ERR_ARG, "null buffer");
+    if (p->core.any_vac && !p->core.d_vac) return fail(CDD_ERR_ARG, "the plan has vacancy instances: call cdd_set_vacancy first");
     cudaStream_t st = (cudaStream_t)stream;
     CDD_CUDA(launch_stress(p->core, beta, p->core.d_sigma, st));
     CDD_CUDA(launch_stencil(p->core, M_FLUX, beta, beta, rhs, speed, t, user_maps(p, beta), st));
@@ -619,6 +641,7 @@ int cdd_flux_with_stress(cdd_plan* p, const void* beta, const void* sigma6, doub
                          void* stream) {
     if (int rc = check_plan(p)) return rc;
     if (!beta || !sigma6 || !rhs) return fail(CDD_ERR_ARG, "null buffer");
+    if (p->core.any_vac && !p->core.d_vac) return fail(CDD_ERR_ARG, "the plan has vacancy instances: call cdd_set_vacancy first");
     PlanCore K = p->core;
     K.d_sigma = const_cast<void*>(sigma6);
     CDD_CUDA(launch_stencil(K, M_FLUX, beta, beta, rhs, speed, t, user_maps(p, beta), (cudaStream_t)stream));
@@ -806,6 +829,12 @@ int cdd_plas_read(cdd_plan* p, int i, const char* path, int file_precision, long
     return import_from_host(p, i, host, file_precision, beta, (cudaStream_t)stream);
 }
 
+int cdd_set_vacancy(cdd_plan* p, void* c) {
+    if (int rc = check_plan(p)) return rc;
+    p->core.d_vac = c;
+    return CDD_OK;
+}
+
 int cdd_observe_field(cdd_plan* p, int kind, const void* beta, void* out, void* stream) {
     if (int rc = check_plan(p)) return rc;
     if (!beta || !out) return fail(CDD_ERR_ARG, "null buffer");
@@ -865,7 +894,7 @@ int cdd_run(cdd_plan* p, void* beta, int n_steps, int use_graph, void* stream) {
             if (int rc = record_step(p, beta, st, 0, 0.0)) return rc;
         return CDD_OK;
     }
-    if (!p->graph || p->graph_beta != beta) {
+    if (!p->graph || p->graph_beta != beta || p->graph_vac != p->core.d_vac) {
         if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
         if (!p->cap_stream) CDD_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
         cudaGraph_t g;
@@ -878,6 +907,7 @@ int cdd_run(cdd_plan* p, void* beta, int n_steps, int use_graph, void* stream) {
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(CDD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
         p->graph_beta = beta;
+        p->graph_vac = p->core.d_vac;
     }
     for (int k = 0; k < n_steps; ++k) CDD_CUDA(cudaGraphLaunch(p->graph, st));
     return CDD_OK;
@@ -904,6 +934,7 @@ namespace {
 int check_adjoint_supported(const cdd_plan* p) {
     for (int i = 0; i < p->core.n_inst; ++i)
         if (p->inst[i].glide) return fail(CDD_ERR_UNSUPPORTED, "instance %d: no adjoint of the glide-only dynamics", i);
+        else if (p->inst[i].vacancy) return fail(CDD_ERR_UNSUPPORTED, "instance %d: no adjoint of the vacancy coupling", i);
     return CDD_OK;
 }
 
@@ -993,6 +1024,8 @@ int cdd_step_record(cdd_plan* p, void* beta, double t, double dt, void* rec, voi
     if (!beta) return fail(CDD_ERR_ARG, "null buffer");
     if (!(dt >= 0)) return fail(CDD_ERR_ARG, "dt must be >= 0");
     if (rec && ((uintptr_t)rec & 255)) return fail(CDD_ERR_ARG, "record must be 256-byte aligned");
+    if (rec)
+        if (int rc = check_adjoint_supported(p)) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     PlanCore& C = p->core;
     const size_t elt = C.precision == CDD_F64 ? sizeof(double) : sizeof(float);

@@ -213,6 +213,7 @@ template <typename T> struct CellCtx {
     const T* bn;    // beta_n of the stage updates
     T* out;         // rhs (flux, stage 1) or the updated state (stages 2, 3)
     T* spd;         // CFL speed (flux mode, optional)
+    const T* vac;   // vacancy concentration (vacancy instances) or null
     long long cells;
     T ih;           // 1 / Dx
     bool has_load, lam_on, glide;
@@ -255,6 +256,12 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         S[0][1] = S[1][0] = s6[1];
         S[0][2] = S[2][0] = s6[2];
         S[1][2] = S[2][1] = s6[4];
+        if (cx.vac) {   // BetaP_VacancyDynamics.GetSigma (VacancyDynamics.py L23-29): sigma_ii -= alpha c
+            const T ac = (T)I.vac_alpha * *cx.vac;   // (read on use: FP64 has no registers to spare)
+            S[0][0] -= ac;
+            S[1][1] -= ac;
+            S[2][2] -= ac;
+        }
     }
     const bool lam_on = cx.lam_on;
     const bool glide = GLIDE && cx.glide;   // glide-only dynamics (Lambda is 0 then)
@@ -594,7 +601,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
                                       const T* __restrict__ sig, T* __restrict__ speed_out,
                                       const InstClock* __restrict__ clk, double t_flux,
                                       double* __restrict__ bmax, double* __restrict__ bsum,
-                                      int* __restrict__ status) {
+                                      int* __restrict__ status, const T* __restrict__ vac) {
     constexpr int RX = TileGeom<T>::RX, OX = TileGeom<T>::OX, PP = tile_pp<T>();
     constexpr int NS = (ND == 3) ? TileGeom<T>::NS : 1;
     constexpr uint32_t PLANE_BYTES = 9u * PP * sizeof(T);
@@ -687,6 +694,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         cx.bn = bn ? bn + I.foff + cl0 : nullptr;   // stage updates only
         cx.out = out + I.foff + cl0;
         cx.spd = speed_out ? speed_out + I.coff + cl0 : nullptr;
+        cx.vac = (I.vacancy && vac) ? vac + I.foff / 9 + cl0 : nullptr;
         cx.cells = cells;
         cx.ih = (T)I.inv_h;
         cx.has_load = I.has_load != 0;
@@ -718,6 +726,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             tv.so[2] = 0;
         }
         stencil_cell<T, ND, MODE, GLIDE>(I, cx, vxy, tv, kc, clk[ii], t_flux, vmax, esum, zsum);
+        if (cx.vac) cx.vac += plane;
         cx.sig += plane;
         if (cx.bn) cx.bn += plane;
         cx.out += plane;
@@ -764,7 +773,7 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
           const T* __restrict__ bs, const T* bn, T* out, const T* __restrict__ sig,
           T* __restrict__ speed_out, const InstClock* __restrict__ clk, double t_flux,
           double* __restrict__ bmax, double* __restrict__ bsum, int* __restrict__ status,
-          const __grid_constant__ StencilMapSet maps) {
+          const T* __restrict__ vac, const __grid_constant__ StencilMapSet maps) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     __shared__ double red[ST_THREADS / 32];
@@ -774,10 +783,10 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
     const int lb = blockIdx.x - pre[ii];
     if (I.nd == 3)
         march<T, 3, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
-                          status);
+                          status, vac);
     else
         march<T, 2, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
-                          status);
+                          status, vac);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -815,6 +824,7 @@ __global__ void __launch_bounds__(256) k_dt(const InstDev* __restrict__ insts,
         double dt;
         if (fixed) dt = dt_fixed;
         else dt = act ? I.cfl / (I.nmax * m) : 0.0;
+        if (!fixed && I.dt_max > 0.0 && dt > I.dt_max) dt = I.dt_max;   // dtBound (FieldMover.py L359-360)
         if (act && c.t + dt > c.t_end) dt = c.t_end - c.t;
         if (!act) dt = 0.0;
         c.dt = dt;
@@ -840,6 +850,39 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
         long long i = i0 + (long long)k * blockDim.x;
         if (i < n) f0[I.foff + i] = u[I.foff + i] + dt * f0[I.foff + i];
     }
+}
+
+// Vacancy coupling, one thread per cell of the vacancy instances (OperatorSplittingTVDRK_FieldMover,
+// FieldMover.py L339-380): tr(beta^P) at the step start (prevTrBetaP), and after the step
+// c += vac_beta (TrBetaP - prevTrBetaP) for the instances whose step was applied; traces summed
+// xx + yy, then zz, as the reference does.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vac_trace(const InstDev* __restrict__ insts, int n_inst,
+                                                   const int* __restrict__ pre, const T* __restrict__ beta,
+                                                   T* __restrict__ tr) {
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    if (!I.vacancy) return;
+    const long long cell = (long long)(blockIdx.x - pre[ii]) * blockDim.x + threadIdx.x;
+    if (cell >= I.cells) return;
+    const T* b = beta + I.foff + cell;
+    tr[I.foff / 9 + cell] = (b[0] + b[4 * I.cells]) + b[8 * I.cells];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_vac_update(const InstDev* __restrict__ insts, int n_inst,
+                                                    const int* __restrict__ pre, const T* __restrict__ beta,
+                                                    const T* __restrict__ tr, T* __restrict__ c,
+                                                    const InstClock* __restrict__ clk) {
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    if (!I.vacancy || !clk[ii].active) return;
+    const long long cell = (long long)(blockIdx.x - pre[ii]) * blockDim.x + threadIdx.x;
+    if (cell >= I.cells) return;
+    const T* b = beta + I.foff + cell;
+    const T trn = (b[0] + b[4 * I.cells]) + b[8 * I.cells];
+    T& cv = c[I.foff / 9 + cell];
+    cv = cv + (T)I.vac_beta * (trn - tr[I.foff / 9 + cell]);
 }
 
 // Energy and mean b_zz partials of a state whose internal stress is in sig (observables).
@@ -901,10 +944,12 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
 #define CDD_LAUNCH_ST(M, SP)                                                                              \
     if (P.any_glide)                                                                                  \
         k_stencil<T, M, true><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                                   P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps); \
+                                                                   P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, \
+                                                                   (const T*)P.d_vac, maps);            \
     else                                                                                              \
         k_stencil<T, M, false><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                                    P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, maps)
+                                                                    P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, \
+                                                                    (const T*)P.d_vac, maps)
     switch (mode) {
         case M_FLUX: CDD_LAUNCH_ST(M_FLUX, (T*)speed); break;
         case M_STAGE1: CDD_LAUNCH_ST(M_STAGE1, nullptr); break;
@@ -912,6 +957,31 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
         default: CDD_LAUNCH_ST(M_STAGE3, nullptr); break;
     }
 #undef CDD_LAUNCH_ST
+}
+
+template <typename T>
+static cudaError_t vac_pre_t(const PlanCore& P, const void* beta, cudaStream_t st) {
+    const LaunchShape& L = P.obs;
+    k_vac_trace<T><<<L.blocks, L.threads, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const T*)beta, (T*)P.d_vtr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vacancy_pre(const PlanCore& P, const void* beta, cudaStream_t st) {
+    return P.precision == CDD_F32 ? vac_pre_t<float>(P, beta, st) : vac_pre_t<double>(P, beta, st);
+}
+
+template <typename T>
+static cudaError_t vac_post_t(const PlanCore& P, const void* beta, cudaStream_t st) {
+    const LaunchShape& L = P.obs;
+    k_vac_update<T><<<L.blocks, L.threads, 0, st>>>(P.d_inst, P.n_inst, L.d_pre, (const T*)beta,
+                                                    (const T*)P.d_vtr, (T*)P.d_vac, P.d_clock);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_vacancy_diffusion(P, st);
+}
+
+cudaError_t launch_vacancy_post(const PlanCore& P, const void* beta, cudaStream_t st) {
+    return P.precision == CDD_F32 ? vac_post_t<float>(P, beta, st) : vac_post_t<double>(P, beta, st);
 }
 
 cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,

@@ -67,7 +67,8 @@ __device__ __forceinline__ double mean_stress(const InstDev& I, const double* m,
 //   RS_SYM:    rows of beta_ij and beta_ji (p == q on the diagonal), 6 components;
 //   RS_FULL:   row ra of a 9-component field (p == q), all 9 components.
 // The value is (p + q) / 2, exact when p == q.
-enum RowSource { RS_STRESS = 1, RS_SYM = 2, RS_FULL = 3 };
+//   RS_VAC:    row ra of the vacancy concentrations (one component; vacancy instances only).
+enum RowSource { RS_STRESS = 1, RS_SYM = 2, RS_FULL = 3, RS_VAC = 4 };
 
 template <typename T>
 __device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mode, long long ra, const T*& p,
@@ -78,6 +79,10 @@ __device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mo
     }
     if (mode == RS_FULL) {
         p = q = base + I.foff + ra * I.nl;
+        return;
+    }
+    if (mode == RS_VAC) {
+        p = q = base + I.foff / 9 + ra * I.nl;
         return;
     }
     const int o = fdiv_q(I.fd_rows, (int)ra);
@@ -107,6 +112,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const int N = I.nl, P = I.tile[PASS_R2C].lines, ld = rows_ld(N);
     const long long nrows = (long long)ncomp * I.rows;
     if (2LL * lb * P >= nrows) return;   // launch sized for more components than this pass carries
+    if (mode == RS_VAC && !I.vacancy) return;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const T half = (T)0.5;
@@ -129,7 +135,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     __syncthreads();
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(beta + I.foff)) & 15) == 0) &&
-                     ((((uintptr_t)(beta + I.soff)) & 15) == 0) && ((I.cells & 3) == 0);
+                     ((((uintptr_t)(beta + I.soff)) & 15) == 0) && ((((uintptr_t)(beta + I.foff / 9)) & 15) == 0) &&
+                     ((I.cells & 3) == 0);
     if (vec) {
 #pragma unroll 2
         for (int i4 = tid; i4 < (P * N) >> 2; i4 += nt) {
@@ -214,7 +221,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
 // ------------------------------------------------------------------------------------------
 //   RD_FIELD9 / RD_FIELD3: row ra of a packed 9- / 3-component array (instance offsets foff and
 //                 foff / 3), with an optional epilogue (RowEpilogue).
-enum RowDest { RD_STRESS = 0, RD_SYM_FIELD = 1, RD_FIELD9 = 2, RD_FIELD3 = 3 };
+//   RD_VAC:       row ra of the vacancy concentrations (vacancy instances whose step was applied).
+enum RowDest { RD_STRESS = 0, RD_SYM_FIELD = 1, RD_FIELD9 = 2, RD_FIELD3 = 3, RD_VAC = 4 };
 
 // Real-space terms the observables subtract from the inverse transform of output component c:
 // out_c -= coef (beta[EPI_P[c]] - beta[EPI_Q[c]]) (EPI_Q < 0: no second term). beta^E: -beta^P;
@@ -237,8 +245,8 @@ __device__ __forceinline__ void dst_rows(const InstDev& I, T* base, int mode, lo
         p = q = base + I.soff + ra * I.nl;
         return;
     }
-    if (mode == RD_FIELD9 || mode == RD_FIELD3) {
-        p = q = base + (mode == RD_FIELD9 ? I.foff : I.foff / 3) + ra * I.nl;
+    if (mode == RD_FIELD9 || mode == RD_FIELD3 || mode == RD_VAC) {
+        p = q = base + (mode == RD_FIELD9 ? I.foff : (mode == RD_FIELD3 ? I.foff / 3 : I.foff / 9)) + ra * I.nl;
         return;
     }
     const int o = fdiv_q(I.fd_rows, (int)ra);
@@ -278,7 +286,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
                                                   T* __restrict__ out,
                                                   const typename VecOf<T>::type* __restrict__ tw,
                                                   const double* __restrict__ sbar, int mode, int ncomp,
-                                                  const T* __restrict__ beta, int epi) {
+                                                  const T* __restrict__ beta, int epi,
+                                                  const InstClock* __restrict__ clk) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -288,6 +297,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const int N = I.nl, P = I.tile[PASS_C2R].lines, ld = rows_ld(N), nh = I.nh;
     const long long nrows = (long long)ncomp * I.rows;
     if (2LL * lb * P >= nrows) return;   // launch sized for more components than this pass carries
+    if (mode == RD_VAC && (!I.vacancy || !clk[ii].active)) return;
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
@@ -350,6 +360,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     s = fft_lines<V, true>(s, s + P * ld, lay, I.lp_last, tws, tid, nt, I.lp_last.twst[0]);
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(out + I.soff)) & 15) == 0) &&
                      ((((uintptr_t)(out + I.foff)) & 15) == 0) && ((((uintptr_t)(out + I.foff / 3)) & 15) == 0) &&
+                     ((((uintptr_t)(out + I.foff / 9)) & 15) == 0) &&
                      (epi == EPI_NONE || ((((uintptr_t)(beta + I.foff)) & 15) == 0)) && ((I.cells & 3) == 0);
     if (vec) {
 #pragma unroll 2
@@ -412,7 +423,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
                                                  const int* __restrict__ pre,
                                                  typename VecOf<T>::type* __restrict__ spec,
                                                  const typename VecOf<T>::type* __restrict__ tw,
-                                                 int pass, int ncomp) {
+                                                 int pass, int ncomp, int vac_only) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -425,6 +436,7 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
     const int i0 = lb % I.n0;
     const int c = lb / I.n0;
     if (c >= ncomp) return;   // launch sized for more components than this pass carries
+    if (vac_only && !I.vacancy) return;
     const int N = I.n1, nhp = I.nhp, nh = I.nh;
     const int col0 = ta * W;
     const int wv = min(W, nh - col0);
@@ -643,10 +655,12 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
 // ---- k-space observables (PlasticityState.py) ----
 // Component counts of the k-space pass per mode (see k_green) and its shared-memory slots (inputs
 // or outputs, whichever are more, plus three scratch slots).
-__host__ __device__ constexpr int green_nin(int gmode) { return gmode == 6 ? 9 : 6; }
+__host__ __device__ constexpr int green_nin(int gmode) { return gmode == 6 ? 9 : (gmode == 7 ? 1 : 6); }
 __host__ __device__ constexpr int green_nout(int gmode) {
-    return (gmode == 3 || gmode == 6) ? 9 : ((gmode == 4 || gmode == 5) ? 3 : 6);
+    return (gmode == 3 || gmode == 6) ? 9 : ((gmode == 4 || gmode == 5) ? 3 : (gmode == 7 ? 1 : 6));
 }
+// transforms run on groups of three components, or one by one for the single-component mode
+__host__ __device__ constexpr int green_group(int gmode) { return gmode == 7 ? 1 : 3; }
 __host__ __device__ constexpr int green_slots(int gmode) {
     return (green_nin(gmode) > green_nout(gmode) ? green_nin(gmode) : green_nout(gmode)) + 3;
 }
@@ -735,15 +749,15 @@ __device__ __forceinline__ void obs_point(const V* b, V* o, T kx, T ky, T kz, bo
 // Shared memory: component slots of N x W (+W pad), the last three being the ping-pong scratch
 // (slot `scr` on). The transforms run three components at a time against the scratch; when the
 // stage count is odd the result is copied back to the component slots.
-template <typename V, bool INV>
-__device__ __forceinline__ void fft_group3(V* s, int g, int lgw, int cs, const LinePlan& lp,
-                                           const V* __restrict__ tws, int tid, int nt, int scr) {
-    V* a = s + 3 * g * cs;
+template <typename V, bool INV, int K>
+__device__ __forceinline__ void fft_group(V* s, int g, int lgw, int cs, const LinePlan& lp,
+                                          const V* __restrict__ tws, int tid, int nt, int scr) {
+    V* a = s + K * g * cs;
     V* b = s + scr * cs;   // scratch slots
-    ColLayout<3> lay{lgw, cs};
+    ColLayout<K> lay{lgw, cs};
     V* r = fft_lines<V, INV>(a, b, lay, lp, tws, tid, nt, lp.twst[0]);
     if (r != a) {
-        for (int i = tid; i < 3 * cs; i += nt) a[i] = b[i];
+        for (int i = tid; i < K * cs; i += nt) a[i] = b[i];
         __syncthreads();
     }
 }
@@ -761,7 +775,8 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
                                                          const typename VecOf<T>::type* __restrict__ tw,
                                                          const T* __restrict__ ktab,
                                                          typename VecOf<T>::type* __restrict__ phi,
-                                                         double* __restrict__ part) {
+                                                         double* __restrict__ part,
+                                                         const InstClock* __restrict__ clk) {
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* s = reinterpret_cast<V*>(smem_raw);
@@ -788,6 +803,8 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     constexpr int NIN = green_nin(GMODE);
     constexpr int NOUT = green_nout(GMODE);
     constexpr int SCR = green_slots(GMODE) - 3;   // first scratch slot
+    constexpr int KG = green_group(GMODE);
+    if (GMODE == 7 && !I.vacancy) return;
     V* tws = s + ((green_slots(GMODE) * cs + 1) & ~1);   // twiddle rows after the slots
     // forward: all six component tiles staged at once (16-byte asynchronous copies keep the whole
     // tile in flight), then the axis-0 transforms in shared memory
@@ -809,7 +826,11 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     stage_tw_to_smem(I.lp_first, tw, tws, tid, nt);
     cp_async_wait_all();
     __syncthreads();
-    for (int g = 0; g < NIN / 3; ++g) fft_group3<V, false>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
+    for (int g = 0; g < NIN / KG; ++g) fft_group<V, false, KG>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
+    // vacancy diffusion factor exp(-gamma dt kSq) (VacancyDynamics.DiffusionEvolution L41-61), dt of
+    // the step just taken
+    const T vg = (GMODE == 7) ? (T)(-I.vac_gamma) : (T)0;
+    const T vdt = (GMODE == 7) ? (T)clk[ii].dt : (T)0;
     // Green contraction, one k point per thread iteration
     const T lam = (T)I.lamb, mu = (T)I.mu;
     const T A = (T)(I.lamb / (I.lamb + 2.0 * I.mu));
@@ -837,7 +858,12 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
         V b[NIN], o[NOUT];
 #pragma unroll
         for (int c = 0; c < NIN; ++c) b[c] = s[c * cs + i];
-        if constexpr (GMODE >= 3) {
+        if constexpr (GMODE == 7) {
+            const T ksq = kx * kx + ky * ky + kz * kz;
+            const T f = exp(ksq * vg * vdt) * scale;
+            o[0].x = b[0].x * f;
+            o[0].y = b[0].y * f;
+        } else if constexpr (GMODE >= 3) {
             obs_point<T, V, GMODE>(b, o, kx, ky, kz, kzero, A, B, scale);
         } else if constexpr (GMODE == 0) {
             // the symmetric 3 x 3 matrix of the six components (row-major, b9[3i + j])
@@ -894,16 +920,16 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
     __syncthreads();
     if (line_plan_io(I.lp_first)) {
         // inverse transforms from the component slots straight to global memory
-        const SColT<V, 3> scratch{s + SCR * cs, lgw, cs};
+        const SColT<V, KG> scratch{s + SCR * cs, lgw, cs};
 #pragma unroll 1
-        for (int g = 0; g < NOUT / 3; ++g) {
-            const SColT<V, 3> slots{s + 3 * g * cs, lgw, cs};
-            const GColT<V, 3> gout{base + 3 * g * cstride, estride, cstride, lgw, wv};
-            fft_io<V, true, 3>(slots, scratch, slots, gout, lgw, I.lp_first, tws, tid, nt, I.lp_first.twst[0]);
+        for (int g = 0; g < NOUT / KG; ++g) {
+            const SColT<V, KG> slots{s + KG * g * cs, lgw, cs};
+            const GColT<V, KG> gout{base + KG * g * cstride, estride, cstride, lgw, wv};
+            fft_io<V, true, KG>(slots, scratch, slots, gout, lgw, I.lp_first, tws, tid, nt, I.lp_first.twst[0]);
         }
         return;
     }
-    for (int g = 0; g < NOUT / 3; ++g) fft_group3<V, true>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
+    for (int g = 0; g < NOUT / KG; ++g) fft_group<V, true, KG>(s, g, lgw, cs, I.lp_first, tws, tid, nt, SCR);
     if (W * (int)sizeof(V) >= 16) {
 #pragma unroll 1
         for (int c = 0; c < NOUT; ++c) tile_store(base + c * cstride, s + c * cs, estride, N, lgw, wv, tid, nt);
@@ -975,22 +1001,22 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     }
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6);
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6, 0);
     if (f32)
         k_green<T, true, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr, nullptr);
     else
         k_green<T, false, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr);
+            P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr, nullptr);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6);
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6, 0);
     if (f32)
         k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS, 6, nullptr, EPI_NONE);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS, 6, nullptr, EPI_NONE, nullptr);
     else
         k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS, 6, nullptr, EPI_NONE);
+            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS, 6, nullptr, EPI_NONE, nullptr);
     return cudaGetLastError();
 }
 
@@ -1008,14 +1034,14 @@ static cudaError_t run_stress_variant(const PlanCore& P, const void* in, void* o
         P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)in, spec, tw, nullptr, GMODE == 1 ? RS_STRESS : RS_SYM, 6);
     if (L[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6);
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6, 0);
     k_green<T, false, GMODE><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, part);
+        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, part, nullptr);
     if (L[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6);
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6, 0);
     k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, GMODE == 1 ? RD_SYM_FIELD : RD_STRESS, 6, nullptr, EPI_NONE);
+        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, GMODE == 1 ? RD_SYM_FIELD : RD_STRESS, 6, nullptr, EPI_NONE, nullptr);
     return cudaGetLastError();
 }
 
@@ -1028,6 +1054,36 @@ cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* 
 cudaError_t launch_stress_dnu(const PlanCore& P, const void* beta, void* out6, cudaStream_t st) {
     if (P.precision == CDD_F32) return run_stress_variant<float, 2>(P, beta, out6, nullptr, nullptr, st);
     return run_stress_variant<double, 2>(P, beta, out6, nullptr, nullptr, st);
+}
+
+// Vacancy diffusion: the concentrations of the vacancy instances (one component) forward, times
+// exp(-gamma dt kSq) in the axis-0 pass, inverse, written back for the instances whose step was
+// applied. The stress passes' launch shapes carry it (blocks past one component exit).
+template <typename T>
+static cudaError_t run_vacancy_diffusion(const PlanCore& P, cudaStream_t st) {
+    typedef typename VecOf<T>::type V;
+    V* spec = (V*)P.d_spec;
+    const V* tw = (const V*)P.d_tw;
+    const LaunchShape* L = P.pass;
+    k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)P.d_vac, spec, tw, nullptr, RS_VAC, 1);
+    if (L[PASS_MID_F].blocks > 0)
+        k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 1, 1);
+    k_green<T, false, 7><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, nullptr, nullptr, P.d_clock);
+    if (L[PASS_MID_I].blocks > 0)
+        k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
+            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 1, 1);
+    k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
+        P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)P.d_vac, tw, nullptr, RD_VAC, 1, nullptr, EPI_NONE,
+        P.d_clock);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vacancy_diffusion(const PlanCore& P, cudaStream_t st) {
+    if (P.precision == CDD_F32) return run_vacancy_diffusion<float>(P, st);
+    return run_vacancy_diffusion<double>(P, st);
 }
 
 // k-space observables: forward transforms of sym(beta) (6 components, the stress passes' launch
@@ -1048,15 +1104,15 @@ static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out
         P.d_inst, P.n_inst, LI[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, NIN == 9 ? RS_FULL : RS_SYM, NIN);
     if (LI[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<LI[PASS_MID_F].blocks, LI[PASS_MID_F].threads, LI[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, LI[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, NIN);
+            P.d_inst, P.n_inst, LI[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, NIN, 0);
     k_green<T, false, GMODE><<<LG.blocks, LG.threads, LG.smem, st>>>(P.d_inst, P.n_inst, LG.d_pre, spec, tw,
-                                                                      (const T*)P.d_k, nullptr, nullptr);
+                                                                      (const T*)P.d_k, nullptr, nullptr, nullptr);
     if (LO[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<LO[PASS_MID_I].blocks, LO[PASS_MID_I].threads, LO[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, LO[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, NOUT);
+            P.d_inst, P.n_inst, LO[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, NOUT, 0);
     k_c2r_rows<T, false><<<LO[PASS_C2R].blocks, LO[PASS_C2R].threads, LO[PASS_C2R].smem, st>>>(
         P.d_inst, P.n_inst, LO[PASS_C2R].d_pre, spec, (T*)out, tw, nullptr, NOUT == 9 ? RD_FIELD9 : RD_FIELD3, NOUT,
-        (const T*)beta, EPI);
+        (const T*)beta, EPI, nullptr);
     return cudaGetLastError();
 }
 
@@ -1098,6 +1154,7 @@ static cudaError_t set_attr_t(size_t smem) {
     if ((e = set_dyn_smem_limit(k_green<T, false, 4>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 5>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 6>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 7>, smem))) return e;
     return cudaSuccess;
 }
 

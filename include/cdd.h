@@ -66,6 +66,16 @@ typedef struct cdd_instance {
     double load_rate[3], load_initial[3], load_t0;
     double load_mu, load_nu;   /* stiffness the load is converted with */
     int dynamics;          /* CDD_DYN_GLIDE_CLIMB (0) or CDD_DYN_GLIDE_ONLY (1) */
+    /* Vacancy coupling (BetaP_VacancyDynamics, Plasticity/FieldDynamics/VacancyDynamics.py L16-45,
+     * stepped by OperatorSplittingTVDRK_FieldMover, Plasticity/FieldMovers/FieldMover.py L318-380):
+     * nonzero `vacancy` adds a vacancy concentration c (see cdd_set_vacancy) with
+     * sigma_ii -= vac_alpha c in the flux, and after each TVD-RK3 step
+     * c += vac_beta (tr beta^P_new - tr beta^P_old) followed by exact diffusion
+     * c^ *= exp(-vac_gamma dt k^2) (DiffusionEvolution L41-61). */
+    int vacancy;
+    double vac_alpha, vac_beta, vac_gamma;
+    double dt_max;         /* > 0: upper bound of the adaptive step before the end-time clamp (the
+                              operator-splitting mover's dtBound, default 0.01 there); 0: none */
 } cdd_instance;
 
 /* Dynamics of an instance: BetaPDynamics of CentralUpwindHJBetaPDynamics3D.py (glide and climb,
@@ -258,6 +268,14 @@ int cdd_stress_noalloc(const cdd_instance* inst, int precision, const void* beta
                        void* stream);
 
 /* Message for the calling thread's last failing call ("" if none). */
+/* Register the device buffer of vacancy concentrations used by every later step and flux call of
+ * the plan (NULL clears it): field_elems / 9 elements of the plan's precision, instance i at
+ * cdd_plan_field_offset(i) / 9 (one value per cell); entries of instances without vacancy coupling
+ * are ignored. Steps update it in place. Required (CDD_ERR_ARG otherwise) before stepping or
+ * evaluating the flux of a plan that has a vacancy instance. A CUDA graph of cdd_run is re-captured
+ * when the buffer changes. The adjoint entry points do not support vacancy instances. */
+int cdd_set_vacancy(cdd_plan* plan, void* c);
+
 /* ---- Field observables in k space (PlasticityState.py) ----
  * out: a packed field buffer of the plan's precision. 9-component observables are written in the
  * field layout (instance i at cdd_plan_field_offset(i)); 3-component ones in a packed 3-component

@@ -372,9 +372,12 @@ class Params:
     """Material, loading and integrator parameters of one instance."""
 
     def __init__(self, mu=1.0, nu=0.3, Lambda=0, cfl=0.25, load_rate=None,
-                 load_initial=(0., 0., 0.), load_t0=0., load_mu=None, load_nu=None, glide=False):
+                 load_initial=(0., 0., 0.), load_t0=0., load_mu=None, load_nu=None, glide=False,
+                 vacancy=None, dt_bound=None):
         self.mu, self.nu, self.Lambda, self.cfl = mu, nu, Lambda, cfl
         self.glide = glide
+        self.vacancy = vacancy            # (alpha, beta, gamma) of the vacancy coupling, or None
+        self.dt_bound = dt_bound          # the splitting mover's dtBound (None: no bound)
         self.load_rate = None if load_rate is None else np.asarray(load_rate, float)
         self.load_initial = np.asarray(load_initial, float)
         self.load_t0 = load_t0
@@ -434,6 +437,49 @@ def run(beta, t0, t_end, p, max_steps=None, observer=None):
             observer(t, beta)
         if t >= t_end or (max_steps is not None and n >= max_steps):
             return beta, t
+
+
+# ----------------------------------------------------------------------------------------------
+# Vacancy coupling: BetaP_VacancyDynamics (VacancyDynamics.py L16-61) stepped by
+# OperatorSplittingTVDRK_FieldMover.CalculateOneAdaptiveTimeStep (FieldMover.py L344-380).
+# ----------------------------------------------------------------------------------------------
+def vacancy_flux(beta, c, p):
+    """CalculateFlux with GetSigma: the internal stress minus alpha c on the diagonal (no load)."""
+    sigma = stress(beta, p.mu, p.nu)
+    for i in range(3):
+        sigma[ci(i, i)] -= p.vacancy[0] * c
+    return flux(beta, sigma, p.Lambda)
+
+
+def diffuse(c, gamma, dt):
+    """DiffusionEvolution: c^ * exp(kSq * -gamma * dt) (kSq of the k tables, no ME)."""
+    shape = c.shape
+    kc = np.fft.rfftn(c)
+    kt = k_tables(shape)[1] * -gamma * dt
+    return np.fft.irfftn(kc * np.exp(kt), s=shape)
+
+
+def vacancy_step(beta, c, t, t_end, p):
+    """One operator-splitting step; returns (beta_new, c_new, dt)."""
+    alpha_rk = [[1.], [3. / 4., 1. / 4.], [1. / 3., 0., 2. / 3.]]
+    beta_rk = [[1.], [0., 1. / 4.], [0., 0., 2. / 3.]]
+    prev_tr = beta[0] + beta[4] + beta[8]
+    rhs, speed = vacancy_flux(beta, c, p)
+    dt = float(p.cfl / (max(beta.shape[1:]) * speed.max()))
+    if p.dt_bound is not None and dt > p.dt_bound:
+        dt = p.dt_bound
+    if t + dt > t_end:
+        dt = t_end - t
+    L0 = dt * rhs
+    F0 = alpha_rk[0][0] * beta + beta_rk[0][0] * L0
+    L1 = dt * vacancy_flux(F0, c, p)[0]
+    F1 = alpha_rk[1][0] * beta + beta_rk[1][0] * L0 + alpha_rk[1][1] * F0 + beta_rk[1][1] * L1
+    L2 = dt * vacancy_flux(F1, c, p)[0]
+    F2 = (alpha_rk[2][0] * beta + beta_rk[2][0] * L0 + alpha_rk[2][1] * F0 + beta_rk[2][1] * L1
+          + alpha_rk[2][2] * F1 + beta_rk[2][2] * L2)
+    tr = F2[0] + F2[4] + F2[8]
+    c = c + p.vacancy[1] * (tr - prev_tr)
+    return F2, diffuse(c, p.vacancy[2], dt), dt
 
 
 # ----------------------------------------------------------------------------------------------

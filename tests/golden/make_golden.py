@@ -2,14 +2,17 @@
 
 The reference (mattbierbaum/cuda-plasticity, ``Plasticity/``) is Python 2 code. This script copies
 the modules of the time-step path into ``oracle/_refpy/Plasticity`` (git-ignored and not shipped to
-GPU machines) and applies six mechanical Python-3 patches, none of which touches arithmetic:
+GPU machines) and applies mechanical Python-3 / numpy-2 patches, none of which touches arithmetic:
 
   (i)   ``raise E, "msg"`` -> ``raise E("msg")`` and ``print "..."`` -> ``print(...)``;
   (ii)  ``/2+1`` -> ``//2+1`` (integer half-spectrum sizes, GridArray/FourierSpaceTools.py L17-45);
   (iii) ``__div__``/``__rdiv__`` -> ``__truediv__``/``__rtruediv__`` (Fields.py, PlasticityState.py);
   (iv)  ``from scipy import fromfunction, sin, pi`` -> ``from numpy import ...`` (PlasticityState.py L4);
   (v)   ``copy=False`` -> ``copy=None`` (numpy-2 semantics, GridArray.py L8-9);
-  (vi)  tabs expanded.
+  (vi)  tabs expanded;
+  (ix)  the operator-splitting mover's CFL step ``dt = self.CFLsafeFactor / sum`` (a 0-d array)
+        becomes a Python float, as the main mover's ``dt = dt.tolist()`` does (FieldMover.py L96-99):
+        under numpy 2 a 0-d array times the reference's Field objects builds an object array.
 
 It then drives the reference through its public API -- ``PlasticityState``, the
 ``BetaPDynamics.CalculateFlux`` of CentralUpwindHJBetaPDynamics3D.py (3-D) or of
@@ -49,6 +52,7 @@ MODULES = [
     "FieldDynamics/CentralUpwindHJBetaPDynamics3D.py",
     "FieldDynamics/CentralUpwindHJBetaPGlideOnlyDynamics.py",
     "FieldMovers/__init__.py", "FieldMovers/FieldMover.py",
+    "PlasticityStates/VacancyState.py", "FieldDynamics/VacancyDynamics.py",
 ]
 
 
@@ -61,6 +65,8 @@ def _patch(text):
     text = text.replace("from scipy import fromfunction, sin, pi",
                         "from numpy import fromfunction, sin, pi")         # (iv)
     text = text.replace("copy=False", "copy=None")                          # (v)
+    text = text.replace("dt = self.CFLsafeFactor / sum\n        if (dt > self.dtBound)",
+                        "dt = float(self.CFLsafeFactor / sum)\n        if (dt > self.dtBound)")  # (ix)
     return text
 
 
@@ -271,6 +277,42 @@ def run_observables_case(name="observables"):
     print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
 
 
+def run_vacancy_case(name="vacancy"):
+    """The vacancy-coupled dynamics (BetaP_VacancyDynamics, VacancyDynamics.py) stepped by
+    OperatorSplittingTVDRK_FieldMover.CalculateOneAdaptiveTimeStep (FieldMover.py L344-380): 3-D
+    8^3 with the default dtBound 0.01, and 2-D 16^2 with dtBound 1 (the CFL step); 3 steps each.
+    DecoupleState builds the beta^P state with PlasticityState's defaults mu 0.5, nu 0.3."""
+    sys.path.insert(0, PATCHED)
+    from Plasticity.PlasticityStates import VacancyState
+    from Plasticity.FieldDynamics import VacancyDynamics
+    from Plasticity.FieldMovers import FieldMover
+    from Plasticity.GridArray import GridArray
+    sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
+    from cdd.initial import gaussian_random_field
+    out = {"alpha": 0.5, "beta": 0.7, "gamma": 0.02, "mu": 0.5, "nu": 0.3, "cfl": 0.25}
+    for key, shape, seed, bound in (("3d", (8, 8, 8), 51, 0.01), ("2d", (16, 16), 52, 1.0)):
+        beta0 = gaussian_random_field(shape, 0.06, 0.05, seed)
+        c0 = 0.01 * np.random.default_rng(seed).standard_normal(shape)
+        st = VacancyState.VacancyState(shape, mu=0.5, nu=0.3)
+        for c, comp in enumerate(COMPONENTS):
+            st.betaP_V[comp] = GridArray.GridArray(beta0[c].copy())
+        st.betaP_V["s", "s"] = GridArray.GridArray(c0.copy())
+        dyn = VacancyDynamics.BetaP_VacancyDynamics(alpha=out["alpha"], beta=out["beta"], gamma=out["gamma"])
+        mover = FieldMover.OperatorSplittingTVDRK_FieldMover(CFLsafeFactor=out["cfl"], dtBound=bound)
+        t, betas, cs, dts = 0.0, [], [], []
+        for _ in range(3):
+            st, dt = mover.CalculateOneAdaptiveTimeStep(t, st, dyn, 1e30)
+            t += dt
+            betas.append(np.stack([np.asarray(st.betaP_V[comp]) for comp in COMPONENTS]))
+            cs.append(np.asarray(st.betaP_V["s", "s"]).copy())
+            dts.append(dt)
+        out["beta0_" + key], out["c0_" + key], out["dt_bound_" + key] = beta0, c0, bound
+        out["betas_" + key], out["cs_" + key], out["dts_" + key] = np.stack(betas), np.stack(cs), np.array(dts)
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
+
+
 CASES = {
     # one flux, one step and 10 steps of 3-D glide+climb dynamics
     "g3d_16": dict(shape=(16, 16, 16), sigma_f=0.05, seed=1, steps=10),
@@ -307,6 +349,8 @@ def main():
         run_io_case(args.reference)
     if args.only in (None, "observables"):
         run_observables_case()
+    if args.only in (None, "vacancy"):
+        run_vacancy_case()
     for name, kw in CASES.items():
         if args.only and name != args.only:
             continue

@@ -34,16 +34,19 @@ def test_instance_struct_layout_matches_ctypes(tmp_path):
     from cdd import _lib
     src = tmp_path / "layout.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\n'
-                   'int main(void){printf("%%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n", sizeof(cdd_instance),'
+                   'int main(void){printf("%%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n", sizeof(cdd_instance),'
                    'offsetof(cdd_instance, mu), offsetof(cdd_instance, has_load),'
                    'offsetof(cdd_instance, load_rate), offsetof(cdd_instance, load_t0),'
-                   'offsetof(cdd_instance, load_nu), offsetof(cdd_instance, dynamics)); return 0;}\n' % HEADER)
+                   'offsetof(cdd_instance, load_nu), offsetof(cdd_instance, dynamics),'
+                   'offsetof(cdd_instance, vacancy), offsetof(cdd_instance, vac_gamma),'
+                   'offsetof(cdd_instance, dt_max)); return 0;}\n' % HEADER)
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-std=c99", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     S = _lib.cdd_instance
     assert got == [ctypes.sizeof(S), S.mu.offset, S.has_load.offset, S.load_rate.offset,
-                   S.load_t0.offset, S.load_nu.offset, S.dynamics.offset]
+                   S.load_t0.offset, S.load_nu.offset, S.dynamics.offset, S.vacancy.offset,
+                   S.vac_gamma.offset, S.dt_max.offset]
 
 
 def test_noalloc_rejects_oversize_grid_without_touching_the_gpu():
