@@ -213,17 +213,20 @@ template <typename T> struct CellCtx {
     const T* bn;    // beta_n of the stage updates
     T* out;         // rhs (flux, stage 1) or the updated state (stages 2, 3)
     T* spd;         // CFL speed (flux mode, optional)
-    const T* vac;   // vacancy concentration (vacancy instances) or null
     long long cells;
     T ih;           // 1 / Dx
     bool has_load, lam_on, glide;
 };
 
-template <typename T, int ND, int MODE, bool GLIDE>
+template <typename T, int ND, int MODE, int VAR>
 __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>& cx, bool valid,
                                              const TileView<T, ND>& tv,
                                              const StageConst& kc_block, const InstClock& ck, double t_flux,
-                                             double& vmax, double& esum, double& zsum) {
+                                             double& vmax, double& esum, double& zsum,
+                                             const T* __restrict__ sig0, const T* __restrict__ vac) {
+    // compile-time variant: bit 0 carries the glide-only projection, bit 1 the vacancy term
+    constexpr bool GLIDE = (VAR & 1) != 0;
+    constexpr bool VAC = (VAR & 2) != 0;
     const T ih = cx.ih;
     const long long cells = cx.cells;
     // FP32 reads the block's stage constants from shared memory; FP64 (no registers to spare across
@@ -256,8 +259,11 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         S[0][1] = S[1][0] = s6[1];
         S[0][2] = S[2][0] = s6[2];
         S[1][2] = S[2][1] = s6[4];
-        if (cx.vac) {   // BetaP_VacancyDynamics.GetSigma (VacancyDynamics.py L23-29): sigma_ii -= alpha c
-            const T ac = (T)I.vac_alpha * *cx.vac;   // (read on use: FP64 has no registers to spare)
+        if (VAC && vac && I.vacancy) {   // BetaP_VacancyDynamics.GetSigma (VacancyDynamics.py L23-29): sigma_ii -= alpha c
+            // the cell's concentration, addressed on use from the kernel arguments (the stress
+            // pointer's offset is the cell index) so that nothing stays live across the march
+            const long long cl = cx.sig - (sig0 + I.soff);
+            const T ac = (T)I.vac_alpha * vac[I.foff / 9 + cl];
             S[0][0] -= ac;
             S[1][1] -= ac;
             S[2][2] -= ac;
@@ -594,7 +600,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
 // grid read zeros, and tiles whose box crosses the periodic boundary patch those cells with
 // wrapped loads after the copy lands. FP32 (6 slots) prefetches plane z+3 while computing z;
 // FP64 (5 slots) refills the slot of z-2 after computing z. Otherwise threads load the box.
-template <typename T, int ND, int MODE, bool GLIDE>
+template <typename T, int ND, int MODE, int VAR>
 __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, double* red, uint64_t* bars,
                                       const StencilMapSet& maps,
                                       const T* __restrict__ bs, const T* bn, T* out,
@@ -694,7 +700,6 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         cx.bn = bn ? bn + I.foff + cl0 : nullptr;   // stage updates only
         cx.out = out + I.foff + cl0;
         cx.spd = speed_out ? speed_out + I.coff + cl0 : nullptr;
-        cx.vac = (I.vacancy && vac) ? vac + I.foff / 9 + cl0 : nullptr;
         cx.cells = cells;
         cx.ih = (T)I.inv_h;
         cx.has_load = I.has_load != 0;
@@ -713,8 +718,12 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         }
         if (use_tma && NS == 6 && more) issued = k + 5;
         if (ND == 3) {
-            // ring planes z-2 .. z+2 live in slots (k + q) mod NS: rotate by one plane per step
-            if (k == 0) {
+            // ring planes z-2 .. z+2 live in slots (k + q) mod NS: FP32 rotates them by one plane
+            // per step; FP64 (no registers to spare across the march) recomputes them
+            if (NS != 6) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) tv.so[q] = ((k + q) % NS) * 9 * PP;
+            } else if (k == 0) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) tv.so[q] = q * 9 * PP;
             } else {
@@ -725,8 +734,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         } else {
             tv.so[2] = 0;
         }
-        stencil_cell<T, ND, MODE, GLIDE>(I, cx, vxy, tv, kc, clk[ii], t_flux, vmax, esum, zsum);
-        if (cx.vac) cx.vac += plane;
+        stencil_cell<T, ND, MODE, VAR>(I, cx, vxy, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac);
         cx.sig += plane;
         if (cx.bn) cx.bn += plane;
         cx.out += plane;
@@ -767,7 +775,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     }
 }
 
-template <typename T, int MODE, bool GLIDE>
+template <typename T, int MODE, int VAR>
 __global__ void __launch_bounds__(ST_THREADS, (sizeof(T) == 4) ? 3 : 2)
 k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre,
           const T* __restrict__ bs, const T* bn, T* out, const T* __restrict__ sig,
@@ -782,10 +790,10 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
     if (I.nd == 3)
-        march<T, 3, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+        march<T, 3, MODE, VAR>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
                           status, vac);
     else
-        march<T, 2, MODE, GLIDE>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
+        march<T, 2, MODE, VAR>(I, ii, lb, sm, red, bars, maps, bs, bn, out, sig, speed_out, clk, t_flux, bmax, bsum,
                           status, vac);
 }
 
@@ -940,22 +948,27 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
     const T* n = (const T*)bn;
     T* o = (T*)out;
     const T* s = (const T*)P.d_sigma;
-    // plans with a glide-only instance run the variant that carries the projection
-#define CDD_LAUNCH_ST(M, SP)                                                                              \
-    if (P.any_glide)                                                                                  \
-        k_stencil<T, M, true><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                                   P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, \
-                                                                   (const T*)P.d_vac, maps);            \
-    else                                                                                              \
-        k_stencil<T, M, false><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP, \
-                                                                    P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status, \
-                                                                    (const T*)P.d_vac, maps)
+    // the variant carries the glide-only projection (bit 0) and the vacancy term (bit 1) only when
+    // the plan has such instances
+    const int var = (P.any_glide ? 1 : 0) | (P.any_vac ? 2 : 0);
+#define CDD_LAUNCH_V(M, V, SP)                                                                           \
+    k_stencil<T, M, V><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP,     \
+                                                             P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status,    \
+                                                             (const T*)P.d_vac, maps)
+#define CDD_LAUNCH_ST(M, SP)                                  \
+    switch (var) {                                            \
+        case 0: CDD_LAUNCH_V(M, 0, SP); break;                \
+        case 1: CDD_LAUNCH_V(M, 1, SP); break;                \
+        case 2: CDD_LAUNCH_V(M, 2, SP); break;                \
+        default: CDD_LAUNCH_V(M, 3, SP); break;               \
+    }
     switch (mode) {
         case M_FLUX: CDD_LAUNCH_ST(M_FLUX, (T*)speed); break;
         case M_STAGE1: CDD_LAUNCH_ST(M_STAGE1, nullptr); break;
         case M_STAGE2: CDD_LAUNCH_ST(M_STAGE2, nullptr); break;
         default: CDD_LAUNCH_ST(M_STAGE3, nullptr); break;
     }
+#undef CDD_LAUNCH_V
 #undef CDD_LAUNCH_ST
 }
 
@@ -1090,14 +1103,17 @@ cudaError_t launch_observe(const PlanCore& P, const void* beta, cudaStream_t st)
 template <typename T>
 static cudaError_t st_attr(size_t smem) {
     cudaError_t e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX, false>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1, false>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2, false>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE3, false>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX, true>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1, true>, smem))) return e;
-    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2, true>, smem))) return e;
-    return set_dyn_smem_limit(k_stencil<T, M_STAGE3, true>, smem);
+#define CDD_ATTR_V(V)                                                                   \
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_FLUX, V>, smem))) return e;              \
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE1, V>, smem))) return e;            \
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE2, V>, smem))) return e;            \
+    if ((e = set_dyn_smem_limit(k_stencil<T, M_STAGE3, V>, smem))) return e;
+    CDD_ATTR_V(0)
+    CDD_ATTR_V(1)
+    CDD_ATTR_V(2)
+    CDD_ATTR_V(3)
+#undef CDD_ATTR_V
+    return cudaSuccess;
 }
 
 cudaError_t stencil_set_attributes(int precision, size_t smem) {
