@@ -242,6 +242,9 @@ __device__ __forceinline__ void vjp_cell(const InstDev& I, long long cl, bool va
     T prod = 1;
 #pragma unroll
     for (int d = 0; d < ND; ++d) prod *= tot[d];
+    // FP32: a cell without gradients has prod = ME^3, below the FP32 range; there hs = 0, and the
+    // smallest normal value keeps every term finite (the forward normalises its weights instead)
+    if (sizeof(T) == 4 && !(prod >= (T)1.17549435e-38f)) prod = (T)1.17549435e-38f;
     const T inv_abc = (T)1 / prod;
     T coef[ND];
 #pragma unroll

@@ -444,6 +444,22 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         pm[d] = -mn;
         tot[d] = pp[d] + pm[d] + (T)ME;
     }
+    // FP32 normalises each axis' upwind weights by its total first (w_d / tot_d in [0, 1]): the
+    // product a_tot b_tot c_tot of a cell without gradients is ME^3, below the smallest FP32
+    // subnormal, and dividing by it would give 0 * inf. FP64 keeps the reference's order.
+    constexpr bool NORMW = (sizeof(T) == 4);
+    T wm[ND], wp[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        if constexpr (NORMW) {
+            const T it = fdiv((T)1, tot[d]);
+            wm[d] = pm[d] * it;
+            wp[d] = pp[d] * it;
+        } else {
+            wm[d] = pm[d];
+            wp[d] = pp[d];
+        }
+    }
     T Q[ND][2][3];
 #pragma unroll
     for (int d = 0; d < ND; ++d)
@@ -459,7 +475,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         sg[2] = (ND == 3) ? (c & 1) : 0;
         T w = (T)1;
 #pragma unroll
-        for (int d = 0; d < ND; ++d) w *= (sg[d] == 0) ? pm[d] : pp[d];
+        for (int d = 0; d < ND; ++d) w *= (sg[d] == 0) ? wm[d] : wp[d];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
             T wv = w * V[c][l];
@@ -467,10 +483,10 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             for (int d = 0; d < ND; ++d) Q[d][sg[d]][l] += wv;
         }
     }
-    T inv_abc = fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
+    const T inv_abc = NORMW ? (T)1 : fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
     T coef[ND];
 #pragma unroll
-    for (int d = 0; d < ND; ++d) coef[d] = fdiv(pm[d] * pp[d], tot[d]);
+    for (int d = 0; d < ND; ++d) coef[d] = NORMW ? pm[d] * wp[d] : fdiv(pm[d] * pp[d], tot[d]);
     T spd = tot[0] + tot[1];
     if (ND == 3) spd += tot[2 % ND];
     if (vsum != vsum) spd = vsum;
