@@ -167,6 +167,18 @@ template <typename V> __device__ __forceinline__ RowPtr* rows_table(V* tws, int 
     return reinterpret_cast<RowPtr*>(tws + ((twspan + 1) & ~1));
 }
 
+// Row passes (R2C / C2R) of a two-stage line plan (R0, R1) in {(16,16), (16,8), (16,4), (8,4)} with
+// P lines per block run their first and last stages in registers (two butterfly loops of P R0 and
+// P R1 trips, whole warps each) and keep one padded buffer of P lines in shared memory; other plans
+// keep two (ping-pong stages).
+__host__ __device__ inline bool rows_io_plan(const LinePlan& lp, int P) {
+    if (lp.nst != 2) return false;
+    const int a = lp.radix[0], b = lp.radix[1];
+    if ((P * a) % 32 != 0 || (P * b) % 32 != 0) return false;
+    return (a == 16 && (b == 16 || b == 8 || b == 4)) || (a == 8 && b == 4);
+}
+__host__ __device__ inline int rows_buffers(const LinePlan& lp, int P) { return rows_io_plan(lp, P) ? 1 : 2; }
+
 // Per-pass tiling of one instance (host-chosen, read by the kernels).
 struct PassTile {
     int blocks;    // blocks this instance contributes to the launch

@@ -187,7 +187,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             t.threads = (velt == 8) ? 256 : 128;
             t.blocks = (int)((npairs + P - 1) / P);
             t.tiles_a = 1;
-            size_t sm = ((2 * (size_t)P * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
+            size_t sm = (((size_t)rows_buffers(I.lp_last, P) * P * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
                         (size_t)I.lp_last.twspan * velt + rows_table_bytes(P);   // buffers + twiddle rows + row table
             if (sm > smem_max[k]) smem_max[k] = sm;
             if (t.threads > thr_max[k]) thr_max[k] = t.threads;

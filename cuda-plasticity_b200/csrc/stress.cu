@@ -93,11 +93,111 @@ __device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mo
 }
 
 // ------------------------------------------------------------------------------------------
+// Row passes of two-stage FFT plans (length N = R0 R1) with the first and the last stage in
+// registers: the first stage's butterflies read their inputs straight from the rows, and the last
+// stage's outputs go straight to the rows, so a tile passes through shared memory once, between
+// the stages. R2C: the last stage's butterfly j of a line (R0 of them, consecutive lanes of one
+// warp) holds X[j + R0 r]; the partner X[N - k] of k = j + R0 r sits in lane R0 - j at register
+// R1 - 1 - r (in its own register R1 - r for j = 0), so one shuffle per r brings it, and the two
+// half spectra of the line's rows are formed and stored from registers. The FP64 row sums of the
+// FP32 form are summed from the first stage's inputs and reduced over the line's R1 lanes.
+// Requires R0 dividing 32, R1 a power of two <= 32 and both stages' butterfly counts multiples of
+// 32 (the block size is too): each warp takes part in a loop trip whole, as the shuffles need
+// (rows_io_plan).
+// ------------------------------------------------------------------------------------------
+template <typename T, bool MEAN64, int R0, int R1>
+__device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int ld, const RowPtr* __restrict__ rt,
+                                            const T* __restrict__ beta, typename VecOf<T>::type* s,
+                                            const typename VecOf<T>::type* __restrict__ tw1,
+                                            typename VecOf<T>::type* __restrict__ dst, double* __restrict__ rowsum,
+                                            long long nrows, long long npairs, int tid, int nt) {
+    typedef typename VecOf<T>::type V;
+    constexpr int N = R0 * R1;
+    const T half = (T)0.5;
+    // stage 0 (span 1): butterfly (l, j) takes elements j + R1 r of pair line l
+#pragma unroll 1
+    for (int g = tid; g < P * R1; g += nt) {
+        const int l = g / R1, j = g - l * R1;
+        const RowPtr ea = rt[2 * l], eb = rt[2 * l + 1];
+        V v[R0];
+        double sa = 0.0, sb = 0.0;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int i = j + R1 * r;
+            T a = 0, b = 0;
+            if (ea.p >= 0) a = half * (beta[ea.p + i] + beta[ea.q + i]);
+            if (eb.p >= 0) b = half * (beta[eb.p + i] + beta[eb.q + i]);
+            if (MEAN64) { sa += (double)a; sb += (double)b; }
+            v[r].x = a;
+            v[r].y = b;
+        }
+        if (MEAN64) {
+#pragma unroll
+            for (int o = R1 / 2; o > 0; o >>= 1) {
+                sa += __shfl_xor_sync(0xffffffffu, sa, o);
+                sb += __shfl_xor_sync(0xffffffffu, sb, o);
+            }
+            const long long row = 2LL * ((long long)lb * P + l);
+            if (j == 0 && row < nrows) rowsum[I.rsoff + row] = sa;
+            if (j == 0 && row + 1 < nrows) rowsum[I.rsoff + row + 1] = sb;
+        }
+        dft<R0, V, false>(v);
+        V* d = s + l * ld + row_pad(j * R0);   // outputs j R0 + r: inside one 16-element pad period
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d[r] = v[r];
+    }
+    __syncthreads();
+    // stage 1 (span R0): butterfly (l, j) takes elements j + R0 r, twiddle row j; outputs X[j + R0 r]
+    const int nh = I.nh;
+#pragma unroll 1
+    for (int g = tid; g < P * R0; g += nt) {
+        const int l = g / R0, j = g - l * R0;
+        V w[R1], v[R1];
+        load_tw_row<R1>(tw1 + j * tw_row(R1), w);
+        const V* sl = s + l * ld + row_pad(j);
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const V x = sl[r * R0 + ((r * R0) >> 4)];
+            v[r] = (r == 0) ? x : vmul(x, w[r]);
+        }
+        dft<R1, V, false>(v);
+        const int lane = tid & 31;
+        const int partner = lane - j + (R0 - j) % R0;
+        const long long p = (long long)lb * P + l;
+        const bool valid = p < npairs;
+        const bool hasb = 2 * p + 1 < nrows;
+        V* da = dst + 2 * p * I.nhp;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            V zs;
+            zs.x = __shfl_sync(0xffffffffu, v[R1 - 1 - r].x, partner);
+            zs.y = __shfl_sync(0xffffffffu, v[R1 - 1 - r].y, partner);
+            const V zm = (j == 0) ? v[(R1 - r) % R1] : zs;
+            const V zk = v[r];
+            const int k = j + R0 * r;
+            if (valid && k < nh) {
+                V a, b;
+                a.x = (T)0.5 * (zk.x + zm.x);
+                a.y = (T)0.5 * (zk.y - zm.y);
+                b.x = (T)0.5 * (zk.y + zm.y);
+                b.y = (T)-0.5 * (zk.x - zm.x);
+                da[k] = a;
+                if (hasb) da[I.nhp + k] = b;
+            }
+        }
+    }
+}
+
+// The two-stage plans the row passes run with register-resident first and last stages (the plans
+// rows_io_plan accepts).
+#define CDD_ROWIO_SEQS(X) X(16, 16) X(16, 8) X(16, 4) X(8, 4)
+
+// ------------------------------------------------------------------------------------------
 // R2C along the contiguous axis of the 6 input components (see RowSource): pairs of real rows
 // (a + i b) per complex FFT. FP32 plans also record FP64 sums of the rows (the k = 0 mode).
 // ------------------------------------------------------------------------------------------
 template <typename T, bool MEAN64>
-__global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_r2c_rows(const InstDev* __restrict__ insts, int n_inst,
                                                   const int* __restrict__ pre,
                                                   const T* __restrict__ beta,
                                                   typename VecOf<T>::type* __restrict__ spec,
@@ -118,7 +218,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     const T half = (T)0.5;
 
     // row table: the two source rows of each of the block's 2P rows (-1: past the last row)
-    V* tws = s + ((2 * P * ld + 1) & ~1);   // twiddle rows, 16-byte aligned after the buffers
+    const bool io = rows_io_plan(I.lp_last, P);
+    V* tws = s + ((rows_buffers(I.lp_last, P) * P * ld + 1) & ~1);   // twiddle rows, 16-byte aligned after the buffers
     RowPtr* rt = rows_table(tws, I.lp_last.twspan);
     for (int r = tid; r < 2 * P; r += nt) {
         const long long ra = 2LL * lb * P + r;
@@ -134,6 +235,18 @@ __global__ void __launch_bounds__(ROW_THREADS) k_r2c_rows(const InstDev* __restr
     }
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     __syncthreads();
+    {
+        const LinePlan& lq = I.lp_last;
+        const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
+#define CDD_R2C_IO(A, B)                                                                                      \
+        if (io && lq.radix[0] == A && lq.radix[1] == B) {                                                     \
+            r2c_rows_io<T, MEAN64, A, B>(I, lb, P, ld, rt, beta, s, tw1, spec + I.spoff, rowsum, nrows, npairs,  \
+                                          tid, nt);                                                           \
+            return;                                                                                           \
+        }
+        CDD_ROWIO_SEQS(CDD_R2C_IO)
+#undef CDD_R2C_IO
+    }
     const bool vec = ((N & 3) == 0) && ((((uintptr_t)(beta + I.foff)) & 15) == 0) &&
                      ((((uintptr_t)(beta + I.soff)) & 15) == 0) && ((((uintptr_t)(beta + I.foff / 9)) & 15) == 0) &&
                      ((I.cells & 3) == 0);
@@ -279,8 +392,83 @@ __device__ __forceinline__ T epilogue1(const T* beta, const RowPtr& e, T coef, i
     return v - coef * (beta[e.p + idx] - b);
 }
 
+// C2R counterpart: the first stage forms z[i] = A[i] + i B[i] of a pair line straight from the
+// half spectra of its two rows (z[N - i] from conjugates), the last stage writes the real rows
+// (plus the FP64 mean stress or the real-space epilogue) straight to global memory.
+template <typename T, bool MEAN64, int R0, int R1>
+__device__ __forceinline__ void c2r_rows_io(const InstDev& I, int lb, int P, int ld, const RowPtr* __restrict__ rt,
+                                            const RowPtr* __restrict__ re, const double* __restrict__ rmean,
+                                            const typename VecOf<T>::type* __restrict__ src,
+                                            typename VecOf<T>::type* s,
+                                            const typename VecOf<T>::type* __restrict__ tw1, T* __restrict__ out,
+                                            const T* __restrict__ beta, int epi, long long nrows, long long npairs,
+                                            int tid, int nt) {
+    typedef typename VecOf<T>::type V;
+    constexpr int N = R0 * R1;
+#pragma unroll 1
+    for (int g = tid; g < P * R1; g += nt) {
+        const int l = g / R1, j = g - l * R1;
+        const long long p = (long long)lb * P + l;
+        const V* sa = (p < npairs) ? src + 2 * p * I.nhp : nullptr;
+        const V* sb = (p < npairs && 2 * p + 1 < nrows) ? sa + I.nhp : nullptr;
+        V v[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int i = j + R1 * r;
+            const int m = (2 * i <= N) ? i : N - i;
+            V A, B;
+            A.x = A.y = B.x = B.y = 0;
+            if (sa) A = sa[m];
+            if (sb) B = sb[m];
+            V z;
+            if (i == 0 || 2 * i == N) { z.x = A.x; z.y = B.x; }
+            else if (2 * i < N) { z.x = A.x - B.y; z.y = A.y + B.x; }
+            else { z.x = A.x + B.y; z.y = B.x - A.y; }
+            v[r] = z;
+        }
+        dft<R0, V, true>(v);
+        V* d = s + l * ld + row_pad(j * R0);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) d[r] = v[r];
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int g = tid; g < P * R0; g += nt) {
+        const int l = g / R0, j = g - l * R0;
+        V w[R1], v[R1];
+        load_tw_row<R1>(tw1 + j * tw_row(R1), w);
+        const V* sl = s + l * ld + row_pad(j);
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const V x = sl[r * R0 + ((r * R0) >> 4)];
+            v[r] = (r == 0) ? x : vmulc(x, w[r]);
+        }
+        dft<R1, V, true>(v);
+        const RowPtr ea = rt[2 * l], eb = rt[2 * l + 1];
+        if (ea.p < 0) continue;
+        const RowPtr xa = re[2 * l], xb = re[2 * l + 1];
+        const T ma = (T)rmean[2 * l], mb = (T)rmean[2 * l + 1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = j + R0 * r;
+            T va = v[r].x, vb = v[r].y;
+            if (MEAN64) { va += ma; vb += mb; }
+            if (epi != EPI_NONE) {
+                va = epilogue1(beta, xa, ma, k, va);
+                if (eb.p >= 0) vb = epilogue1(beta, xb, mb, k, vb);
+            }
+            out[ea.p + k] = va;
+            if (ea.q != ea.p) out[ea.q + k] = va;
+            if (eb.p >= 0) {
+                out[eb.p + k] = vb;
+                if (eb.q != eb.p) out[eb.q + k] = vb;
+            }
+        }
+    }
+}
+
 template <typename T, bool MEAN64>
-__global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_c2r_rows(const InstDev* __restrict__ insts, int n_inst,
                                                   const int* __restrict__ pre,
                                                   const typename VecOf<T>::type* __restrict__ spec,
                                                   T* __restrict__ out,
@@ -301,30 +489,8 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
     const long long npairs = (nrows + 1) / 2;
     const int tid = threadIdx.x, nt = blockDim.x;
     const V* src = spec + I.spoff;
-
-#pragma unroll 4
-    for (int i = tid; i < P * nh; i += nt) {
-        int pl = fdiv_q(I.fd_nh, i), k = i - pl * nh;
-        long long p = (long long)lb * P + pl;
-        V A, B;
-        A.x = A.y = B.x = B.y = 0;
-        if (p < npairs) {
-            long long ra = 2 * p;
-            A = src[ra * I.nhp + k];
-            if (ra + 1 < nrows) B = src[(ra + 1) * I.nhp + k];
-        }
-        V z;
-        if (k == 0 || 2 * k == N) {
-            z.x = A.x; z.y = B.x;
-            s[pl * ld + row_pad(k)] = z;
-        } else {
-            z.x = A.x - B.y; z.y = A.y + B.x;
-            s[pl * ld + row_pad(k)] = z;
-            z.x = A.x + B.y; z.y = B.x - A.y;
-            s[pl * ld + row_pad(N - k)] = z;
-        }
-    }
-    V* tws = s + ((2 * P * ld + 1) & ~1);
+    const bool io = rows_io_plan(I.lp_last, P);
+    V* tws = s + ((rows_buffers(I.lp_last, P) * P * ld + 1) & ~1);
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
     // row table: the destination rows of each of the block's 2P rows and their FP64 mean stress
     RowPtr* rt = rows_table(tws, I.lp_last.twspan);
@@ -354,6 +520,40 @@ __global__ void __launch_bounds__(ROW_THREADS) k_c2r_rows(const InstDev* __restr
         rt[r] = e;
         re[r] = ep;
         rmean[r] = m;
+    }
+    {
+        const LinePlan& lq = I.lp_last;
+        const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
+#define CDD_C2R_IO(A, B)                                                                                      \
+        if (io && lq.radix[0] == A && lq.radix[1] == B) {                                                     \
+            c2r_rows_io<T, MEAN64, A, B>(I, lb, P, ld, rt, re, rmean, src, s, tw1, out, beta, epi, nrows, npairs, \
+                                          tid, nt);                                                           \
+            return;                                                                                           \
+        }
+        CDD_ROWIO_SEQS(CDD_C2R_IO)
+#undef CDD_C2R_IO
+    }
+#pragma unroll 4
+    for (int i = tid; i < P * nh; i += nt) {
+        int pl = fdiv_q(I.fd_nh, i), k = i - pl * nh;
+        long long p = (long long)lb * P + pl;
+        V A, B;
+        A.x = A.y = B.x = B.y = 0;
+        if (p < npairs) {
+            long long ra = 2 * p;
+            A = src[ra * I.nhp + k];
+            if (ra + 1 < nrows) B = src[(ra + 1) * I.nhp + k];
+        }
+        V z;
+        if (k == 0 || 2 * k == N) {
+            z.x = A.x; z.y = B.x;
+            s[pl * ld + row_pad(k)] = z;
+        } else {
+            z.x = A.x - B.y; z.y = A.y + B.x;
+            s[pl * ld + row_pad(k)] = z;
+            z.x = A.x + B.y; z.y = B.x - A.y;
+            s[pl * ld + row_pad(N - k)] = z;
+        }
     }
     __syncthreads();
     RowLayout lay{P, ld};
