@@ -151,6 +151,241 @@ __device__ __forceinline__ void derivs5(const T* v, T ih, T& up, T& um) {
     um = (dm1 + (T)0.5 * ddm) * ih;
 }
 
+// ---- FP32 flux with paired arithmetic ----
+// Every quantity of the central-upwind flux that comes in a forward / backward pair (one-sided
+// derivatives u+ / u-, the A, S_d, P, trace and Q sums, the final per-axis coefficients) is kept
+// as one float2 (x: forward, y: backward) and updated with the packed FP32 instructions
+// (__ffma2_rn, __fadd2_rn, __fmul2_rn: two lanes per instruction, each rounded as the scalar
+// operation). The corners pair up along the last axis: corners 2m and 2m + 1 differ only in
+// its sign. Same formulas as the scalar path; the rhs sums are regrouped per one-sided
+// derivative: rhs_ij = sum_d [(c_d - Q+_dd) (u+_d)_ij + (-c_d - Q-_dd) (u-_d)_ij]
+//                      + [i < ND] sum_{s,l} Q^s_il (u^s_i)_lj,
+// with c_d = a+_d a-_d / tot_d, i.e. -H / (a_tot b_tot c_tot) + the viscous term of the scalar form.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 derivs5_f2(const float* v, float2 ihh) {
+    const float dm2 = v[1] - v[0], dm1 = v[2] - v[1], d0 = v[3] - v[2], d1 = v[4] - v[3];
+    const float e0 = d1 - d0, em1 = d0 - dm1, em2 = dm1 - dm2;
+    float dd0, ddm;
+    minmod_pair(e0, em1, em2, dd0, ddm);
+    return __fmul2_rn(__ffma2_rn(f2(dd0, ddm), f2(-0.5f, 0.5f), f2(d0, dm1)), ihh);
+}
+__device__ __forceinline__ float lane(const float2& v, int s) { return s ? v.y : v.x; }
+
+template <int ND, bool GLIDE>
+__device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih, const float (&S)[3][3],
+                                         bool lam_on, bool glide, float Lambda, float (&rhs)[9], float& spd) {
+    constexpr int NC = 1 << ND;
+    constexpr int NP = (ND == 3) ? 3 : 1;
+    const float2 z2 = f2(0.0f, 0.0f);
+    float2 U[ND][9];   // (u+_d, u-_d) of component c = 3 l + j (row l, column j)
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            float v5[5];
+            tv.load5(c, d, v5);
+            U[d][c] = derivs5_f2(v5, f2(ih, ih));
+        }
+    const float str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / 3.0f * Lambda : 0.0f;
+
+    // pass 1: A_d l = sum_j (u_d)_lj S_dj, S_d = sum_{l,j} (u_d)_lj S_lj, P_d = sum_{l != d, j} (u_d)_lj^2,
+    // tr(u_d), C_de[s_d][s_e] = sum_j (u_d)_ej (u_e)_dj
+    float2 A[ND][3], Sd[ND], Pq[ND], trU[ND];
+    float Cp[NP][2][2];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        Sd[d] = z2; Pq[d] = z2; trU[d] = z2;
+#pragma unroll
+        for (int l = 0; l < 3; ++l) A[d][l] = z2;
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) Cp[p][a][b] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const float2 sdj = f2(S[d][j], S[d][j]);
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                const float2 u = U[d][3 * l + j];
+                A[d][l] = __ffma2_rn(u, sdj, A[d][l]);
+                Sd[d] = __ffma2_rn(u, f2(S[l][j], S[l][j]), Sd[d]);
+                if (l != d) Pq[d] = __ffma2_rn(u, u, Pq[d]);
+            }
+            if (lam_on || glide) trU[d] = __fadd2_rn(trU[d], U[d][4 * j]);
+            if (lam_on && j == d) {
+#pragma unroll
+                for (int l = 0; l < 3; ++l) A[d][l] = __ffma2_rn(f2(-str, -str), U[d][3 * l + j], A[d][l]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                Cp[0][a][b] += lane(U[0][3 + j], a) * lane(U[1 % ND][j], b);
+                if (ND == 3) {
+                    Cp[1 % NP][a][b] += lane(U[1 % ND][6 + j], a) * lane(U[2 % ND][3 + j], b);
+                    Cp[2 % NP][a][b] += lane(U[2 % ND][j], a) * lane(U[0][6 + j], b);
+                }
+            }
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        A[d][d] = __fadd2_rn(A[d][d], f2(-Sd[d].x, -Sd[d].y));
+        if (lam_on) A[d][d] = __ffma2_rn(f2(str, str), trU[d], A[d][d]);
+    }
+
+    // corners: V = (A_x[sx] + A_y[sy] (+ A_z[sz])) / |rho|, paired along the last axis
+    float2 V[NC / 2][3];
+    float2 vs2 = z2;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
+#pragma unroll
+    for (int m = 0; m < NC / 2; ++m) {
+        float av[2][3], inv[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = 2 * m + h;
+            const int sx = (c >> (ND - 1)) & 1, sy = (c >> (ND - 2)) & 1;
+            const int sz = (ND == 3) ? (c & 1) : 0;
+            float rho2;
+            if (ND == 3)
+                rho2 = (float)ME + lane(Pq[0], sx) + lane(Pq[1 % ND], sy) + lane(Pq[2 % ND], sz)
+                       - 2.0f * (Cp[0][sx][sy] + Cp[1 % NP][sy][sz] + Cp[2 % NP][sz][sx]);
+            else
+                rho2 = (float)ME + lane(Pq[0], sx) + lane(Pq[1 % ND], sy) - 2.0f * Cp[0][sx][sy];
+            inv[h] = inv_sqrt(rho2);
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                float a = lane(A[0][l], sx) + lane(A[1 % ND][l], sy);
+                if (ND == 3) a += lane(A[2 % ND][l], sz);
+                av[h][l] = a;
+            }
+            if (GLIDE && glide) {
+                // glide-only projection (CentralUpwindHJBetaPGlideOnlyDynamics.py L152-201, 2-D L96-129):
+                // g_d = tr(u_d) - sum_e (u_e)_{d e}, v += g (ME + v.g) / (ME + g.g), then v / |rho|
+                const int sgc[3] = {sx, sy, sz};
+                float gv[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    float Dd = 0.0f;
+#pragma unroll
+                    for (int e = 0; e < ND; ++e) Dd += lane(U[e][3 * d + e], sgc[e]);
+                    const float tr = (d < ND) ? lane(trU[d % ND], sgc[d]) : 0.0f;
+                    gv[d] = tr - Dd;
+                }
+                const float rr = (float)ME + gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
+                const float rv = (float)ME + av[h][0] * gv[0] + av[h][1] * gv[1] + av[h][2] * gv[2];
+                const float f = fdiv(rv, rr);
+#pragma unroll
+                for (int l = 0; l < 3; ++l) av[h][l] += gv[l] * f;
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            V[m][l] = __fmul2_rn(f2(av[0][l], av[1][l]), f2(inv[0], inv[1]));
+            vs2 = __fadd2_rn(vs2, V[m][l]);
+        }
+    }
+    // one-sided speeds a+_d = max(0, max V_d), a-_d = -min(0, min V_d); weights normalised by
+    // tot_d = a+_d + a-_d + ME first (the product of the three totals can underflow FP32)
+    float pp[ND], pm[ND], wm[ND], wp[ND];
+    spd = 0.0f;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        float mx = 0.0f, mn = 0.0f;
+#pragma unroll
+        for (int m = 0; m < NC / 2; ++m) {
+            mx = fmaxf(mx, fmaxf(V[m][d].x, V[m][d].y));
+            mn = fminf(mn, fminf(V[m][d].x, V[m][d].y));
+        }
+        pp[d] = mx;
+        pm[d] = -mn;
+        const float tot = pp[d] + pm[d] + (float)ME;
+        spd += tot;
+        const float it = fdiv(1.0f, tot);
+        wm[d] = pm[d] * it;
+        wp[d] = pp[d] * it;
+    }
+    const float vsum = vs2.x + vs2.y;
+    if (vsum != vsum) spd = vsum;
+
+    // Q^s_dl = sum over corners with s_d = s of w_c V_cl (w_c: product of the weights a-_d / tot_d
+    // or a+_d / tot_d of the corner's signs)
+    float2 Q[ND][3];
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) Q[d][l] = z2;
+#pragma unroll
+    for (int m = 0; m < NC / 2; ++m) {
+        const int c = 2 * m;
+        int sg[2];
+        sg[0] = (c >> (ND - 1)) & 1;
+        sg[1] = (ND == 3) ? ((c >> 1) & 1) : 0;
+        float wb = 1.0f;
+#pragma unroll
+        for (int d = 0; d < ND - 1; ++d) wb *= (sg[d] == 0) ? wm[d] : wp[d];
+        const float2 w2 = f2(wb * wm[ND - 1], wb * wp[ND - 1]);
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const float2 wv = __fmul2_rn(w2, V[m][l]);
+            const float sum = wv.x + wv.y;
+#pragma unroll
+            for (int d = 0; d < ND - 1; ++d) {
+                if (sg[d] == 0) Q[d][l].x += sum;
+                else Q[d][l].y += sum;
+            }
+            Q[ND - 1][l] = __fadd2_rn(Q[ND - 1][l], wv);
+        }
+    }
+
+    // pass 2: rhs
+    float2 G[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const float coef = pm[d] * wp[d];
+        const float2 qdd = (d == 0) ? Q[d][0] : ((d == 1) ? Q[d][1] : Q[d][2]);
+        G[d] = f2(coef - qdd.x, -coef - qdd.y);
+    }
+    float2 Jp2 = z2;   // Lambda trace term, J = -Lambda/3 (Jp2.x + Jp2.y)
+    if (lam_on) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const float2 qdd = (d == 0) ? Q[d][0] : ((d == 1) ? Q[d][1] : Q[d][2]);
+            Jp2 = __ffma2_rn(qdd, trU[d], Jp2);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float2 acc = __fmul2_rn(G[0], U[0][3 * i + j]);
+#pragma unroll
+            for (int d = 1; d < ND; ++d) acc = __ffma2_rn(G[d], U[d][3 * i + j], acc);
+            if (i < ND) {
+#pragma unroll
+                for (int l = 0; l < 3; ++l) acc = __ffma2_rn(Q[i % ND][l], U[i % ND][3 * l + j], acc);
+            }
+            rhs[3 * i + j] = acc.x + acc.y;
+        }
+        if (lam_on && j < ND) {
+#pragma unroll
+            for (int l = 0; l < 3; ++l)
+                Jp2 = __ffma2_rn(f2(-Q[j % ND][l].x, -Q[j % ND][l].y), U[j % ND][3 * l + j], Jp2);
+        }
+    }
+    if (lam_on) {
+        // the trace term enters H_ii, so rhs_ii gets -J / (a_tot b_tot c_tot) (weights normalised)
+        const float J = -Lambda / 3.0f * (Jp2.x + Jp2.y);
+        rhs[0] -= J;
+        rhs[4] -= J;
+        rhs[8] -= J;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T block_reduce_max(T v, T* red) {
 #pragma unroll
@@ -269,299 +504,304 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             S[2][2] -= ac;
         }
     }
-    const bool lam_on = cx.lam_on;
-    const bool glide = GLIDE && cx.glide;   // glide-only dynamics (Lambda is 0 then)
-    const T str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / (T)3 * (T)I.Lambda : (T)0;
-
-    // ---------------- pass 1: A, P, C, trace ----------------
-    T A[ND][2][3], Sd[ND][2], Pq[ND][2], trU[ND][2];
-    constexpr int NP = (ND == 3) ? 3 : 1;
-    T Cp[NP][2][2];
-#pragma unroll
-    for (int d = 0; d < ND; ++d)
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            Sd[d][s] = 0; Pq[d][s] = 0; trU[d][s] = 0;
-#pragma unroll
-            for (int l = 0; l < 3; ++l) A[d][s][l] = 0;
-        }
-#pragma unroll
-    for (int p = 0; p < NP; ++p)
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) Cp[p][a][b] = 0;
-
-    // FP32 keeps all 54 one-sided derivatives in registers for pass 2; FP64 recomputes them
-    // from shared memory (register budget).
-    constexpr bool KEEPU = (sizeof(T) == 4);
-    T Ukeep[KEEPU ? ND : 1][2][9];
-    T Dv[(KEEPU || !GLIDE) ? 1 : ND][2][3];   // glide-only, FP64: (u_e)_{d e} per axis e and sign
-    if constexpr (KEEPU) {
-        // all derivatives first (shared memory only), so that the stress loads issued above have
-        // the whole derivative evaluation to arrive before the first use
-#pragma unroll
-        for (int c = 0; c < 9; ++c)
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                T v5[5];
-                tv.load5(c, d, v5);
-                derivs5(v5, ih, Ukeep[d][0][c], Ukeep[d][1][c]);
-            }
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        T U[ND][2][3];
-        if constexpr (KEEPU) {
-#pragma unroll
-            for (int d = 0; d < ND; ++d)
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
-        } else {
-#pragma unroll
-            for (int l = 0; l < 3; ++l) {
-#pragma unroll
-                for (int d = 0; d < ND; ++d) {
-                    T v5[5];
-                    tv.load5(3 * l + j, d, v5);
-                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
-                }
-            }
-        }
-        T Sj[3], Sdj[3];
-#pragma unroll
-        for (int l = 0; l < 3; ++l) { Sj[l] = (j == 0) ? S[l][0] : ((j == 1) ? S[l][1] : S[l][2]); }
-#pragma unroll
-        for (int d = 0; d < ND; ++d) Sdj[d] = (j == 0) ? S[d][0] : ((j == 1) ? S[d][1] : S[d][2]);
-#pragma unroll
-        for (int d = 0; d < ND; ++d)
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-#pragma unroll
-                for (int l = 0; l < 3; ++l) {
-                    T v = U[d][s][l];
-                    A[d][s][l] += v * Sdj[d];
-                    Sd[d][s] += v * Sj[l];
-                    if (l != d) Pq[d][s] += v * v;
-                }
-                if (lam_on || glide) {
-                    // trace of u_d (components (j, j))
-                    T dj = (j == 0) ? U[d][s][0] : ((j == 1) ? U[d][s][1] : U[d][s][2]);
-                    trU[d][s] += dj;
-                }
-                if (lam_on && j == d) {
-                    // the -str (u_d)_{l d} terms
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) A[d][s][l] -= str * U[d][s][l];
-                }
-            }
-        if constexpr (!KEEPU && GLIDE) {
-            if (glide && j < ND) {
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) Dv[j % ND][s][l] = U[j % ND][s][l];
-            }
-        }
-        // pair terms C_de[s_d][s_e] = sum_j (u_d)_ej (u_e)_dj
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                Cp[0][a][b] += U[0][a][1] * U[1][b][0];
-                if (ND == 3) {
-                    Cp[1 % NP][a][b] += U[1 % ND][a][2] * U[2 % ND][b][1];
-                    Cp[2 % NP][a][b] += U[2 % ND][a][0] * U[0][b][2];
-                }
-            }
-    }
-#pragma unroll
-    for (int d = 0; d < ND; ++d)
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            T ad = (d == 0) ? A[d][s][0] : ((d == 1) ? A[d][s][1] : A[d][s][2]);
-            ad -= Sd[d][s];
-            if (lam_on) ad += str * trU[d][s];
-            if (d == 0) A[d][s][0] = ad; else if (d == 1) A[d][s][1] = ad; else A[d][s][2] = ad;
-        }
-
-    // ---------------- corners: V, speeds, weights, Q ----------------
-    constexpr int NC = 1 << ND;
-    T V[NC][3];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const int sx = (c >> (ND - 1)) & 1, sy = (c >> (ND - 2)) & 1;
-        const int sz = (ND == 3) ? (c & 1) : 0;
-        T rho2;
-        if (ND == 3)
-            rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] + Pq[2 % ND][sz]
-                   - (T)2 * (Cp[0][sx][sy] + Cp[1 % NP][sy][sz] + Cp[2 % NP][sz][sx]);
-        else
-            rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] - (T)2 * Cp[0][sx][sy];
-        T inv = inv_sqrt(rho2);
-        T av[3];
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            T a = A[0][sx][l] + A[1][sy][l];
-            if (ND == 3) a += A[2 % ND][sz][l];
-            av[l] = a;
-        }
-        if (glide) {
-            // glide-only projection (CentralUpwindHJBetaPGlideOnlyDynamics.py L152-201, 2-D L96-129):
-            // g_d = tr(u_d) - sum_e (u_e)_{d e}, v += g (ME + v.g) / (ME + g.g), then v / |rho|
-            const int sgc[3] = {sx, sy, sz};
-            T gv[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                T Dd = (T)0;
-#pragma unroll
-                for (int e = 0; e < ND; ++e) {
-                    if constexpr (KEEPU) Dd += Ukeep[e][sgc[e]][3 * d + e];
-                    else if constexpr (GLIDE) Dd += Dv[e][sgc[e]][d];
-                }
-                const T tr = (d < ND) ? trU[d % ND][sgc[d]] : (T)0;
-                gv[d] = tr - Dd;
-            }
-            const T rr = (T)ME + gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
-            const T rv = (T)ME + av[0] * gv[0] + av[1] * gv[1] + av[2] * gv[2];
-            const T f = fdiv(rv, rr);
-#pragma unroll
-            for (int l = 0; l < 3; ++l) av[l] += gv[l] * f;
-        }
-#pragma unroll
-        for (int l = 0; l < 3; ++l) V[c][l] = av[l] * inv;
-    }
-    T pp[ND], pm[ND], tot[ND];
-    T vsum = 0;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        T mx = (T)0, mn = (T)0;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) { mx = fmax(mx, V[c][d]); mn = fmin(mn, V[c][d]); vsum += V[c][d]; }
-        pp[d] = mx;
-        pm[d] = -mn;
-        tot[d] = pp[d] + pm[d] + (T)ME;
-    }
-    // FP32 normalises each axis' upwind weights by its total first (w_d / tot_d in [0, 1]): the
-    // product a_tot b_tot c_tot of a cell without gradients is ME^3, below the smallest FP32
-    // subnormal, and dividing by it would give 0 * inf. FP64 keeps the reference's order.
-    constexpr bool NORMW = (sizeof(T) == 4);
-    T wm[ND], wp[ND];
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        if constexpr (NORMW) {
-            const T it = fdiv((T)1, tot[d]);
-            wm[d] = pm[d] * it;
-            wp[d] = pp[d] * it;
-        } else {
-            wm[d] = pm[d];
-            wp[d] = pp[d];
-        }
-    }
-    T Q[ND][2][3];
-#pragma unroll
-    for (int d = 0; d < ND; ++d)
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-            for (int l = 0; l < 3; ++l) Q[d][s][l] = 0;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        int sg[3];
-        sg[0] = (c >> (ND - 1)) & 1;
-        sg[1] = (c >> (ND - 2)) & 1;
-        sg[2] = (ND == 3) ? (c & 1) : 0;
-        T w = (T)1;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) w *= (sg[d] == 0) ? wm[d] : wp[d];
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            T wv = w * V[c][l];
-#pragma unroll
-            for (int d = 0; d < ND; ++d) Q[d][sg[d]][l] += wv;
-        }
-    }
-    const T inv_abc = NORMW ? (T)1 : fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
-    T coef[ND];
-#pragma unroll
-    for (int d = 0; d < ND; ++d) coef[d] = NORMW ? pm[d] * wp[d] : fdiv(pm[d] * pp[d], tot[d]);
-    T spd = tot[0] + tot[1];
-    if (ND == 3) spd += tot[2 % ND];
-    if (vsum != vsum) spd = vsum;
-
-    // ---------------- pass 2: rhs ----------------
     T rhs[9];
-    T Jp = 0;   // Lambda trace term, J = -Lambda/3 * Jp
-    if (lam_on) {
-#pragma unroll
+    T spd;
+    if constexpr (sizeof(T) == 4) {
+        flux_f32<ND, GLIDE>(tv, ih, S, cx.lam_on, GLIDE && cx.glide, (float)I.Lambda, rhs, spd);
+    } else {
+        const bool lam_on = cx.lam_on;
+        const bool glide = GLIDE && cx.glide;   // glide-only dynamics (Lambda is 0 then)
+        const T str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / (T)3 * (T)I.Lambda : (T)0;
+
+        // ---------------- pass 1: A, P, C, trace ----------------
+        T A[ND][2][3], Sd[ND][2], Pq[ND][2], trU[ND][2];
+        constexpr int NP = (ND == 3) ? 3 : 1;
+        T Cp[NP][2][2];
+    #pragma unroll
         for (int d = 0; d < ND; ++d)
-#pragma unroll
+    #pragma unroll
             for (int s = 0; s < 2; ++s) {
-                T qdd = (d == 0) ? Q[d][s][0] : ((d == 1) ? Q[d][s][1] : Q[d][s][2]);
-                Jp += qdd * trU[d][s];
+                Sd[d][s] = 0; Pq[d][s] = 0; trU[d][s] = 0;
+    #pragma unroll
+                for (int l = 0; l < 3; ++l) A[d][s][l] = 0;
             }
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        T U[ND][2][3];
+    #pragma unroll
+        for (int p = 0; p < NP; ++p)
+    #pragma unroll
+            for (int a = 0; a < 2; ++a)
+    #pragma unroll
+                for (int b = 0; b < 2; ++b) Cp[p][a][b] = 0;
+
+        // FP32 keeps all 54 one-sided derivatives in registers for pass 2; FP64 recomputes them
+        // from shared memory (register budget).
+        constexpr bool KEEPU = (sizeof(T) == 4);
+        T Ukeep[KEEPU ? ND : 1][2][9];
+        T Dv[(KEEPU || !GLIDE) ? 1 : ND][2][3];   // glide-only, FP64: (u_e)_{d e} per axis e and sign
         if constexpr (KEEPU) {
-#pragma unroll
-            for (int d = 0; d < ND; ++d)
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
-        } else {
-#pragma unroll
-            for (int l = 0; l < 3; ++l) {
-#pragma unroll
+            // all derivatives first (shared memory only), so that the stress loads issued above have
+            // the whole derivative evaluation to arrive before the first use
+    #pragma unroll
+            for (int c = 0; c < 9; ++c)
+    #pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     T v5[5];
-                    tv.load5(3 * l + j, d, v5);
-                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                    tv.load5(c, d, v5);
+                    derivs5(v5, ih, Ukeep[d][0][c], Ukeep[d][1][c]);
+                }
+        }
+    #pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T U[ND][2][3];
+            if constexpr (KEEPU) {
+    #pragma unroll
+                for (int d = 0; d < ND; ++d)
+    #pragma unroll
+                    for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
+            } else {
+    #pragma unroll
+                for (int l = 0; l < 3; ++l) {
+    #pragma unroll
+                    for (int d = 0; d < ND; ++d) {
+                        T v5[5];
+                        tv.load5(3 * l + j, d, v5);
+                        derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                    }
                 }
             }
+            T Sj[3], Sdj[3];
+    #pragma unroll
+            for (int l = 0; l < 3; ++l) { Sj[l] = (j == 0) ? S[l][0] : ((j == 1) ? S[l][1] : S[l][2]); }
+    #pragma unroll
+            for (int d = 0; d < ND; ++d) Sdj[d] = (j == 0) ? S[d][0] : ((j == 1) ? S[d][1] : S[d][2]);
+    #pragma unroll
+            for (int d = 0; d < ND; ++d)
+    #pragma unroll
+                for (int s = 0; s < 2; ++s) {
+    #pragma unroll
+                    for (int l = 0; l < 3; ++l) {
+                        T v = U[d][s][l];
+                        A[d][s][l] += v * Sdj[d];
+                        Sd[d][s] += v * Sj[l];
+                        if (l != d) Pq[d][s] += v * v;
+                    }
+                    if (lam_on || glide) {
+                        // trace of u_d (components (j, j))
+                        T dj = (j == 0) ? U[d][s][0] : ((j == 1) ? U[d][s][1] : U[d][s][2]);
+                        trU[d][s] += dj;
+                    }
+                    if (lam_on && j == d) {
+                        // the -str (u_d)_{l d} terms
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) A[d][s][l] -= str * U[d][s][l];
+                    }
+                }
+            if constexpr (!KEEPU && GLIDE) {
+                if (glide && j < ND) {
+    #pragma unroll
+                    for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) Dv[j % ND][s][l] = U[j % ND][s][l];
+                }
+            }
+            // pair terms C_de[s_d][s_e] = sum_j (u_d)_ej (u_e)_dj
+    #pragma unroll
+            for (int a = 0; a < 2; ++a)
+    #pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    Cp[0][a][b] += U[0][a][1] * U[1][b][0];
+                    if (ND == 3) {
+                        Cp[1 % NP][a][b] += U[1 % ND][a][2] * U[2 % ND][b][1];
+                        Cp[2 % NP][a][b] += U[2 % ND][a][0] * U[0][b][2];
+                    }
+                }
         }
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            T hs = 0, vis = 0;
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                T gp = (d == 0) ? Q[d][0][0] : ((d == 1) ? Q[d][0][1] : Q[d][0][2]);
-                T gm = (d == 0) ? Q[d][1][0] : ((d == 1) ? Q[d][1][1] : Q[d][1][2]);
-                hs += gp * U[d][0][i] + gm * U[d][1][i];
-                vis += (U[d][0][i] - U[d][1][i]) * coef[d];
+    #pragma unroll
+        for (int d = 0; d < ND; ++d)
+    #pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                T ad = (d == 0) ? A[d][s][0] : ((d == 1) ? A[d][s][1] : A[d][s][2]);
+                ad -= Sd[d][s];
+                if (lam_on) ad += str * trU[d][s];
+                if (d == 0) A[d][s][0] = ad; else if (d == 1) A[d][s][1] = ad; else A[d][s][2] = ad;
             }
-            if (i < ND) {
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) hs -= Q[i % ND][s][l] * U[i % ND][s][l];
+
+        // ---------------- corners: V, speeds, weights, Q ----------------
+        constexpr int NC = 1 << ND;
+        T V[NC][3];
+    #pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int sx = (c >> (ND - 1)) & 1, sy = (c >> (ND - 2)) & 1;
+            const int sz = (ND == 3) ? (c & 1) : 0;
+            T rho2;
+            if (ND == 3)
+                rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] + Pq[2 % ND][sz]
+                       - (T)2 * (Cp[0][sx][sy] + Cp[1 % NP][sy][sz] + Cp[2 % NP][sz][sx]);
+            else
+                rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] - (T)2 * Cp[0][sx][sy];
+            T inv = inv_sqrt(rho2);
+            T av[3];
+    #pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                T a = A[0][sx][l] + A[1][sy][l];
+                if (ND == 3) a += A[2 % ND][sz][l];
+                av[l] = a;
             }
-            T r = -hs * inv_abc + vis;
-            if (j == 0) { if (i == 0) rhs[0] = r; else if (i == 1) rhs[3] = r; else rhs[6] = r; }
-            else if (j == 1) { if (i == 0) rhs[1] = r; else if (i == 1) rhs[4] = r; else rhs[7] = r; }
-            else { if (i == 0) rhs[2] = r; else if (i == 1) rhs[5] = r; else rhs[8] = r; }
+            if (glide) {
+                // glide-only projection (CentralUpwindHJBetaPGlideOnlyDynamics.py L152-201, 2-D L96-129):
+                // g_d = tr(u_d) - sum_e (u_e)_{d e}, v += g (ME + v.g) / (ME + g.g), then v / |rho|
+                const int sgc[3] = {sx, sy, sz};
+                T gv[3];
+    #pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    T Dd = (T)0;
+    #pragma unroll
+                    for (int e = 0; e < ND; ++e) {
+                        if constexpr (KEEPU) Dd += Ukeep[e][sgc[e]][3 * d + e];
+                        else if constexpr (GLIDE) Dd += Dv[e][sgc[e]][d];
+                    }
+                    const T tr = (d < ND) ? trU[d % ND][sgc[d]] : (T)0;
+                    gv[d] = tr - Dd;
+                }
+                const T rr = (T)ME + gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
+                const T rv = (T)ME + av[0] * gv[0] + av[1] * gv[1] + av[2] * gv[2];
+                const T f = fdiv(rv, rr);
+    #pragma unroll
+                for (int l = 0; l < 3; ++l) av[l] += gv[l] * f;
+            }
+    #pragma unroll
+            for (int l = 0; l < 3; ++l) V[c][l] = av[l] * inv;
+        }
+        T pp[ND], pm[ND], tot[ND];
+        T vsum = 0;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
+    #pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            T mx = (T)0, mn = (T)0;
+    #pragma unroll
+            for (int c = 0; c < NC; ++c) { mx = fmax(mx, V[c][d]); mn = fmin(mn, V[c][d]); vsum += V[c][d]; }
+            pp[d] = mx;
+            pm[d] = -mn;
+            tot[d] = pp[d] + pm[d] + (T)ME;
+        }
+        // FP32 normalises each axis' upwind weights by its total first (w_d / tot_d in [0, 1]): the
+        // product a_tot b_tot c_tot of a cell without gradients is ME^3, below the smallest FP32
+        // subnormal, and dividing by it would give 0 * inf. FP64 keeps the reference's order.
+        constexpr bool NORMW = (sizeof(T) == 4);
+        T wm[ND], wp[ND];
+    #pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            if constexpr (NORMW) {
+                const T it = fdiv((T)1, tot[d]);
+                wm[d] = pm[d] * it;
+                wp[d] = pp[d] * it;
+            } else {
+                wm[d] = pm[d];
+                wp[d] = pp[d];
+            }
+        }
+        T Q[ND][2][3];
+    #pragma unroll
+        for (int d = 0; d < ND; ++d)
+    #pragma unroll
+            for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                for (int l = 0; l < 3; ++l) Q[d][s][l] = 0;
+    #pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            int sg[3];
+            sg[0] = (c >> (ND - 1)) & 1;
+            sg[1] = (c >> (ND - 2)) & 1;
+            sg[2] = (ND == 3) ? (c & 1) : 0;
+            T w = (T)1;
+    #pragma unroll
+            for (int d = 0; d < ND; ++d) w *= (sg[d] == 0) ? wm[d] : wp[d];
+    #pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                T wv = w * V[c][l];
+    #pragma unroll
+                for (int d = 0; d < ND; ++d) Q[d][sg[d]][l] += wv;
+            }
+        }
+        const T inv_abc = NORMW ? (T)1 : fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
+        T coef[ND];
+    #pragma unroll
+        for (int d = 0; d < ND; ++d) coef[d] = NORMW ? pm[d] * wp[d] : fdiv(pm[d] * pp[d], tot[d]);
+        spd = tot[0] + tot[1];
+        if (ND == 3) spd += tot[2 % ND];
+        if (vsum != vsum) spd = vsum;
+
+        // ---------------- pass 2: rhs ----------------
+        T Jp = 0;   // Lambda trace term, J = -Lambda/3 * Jp
+        if (lam_on) {
+    #pragma unroll
+            for (int d = 0; d < ND; ++d)
+    #pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    T qdd = (d == 0) ? Q[d][s][0] : ((d == 1) ? Q[d][s][1] : Q[d][s][2]);
+                    Jp += qdd * trU[d][s];
+                }
+        }
+    #pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T U[ND][2][3];
+            if constexpr (KEEPU) {
+    #pragma unroll
+                for (int d = 0; d < ND; ++d)
+    #pragma unroll
+                    for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
+            } else {
+    #pragma unroll
+                for (int l = 0; l < 3; ++l) {
+    #pragma unroll
+                    for (int d = 0; d < ND; ++d) {
+                        T v5[5];
+                        tv.load5(3 * l + j, d, v5);
+                        derivs5(v5, ih, U[d][0][l], U[d][1][l]);
+                    }
+                }
+            }
+    #pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                T hs = 0, vis = 0;
+    #pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T gp = (d == 0) ? Q[d][0][0] : ((d == 1) ? Q[d][0][1] : Q[d][0][2]);
+                    T gm = (d == 0) ? Q[d][1][0] : ((d == 1) ? Q[d][1][1] : Q[d][1][2]);
+                    hs += gp * U[d][0][i] + gm * U[d][1][i];
+                    vis += (U[d][0][i] - U[d][1][i]) * coef[d];
+                }
+                if (i < ND) {
+    #pragma unroll
+                    for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) hs -= Q[i % ND][s][l] * U[i % ND][s][l];
+                }
+                T r = -hs * inv_abc + vis;
+                if (j == 0) { if (i == 0) rhs[0] = r; else if (i == 1) rhs[3] = r; else rhs[6] = r; }
+                else if (j == 1) { if (i == 0) rhs[1] = r; else if (i == 1) rhs[4] = r; else rhs[7] = r; }
+                else { if (i == 0) rhs[2] = r; else if (i == 1) rhs[5] = r; else rhs[8] = r; }
+            }
+            if (lam_on) {
+    #pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    if (d != j) continue;
+    #pragma unroll
+                    for (int s = 0; s < 2; ++s)
+    #pragma unroll
+                        for (int l = 0; l < 3; ++l) Jp -= Q[d][s][l] * U[d][s][l];
+                }
+            }
         }
         if (lam_on) {
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                if (d != j) continue;
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int l = 0; l < 3; ++l) Jp -= Q[d][s][l] * U[d][s][l];
-            }
+            // the trace term enters H_ii, so rhs_ii gets -J / (a_tot b_tot c_tot)
+            T J = -(T)I.Lambda / (T)3 * Jp;
+            rhs[0] -= J * inv_abc;
+            rhs[4] -= J * inv_abc;
+            rhs[8] -= J * inv_abc;
         }
-    }
-    if (lam_on) {
-        // the trace term enters H_ii, so rhs_ii gets -J / (a_tot b_tot c_tot)
-        T J = -(T)I.Lambda / (T)3 * Jp;
-        rhs[0] -= J * inv_abc;
-        rhs[4] -= J * inv_abc;
-        rhs[8] -= J * inv_abc;
     }
 
     // ---------------- outputs ----------------
@@ -664,6 +904,37 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             dst[e] = __ldg(sp0 + c * cells + (long long)yy * nX + xx);
         }
     };
+    // Patch after a TMA copy: only the box's out-of-grid cells, i.e. its columns outside
+    // [xl, xr) (all rows) and its rows outside [yl, yr) (the in-grid columns). Tiles with more
+    // than 8 such columns or 4 such rows (grids narrower than a tile) scan the whole box.
+    auto patch_box = [&](int slot, int zp) {
+        const int xl = max(0, OX - x0), xr = max(xl, min(RX, nX - x0 + OX));
+        const int yl = max(0, 2 - y0), yr = max(yl, min(RY, nY - y0 + 2));
+        const int nxo = xl + (RX - xr), nyo = yl + (RY - yr);
+        if (nxo > 8 || nyo > 4) { load_box(slot, zp, false); return; }
+        T* dst = sm + slot * 9 * PP;
+        const T* sp0 = src + (long long)zp * plane;
+        auto put = [&](int c, int iy, int ix) {
+            int yy = y0 - 2 + iy, xx = x0 - OX + ix;
+            if (yy < 0) yy += nY;
+            if (yy >= nY) yy -= nY;
+            if (xx < 0) xx += nX;
+            if (xx >= nX) xx -= nX;
+            dst[c * PP + iy * RX + ix] = __ldg(sp0 + c * cells + (long long)yy * nX + xx);
+        };
+        if (nxo > 0) {
+            for (int e = tid; e < 9 * RY * 8; e += ST_THREADS) {
+                const int c = e / (RY * 8), r = e - c * (RY * 8), iy = r >> 3, j = r & 7;
+                if (j < nxo) put(c, iy, j < xl ? j : xr + (j - xl));
+            }
+        }
+        if (nyo > 0) {
+            for (int e = tid; e < 9 * 4 * RX; e += ST_THREADS) {
+                const int c = e / (4 * RX), r = e - c * (4 * RX), q = r / RX, ix = r - q * RX;
+                if (q < nyo && ix >= xl && ix < xr) put(c, q < yl ? q : yr + (q - yl), ix);
+            }
+        }
+    };
     // plane with relative index pr (= z - (z0 - 2)) lives in slot pr % NS
     auto issue = [&](int pr) {
         const int slot = pr % NS;
@@ -681,7 +952,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             if (tid == 0) atomicOr(status, (int)ST_TIMEOUT);
             return;
         }
-        if (edge) load_box(slot, wrapz(z0 - 2 + pr), false);
+        if (edge) patch_box(slot, wrapz(z0 - 2 + pr));
     };
 
     int issued = -1;   // highest plane index handed to TMA
