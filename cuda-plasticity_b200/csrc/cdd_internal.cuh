@@ -11,7 +11,7 @@
 namespace cdd {
 
 constexpr int MAX_STAGES = 12;
-#define CDD_MAX_TMA_INSTANCES 16
+#define CDD_MAX_TMA_MAPS 32   // stencil tensor maps per plan (one per run of same-shape instances)
 constexpr double ME = 2.220446049250313080847263336181640625e-16;   // DBL_EPSILON
 
 // Exact division by an invariant divisor d >= 1 for 0 <= n < 2^31 with one wide multiply and a
@@ -214,6 +214,7 @@ struct InstDev {
     int stencil_blocks;
     int st_zc;              // planes per stencil block along axis 0 (3-D)
     int tma_slot;           // index of this instance's tensor map, -1: threads stage the planes
+    int tma_sub;            // index of this instance in its map's run of same-shape instances
     double mu, nu, lamb, Lambda, cfl, nmax;
     double h, inv_h;        // Dx = 1 / shape[-1] (CentralUpwindHJ3D.py L15-16)
     double inv_cells;
@@ -807,7 +808,7 @@ struct PlanCore {
 // Tensor maps of one stage-input buffer for the TMA-staged instances (see stencil.cu).
 struct StencilMapSet {
     int enabled = 0;
-    CUtensorMap m[CDD_MAX_TMA_INSTANCES];
+    CUtensorMap m[CDD_MAX_TMA_MAPS];
 };
 
 // stress.cu
@@ -830,7 +831,7 @@ cudaError_t launch_flux_vjp(const PlanCore& P, const void* beta, double t, const
 enum StencilMode { M_FLUX = 0, M_STAGE1 = 1, M_STAGE2 = 2, M_STAGE3 = 3 };
 cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const void* bn, void* out,
                            void* speed, double t_flux, const StencilMapSet& maps, cudaStream_t st);
-// Encode the tensor maps of buffer `base` for every instance with tma_slot >= 0; returns false
+// Encode the tensor maps of buffer `base` for every run of instances with tma_slot >= 0; returns false
 // (and leaves maps disabled) if the driver entry point is missing or an address is misaligned.
 bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* base, StencilMapSet& maps);
 bool stencil_tma_eligible(const InstDev& I, int precision);

@@ -253,8 +253,18 @@ int build_shapes(cdd_plan* p, size_t elt) {
         p->tune[i].mid_cols = (I.nd == 3) ? I.tile[PASS_MID_F].lines : 0;
         p->tune[i].green_cols = I.tile[PASS_GREEN].lines;
         p->tune[i].stencil_planes = (I.nd == 3) ? I.st_zc : 0;
+        // consecutive instances of one shape (contiguous in every field) share one 5-D tensor map
         I.tma_slot = -1;
-        if (stencil_tma_eligible(I, C.precision) && n_tma < CDD_MAX_TMA_INSTANCES) I.tma_slot = n_tma++;
+        I.tma_sub = 0;
+        if (stencil_tma_eligible(I, C.precision)) {
+            const InstDev* Q = (i > 0) ? &p->inst[i - 1] : nullptr;
+            if (Q && Q->tma_slot >= 0 && Q->nd == I.nd && Q->n0 == I.n0 && Q->n1 == I.n1 && Q->n2 == I.n2) {
+                I.tma_slot = Q->tma_slot;
+                I.tma_sub = Q->tma_sub + 1;
+            } else if (n_tma < CDD_MAX_TMA_MAPS) {
+                I.tma_slot = n_tma++;
+            }
+        }
         pre_st.push_back(pre_st.back() + I.stencil_blocks);
         pre_ob.push_back(pre_ob.back() + (int)((I.cells + 255) / 256));
         pre_cw.push_back(pre_cw.back() + (int)((9 * I.cells + 1023) / 1024));

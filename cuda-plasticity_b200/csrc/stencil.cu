@@ -117,12 +117,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     }
     return false;
 }
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
-                                            int z, int c) {
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                            int z, int c, int n) {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(smem_addr(bar))
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(n), "r"(smem_addr(bar))
         : "memory");
 }
 
@@ -852,7 +852,8 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
 
 // One block: a TXS x TYS tile of planes [z0, z0 + zc) (3-D) or of the single plane (2-D).
 // The 3-D ring holds planes z-2 .. z+2 of all 9 components of beta_s (NS slots). With TMA
-// (I.tma_slot >= 0) one 4-D bulk-tensor copy stages a whole plane box; coordinates outside the
+// (I.tma_slot >= 0) one 5-D bulk-tensor copy stages a whole plane box (2-D: the one plane) from
+// the tensor map of the instance's run of same-shape instances; coordinates outside the
 // grid read zeros, and tiles whose box crosses the periodic boundary patch those cells with
 // wrapped loads after the copy lands. FP32 (6 slots) prefetches plane z+3 while computing z;
 // FP64 (5 slots) refills the slot of z-2 after computing z. Otherwise threads load the box.
@@ -877,13 +878,19 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     const int z0 = b * I.st_zc;
     const int z1 = min(z0 + I.st_zc, nZ);
     const int tid = threadIdx.x, tx = tid % TXS, ty = tid / TXS;
-    const int x0 = bx * TXS, y0 = by * TYS;
+    // the tile's own cells start at (x0n, y0n); a last, partial tile is shifted back inside the
+    // grid (it recomputes cells of its neighbour without storing them), so that its box leaves the
+    // grid by the halo only (x0 stays a multiple of 4 when nX is: the TMA origin x0 - OX is aligned)
+    const int x0n = bx * TXS, y0n = by * TYS;
+    const int x0 = (x0n + TXS > nX && nX >= TXS) ? nX - TXS : x0n;
+    const int y0 = (y0n + TYS > nY && nY >= TYS) ? nY - TYS : y0n;
     const int x = x0 + tx, y = y0 + ty;
     const bool vxy = (x < nX) && (y < nY);
+    const bool own = vxy && x >= x0n && y >= y0n;
     const long long cells = I.cells;
     const long long plane = (long long)nY * nX;
     const T* src = bs + I.foff;
-    const bool use_tma = (ND == 3) && maps.enabled && (I.tma_slot >= 0);
+    const bool use_tma = maps.enabled && (I.tma_slot >= 0);
     const bool edge = (x0 - OX < 0) || (x0 - OX + RX > nX) || (y0 - 2 < 0) || (y0 - 2 + RY > nY);
 
     auto wrapz = [&](int z) { while (z < 0) z += nZ; while (z >= nZ) z -= nZ; return z; };
@@ -939,8 +946,8 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     auto issue = [&](int pr) {
         const int slot = pr % NS;
         mbar_expect_tx(&bars[slot], PLANE_BYTES);
-        tma_load_4d(sm + slot * 9 * PP, &maps.m[I.tma_slot], &bars[slot], x0 - OX, y0 - 2,
-                    wrapz(z0 - 2 + pr), 0);
+        tma_load_5d(sm + slot * 9 * PP, &maps.m[I.tma_slot], &bars[slot], x0 - OX, y0 - 2,
+                    wrapz(z0 - 2 + pr), 0, I.tma_sub);
     };
     int ok = 1;
     auto arrive = [&](int pr) {   // wait for plane pr and patch it; block-uniform result in ok
@@ -963,11 +970,12 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
             fence_mbar_init();
         }
         __syncthreads();
+        constexpr int NPL = (ND == 3) ? 5 : 1;   // planes z0-2 .. z0+2 (3-D), the plane (2-D)
         if (tid == 0)
-            for (int pr = 0; pr < 5; ++pr) issue(pr);
-        issued = 4;
+            for (int pr = 0; pr < NPL; ++pr) issue(pr);
+        issued = NPL - 1;
 #pragma unroll 1
-        for (int pr = 0; pr < 5; ++pr) arrive(pr);
+        for (int pr = 0; pr < NPL; ++pr) arrive(pr);
     } else if (ND == 3) {
 #pragma unroll 1
         for (int q = 0; q < 5; ++q) load_box(q, wrapz(z0 - 2 + q), true);
@@ -1021,7 +1029,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         } else {
             tv.so[2] = 0;
         }
-        stencil_cell<T, ND, MODE, VAR>(I, cx, vxy, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac);
+        stencil_cell<T, ND, MODE, VAR>(I, cx, own, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac);
         cx.sig += plane;
         if (cx.bn) cx.bn += plane;
         cx.out += plane;
@@ -1292,10 +1300,11 @@ cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const vo
 }
 
 bool stencil_tma_eligible(const InstDev& I, int precision) {
-    if (I.nd != 3) return false;
     const int RX = precision == CDD_F32 ? TileGeom<float>::RX : TileGeom<double>::RX;
-    if (I.n2 < RX || I.n1 < RY) return false;
-    if (precision == CDD_F32 && I.n2 % 4) return false;
+    const int nX = (I.nd == 3) ? I.n2 : I.n1, nY = (I.nd == 3) ? I.n1 : I.n0;
+    if (nX < RX || nY < RY) return false;
+    if (precision == CDD_F32 && nX % 4) return false;   // 16-byte row strides
+    if (precision != CDD_F32 && nX % 2) return false;
     return true;
 }
 
@@ -1313,8 +1322,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// 4-D map per instance: (x = last axis, y, z = axis 0, component); box = one staged plane of all
-// 9 components, RX x RY cells; out-of-grid coordinates read zeros (patched by the kernel).
+// 5-D map per run of consecutive same-shape instances: (x = last axis, y, z = axis 0 (3-D), component,
+// instance of the run); box = one staged plane of all 9 components of one instance, RX x RY cells;
+// out-of-grid coordinates read zeros (patched by the kernel).
 bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* base, StencilMapSet& maps) {
     maps.enabled = 0;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1325,16 +1335,20 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
     bool any = false;
     for (int i = 0; i < P.n_inst; ++i) {
         const InstDev& I = insts[i];
-        if (I.tma_slot < 0) continue;
+        if (I.tma_slot < 0 || I.tma_sub != 0) continue;
+        int run = 1;
+        while (i + run < P.n_inst && insts[i + run].tma_slot == I.tma_slot) ++run;
         const char* addr = (const char*)base + (size_t)I.foff * elt;
         if (((uintptr_t)addr) % 16) return false;
-        cuuint64_t dims[4] = {(cuuint64_t)I.n2, (cuuint64_t)I.n1, (cuuint64_t)I.n0, 9};
-        cuuint64_t strides[3] = {(cuuint64_t)I.n2 * elt, (cuuint64_t)I.n2 * I.n1 * elt,
-                                 (cuuint64_t)I.cells * elt};
-        cuuint32_t box[4] = {RX, (cuuint32_t)RY, 1, 9};
-        cuuint32_t estr[4] = {1, 1, 1, 1};
+        // 2-D: (x = axis 1, y = axis 0, z of size 1)
+        const cuuint64_t nX = (I.nd == 3) ? I.n2 : I.n1, nY = (I.nd == 3) ? I.n1 : I.n0;
+        const cuuint64_t nZ = (I.nd == 3) ? I.n0 : 1;
+        cuuint64_t dims[5] = {nX, nY, nZ, 9, (cuuint64_t)run};
+        cuuint64_t strides[4] = {nX * elt, nX * nY * elt, (cuuint64_t)I.cells * elt, (cuuint64_t)9 * I.cells * elt};
+        cuuint32_t box[5] = {RX, (cuuint32_t)RY, 1, 9, 1};
+        cuuint32_t estr[5] = {1, 1, 1, 1, 1};
         CUresult r = enc(&maps.m[I.tma_slot], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                         4, (void*)addr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         5, (void*)addr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return false;

@@ -242,9 +242,12 @@ def test_fp32_form_error_against_fp64():
     assert abs(m32[0] - m64[0]) <= 1e-6 * max(abs(m64[0]), 1e-3)
 
 
-@pytest.mark.parametrize("shape,load", [((12, 40, 72), None), ((10, 24, 64), (-0.025, -0.025, 0.05))])
+@pytest.mark.parametrize("shape,load", [((12, 40, 72), None), ((10, 24, 64), (-0.025, -0.025, 0.05)),
+                                        ((8, 18, 48), (-0.025, -0.025, 0.05)), ((18, 48), None),
+                                        ((40, 64), (-0.025, -0.025, 0.05))])
 def test_tma_staged_planes_against_oracle(shape, load):
-    """3-D grids wide enough for the TMA plane path (x >= 40): edge tiles in x and y, FP64."""
+    """Grids wide enough for the TMA plane path (x >= 40), 3-D and 2-D: edge tiles in x and y,
+    partial last tiles (x 72 and 48, y 18: shifted back inside the grid), FP64."""
     b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 31)
     p = O.Params(mu=1.0, nu=0.3, load_rate=load)
     plan = cdd.Plan([cdd.Instance(shape, load_rate=load)], "f64")
@@ -287,6 +290,28 @@ def test_tma_fp32_matches_fp64_and_batch_mixes_paths():
         assert torch.equal(single.field_view(bs, 0), p64.field_view(b64, i))
     p64.check_status()
     p32.check_status()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_same_shape_runs_share_tensor_maps_and_overflow_to_thread_staging(prec):
+    """Runs of consecutive same-shape instances share one 5-D tensor map (instance = 5th
+    coordinate); past the plan's map budget (32 runs) instances fall back to thread-staged planes.
+    Every instance equals its single-instance plan bitwise."""
+    a, b = (4, 8, 40), (6, 8, 48)
+    shapes = [a, a, a, b, a, a] + [a if k % 2 == 0 else b for k in range(34)]
+    fields = [cdd.gaussian_random_field(s, 0.08, 0.05, 300 + i) for i, s in enumerate(shapes)]
+    insts = [cdd.Instance(s, load_rate=(-0.025, -0.025, 0.05)) for s in shapes]
+    batch = cdd.Plan(insts, prec)
+    bb = batch.pack(fields)
+    batch.set_time(0.0, 1e30)
+    batch.run(bb, 2, graph=False)
+    batch.check_status()
+    for i in [0, 1, 2, 3, 4, 5, 6, 7, 36, 37, 38, 39]:
+        single = cdd.Plan([insts[i]], prec)
+        bs = single.pack([fields[i]])
+        single.set_time(0.0, 1e30)
+        single.run(bs, 2, graph=False)
+        assert torch.equal(batch.field_view(bb, i), single.field_view(bs, 0)), i
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
