@@ -29,11 +29,11 @@ UNIT = "cell-stage updates/s"
 WORDS_PER_CELL_STAGE = 48      # stress operator: read 9 + write 6; stencil + stage: read 24, write 9
 STRESS_WORDS = 15               # stress operator: read beta 9, write sigma 6
 FLUX_WORDS = 24                 # stencil, flux form: read beta 9 + sigma 6, write rhs 9
-FLUX_TRAFFIC_BYTES_PER_CELL = 117.1   # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
-# executed FP32 operations (add + mul + 2 fma) and thread instructions per cell of the FP32 flux-form
-# stencil, from ncu's instruction counters at 192^3
-FLUX_FLOP_PER_CELL = 1312.4
-FLUX_INST_PER_CELL = 1967.0
+FLUX_TRAFFIC_BYTES_PER_CELL = 93.2    # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
+# executed FP32 operations (add + mul + 2 fma, packed pairs counted per lane) and warp instructions
+# per cell of the FP32 flux-form stencil, from ncu's instruction counters at 192^3
+FLUX_FLOP_PER_CELL = 1176.2
+FLUX_WARP_INST_PER_CELL = 44.06
 FLUX_COUNTS_SOURCE = "profiles/k_stencil_flux_flops_192cube.md"
 
 
@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--only-flux", nargs="?", const="f32", default=None, choices=["f32", "f64"],
                     help="run three flux evaluations of the workload at the given precision and exit "
                          "(for profiling the stencil)")
+    ap.add_argument("--only-vjp", action="store_true",
+                    help="run three FP32 flux VJPs (cdd_flux_vjp) of the workload and exit (for profiling "
+                         "the adjoint kernels)")
     return ap.parse_args()
 
 
@@ -356,6 +359,23 @@ def main():
         barrier()
         return ev0.elapsed_time(ev1) / 1e3
 
+    if args.only_vjp:
+        import ctypes
+        p = cdd.Plan([inst], "f32")
+        b = p.empty_field()
+        b.copy_(b0.reshape(-1).to(p.dtype))
+        g = torch.randn(p.field_elems, dtype=p.dtype, device=dev, generator=torch.Generator(dev).manual_seed(3))
+        bb, sb = torch.zeros_like(g), p.empty_stress()
+        for _ in range(3):
+            rc = p.lib.cdd_flux_vjp(p.handle, ctypes.c_void_p(b.data_ptr()), 0.0, ctypes.c_void_p(g.data_ptr()),
+                                    ctypes.c_void_p(bb.data_ptr()), ctypes.c_void_p(sb.data_ptr()), None,
+                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+            if rc != 0:
+                raise RuntimeError("cdd_flux_vjp failed: %d" % rc)
+        torch.cuda.synchronize()
+        print(json.dumps({"only_vjp": "f32", "grid": list(shape)}))
+        return
+
     if args.only_flux:
         p = cdd.Plan([inst], args.only_flux, tuning=None if args.no_tune else "auto")
         b = p.empty_field()
@@ -483,7 +503,7 @@ def main():
     fp32_peak = gemm_peak_tflops(dev, torch.float32)
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     issue_peak = nsm * 4 * (clk.get("sm_mhz") or 1965.0) * 1e6 / 1e9   # warp instructions per ns
-    issue_ach = FLUX_INST_PER_CELL / 32 * cells / t_stencil / 1e9
+    issue_ach = FLUX_WARP_INST_PER_CELL * cells / t_stencil / 1e9
     stage_s = el32 / K / 3
     achieved = WORDS_PER_CELL_STAGE * 4 * cells / stage_s / 1e9
     launches_per_step = 3 * 6 + 3 + 2
@@ -507,13 +527,13 @@ def main():
                      "launch_ms": 1e3 * t_stencil,
                      "algorithmic_bytes_per_launch": FLUX_WORDS * 4 * cells,
                      "traffic": FLUX_TRAFFIC_BYTES_PER_CELL * cells,
-                     "traffic_source": "profiles/k_stencil_flux_192cube_fp32.md (117.1 B/cell at 192^3, scaled)",
+                     "traffic_source": "profiles/k_stencil_flux_192cube_fp32.md (93.2 B/cell at 192^3, scaled)",
                      "flop": {"bound": "fp32", "flop_per_cell": FLUX_FLOP_PER_CELL,
                               "achieved": FLUX_FLOP_PER_CELL * cells / t_stencil / 1e12, "peak": fp32_peak,
                               "unit": "TFLOP/s", "frac": FLUX_FLOP_PER_CELL * cells / t_stencil / 1e12 / fp32_peak,
                               "peak_kind": "measured: cuBLAS FP32 GEMM (TF32 off), 8192^3, this run",
                               "counts_source": FLUX_COUNTS_SOURCE},
-                     "issue": {"thread_inst_per_cell": FLUX_INST_PER_CELL, "achieved_ginst_s": issue_ach,
+                     "issue": {"warp_inst_per_cell": FLUX_WARP_INST_PER_CELL, "achieved_ginst_s": issue_ach,
                                "peak_ginst_s": issue_peak, "frac": issue_ach / issue_peak,
                                "peak_kind": "4 warp instructions per cycle per SM at the median SM clock of the run"},
                      "step": {"achieved": achieved, "frac": achieved / peak,

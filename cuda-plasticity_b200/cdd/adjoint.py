@@ -58,9 +58,10 @@ class Rollout:
     shape, mu, nu: grid and material; rate_zz: r of the traceless applied strain rate
     r (-1/2, -1/2, 1) (None: no load); dt: fixed step; precision "f64" or "f32"; tuning: launch
     shapes as for ``cdd.Plan`` (None, [dict] or "auto").
-    The forward keeps a copy of the state every ``checkpoint_every`` steps; the reverse sweep
-    re-runs each segment from its checkpoint with cdd_step_record (saving stage states, stresses
-    and k-space data) and walks it backwards with cdd_step_adjoint. Nothing synchronises the host
+    The forward keeps a copy of the state every ``checkpoint_every`` steps and runs the last
+    segment with cdd_step_record (saving stage states, stresses and k-space data); the reverse
+    sweep walks that segment backwards with cdd_step_adjoint straight away and re-runs each earlier
+    segment from its checkpoint with records before walking it back. Nothing synchronises the host
     until the parameter cotangents are read at the end.
     """
 
@@ -81,6 +82,7 @@ class Rollout:
         self.checkpoints = {}
         self.rec_elems = int(self.lib.cdd_plan_record_elems(self.plan.handle))
         self._records = None
+        self._tail = None   # start of the segment whose records the last forward left in the buffer
 
     def time(self, n):
         return self.t0 + n * self.dt
@@ -94,10 +96,14 @@ class Rollout:
         p = self.plan
         u = beta0.detach().clone()
         self.checkpoints = {}
+        tail = ((self.n_steps - 1) // self.K) * self.K
+        recs = self._record_buffer(self.K)
+        self._tail = None
         for n in range(self.n_steps):
             if n % self.K == 0:
                 self.checkpoints[n] = u.clone()
-            self._step(u, n)
+            self._step(u, n, recs[n - tail] if n >= tail else None)
+        self._tail = tail
         self.uN = u
         s6 = p.stress_view(p.stress(u), 0)
         loss = energy_of_stress(s6, self.mu, self.nu) + self.w_zz * p.field_view(u, 0)[8].double().mean()
@@ -111,6 +117,7 @@ class Rollout:
         p = self.plan
         out = torch.empty((3 * self.n_steps, 4 * self.cells), dtype=torch.int32, device=p.device)
         rec = self._record_buffer(1)[0]
+        self._tail = None   # the forward's records of its last segment are overwritten
         u = beta0.detach().clone()
         for n in range(self.n_steps):
             self._step(u, n, rec)
@@ -161,9 +168,11 @@ class Rollout:
         recs = self._record_buffer(self.K)
         for s0 in sorted(self.checkpoints, reverse=True):
             s1 = min(s0 + self.K, self.n_steps)
-            v = self.checkpoints[s0].clone()
-            for n in range(s0, s1):
-                self._step(v, n, recs[n - s0])
+            if s0 != self._tail:
+                v = self.checkpoints[s0].clone()
+                for n in range(s0, s1):
+                    self._step(v, n, recs[n - s0])
+            self._tail = None
             for n in range(s1 - 1, s0 - 1, -1):
                 check(self.lib.cdd_step_adjoint(p.handle, _ptr(recs[n - s0]), self.time(n), self.dt, _ptr(ub),
                                                 _ptr(pbar), _stream()))

@@ -612,26 +612,38 @@ __device__ __forceinline__ void gather_cell(const InstDev& I, long long y, const
     const T ih = (T)I.inv_h;
     const T* ub = ubar + 54 * I.coff + y;
     const uint32_t* fl = flags + 4 * I.coff + y;
-#pragma unroll 1
-    for (int c = 0; c < 9; ++c) {
-        T acc = 0;
+    // neighbour-major: the four selection words of each of the 5 ND neighbours are read once; a
+    // one-sided derivative at distance q = -2 (forward) or q = +2 (backward) does not involve y
+    // (coef_p(-2, .) = coef_m(2, .) = 0), so those values are not read
+    T acc[9];
 #pragma unroll
-        for (int d = 0; d < ND; ++d) {
-            // cell x = y - q holds y at offset q
-            const long long off[5] = {nb[d].p2, nb[d].p1, 0, nb[d].m1, nb[d].m2};   // q = -2 .. 2
-            const int slot = c * 3 + d;
+    for (int c = 0; c < 9; ++c) acc[c] = 0;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                const int q = k - 2;
-                const long long x = off[k];
-                const uint32_t f = (fl[x + (long long)(slot >> 3) * cells] >> (4 * (slot & 7))) & 15u;
-                const T up = ub[x + (long long)((2 * d + 0) * 9 + c) * cells];
-                const T um = ub[x + (long long)((2 * d + 1) * 9 + c) * cells];
-                acc += up * (T)coef_p(q, (int)(f & 3u)) + um * (T)coef_m(q, (int)(f >> 2));
+    for (int d = 0; d < ND; ++d) {
+        // cell x = y - q holds y at offset q
+        const long long off[5] = {nb[d].p2, nb[d].p1, 0, nb[d].m1, nb[d].m2};   // q = -2 .. 2
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const int q = k - 2;
+            const long long x = off[k];
+            uint32_t fw[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) fw[w] = fl[x + (long long)w * cells];
+            const T* up = ub + x + (long long)(2 * d * 9) * cells;
+            const T* um = up + 9 * cells;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                const int slot = c * 3 + d;
+                const uint32_t f = (fw[slot >> 3] >> (4 * (slot & 7))) & 15u;
+                if (q > -2) acc[c] += up[(long long)c * cells] * (T)coef_p(q, (int)(f & 3u));
+                if (q < 2) acc[c] += um[(long long)c * cells] * (T)coef_m(q, (int)(f >> 2));
             }
         }
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
         const long long o = I.foff + (long long)c * cells + y;
-        T v = acc * ih;
+        T v = acc[c] * ih;
         if (addend) v += addend[o];
         v *= ax.c;
 #pragma unroll
