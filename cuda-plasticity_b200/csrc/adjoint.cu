@@ -35,19 +35,32 @@ __device__ __forceinline__ Nbr make_nbr(int i, int n, long long stride) {
     return r;
 }
 
+// Grid coordinates of cell cl of a 3-D (n0, n1, n2) or 2-D (n0, n1) grid; cells < 2^31, so the
+// divisions are 32-bit.
+__device__ __forceinline__ void cell_coords(long long cl, int nd, int n1, int n2, int& i0, int& i1, int& i2) {
+    const unsigned c = (unsigned)cl;
+    const unsigned nx = (unsigned)(nd == 3 ? n2 : n1);
+    const unsigned r = c / nx;
+    i2 = (int)(c - r * nx);
+    if (nd == 3) {
+        i0 = (int)(r / (unsigned)n1);
+        i1 = (int)(r - (unsigned)i0 * (unsigned)n1);
+    } else {
+        i0 = (int)r;
+        i1 = i2;
+    }
+}
+
 __device__ __forceinline__ float inv_sqrt_a(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double inv_sqrt_a(double x) { return 1.0 / sqrt(x); }
 
 // minmod of two values and which one it returned (1: a, 2: c, 0: neither)
 template <typename T>
 __device__ __forceinline__ T mm_sel(T a, T c, int& sel) {
-    if ((a > (T)0 && c > (T)0) || (a < (T)0 && c < (T)0)) {
-        if (fabs(a) <= fabs(c)) { sel = 1; return a; }
-        sel = 2;
-        return c;
-    }
-    sel = 0;
-    return (T)0;
+    const bool same = (a > (T)0 && c > (T)0) || (a < (T)0 && c < (T)0);
+    const bool pa = fabs(a) <= fabs(c);
+    sel = same ? (pa ? 1 : 2) : 0;
+    return same ? (pa ? a : c) : (T)0;
 }
 
 template <typename T>
@@ -85,19 +98,17 @@ __device__ __forceinline__ void vjp_cell(const InstDev& I, long long cl, bool va
                                          T* __restrict__ sigbar, double* lsum) {
     const long long cells = I.cells;
     Nbr nb[ND];
-    if (ND == 3) {
-        int i2 = (int)(cl % I.n2);
-        long long r = cl / I.n2;
-        int i1 = (int)(r % I.n1);
-        int i0 = (int)(r / I.n1);
-        nb[0] = make_nbr(i0, I.n0, (long long)I.n1 * I.n2);
-        nb[1] = make_nbr(i1, I.n1, I.n2);
-        nb[ND - 1] = make_nbr(i2, I.n2, 1);
-    } else {
-        int i1 = (int)(cl % I.n1);
-        int i0 = (int)(cl / I.n1);
-        nb[0] = make_nbr(i0, I.n0, I.n1);
-        nb[ND - 1] = make_nbr(i1, I.n1, 1);
+    {
+        int i0, i1, i2;
+        cell_coords(cl, ND, I.n1, I.n2, i0, i1, i2);
+        if (ND == 3) {
+            nb[0] = make_nbr(i0, I.n0, (long long)I.n1 * I.n2);
+            nb[1] = make_nbr(i1, I.n1, I.n2);
+            nb[ND - 1] = make_nbr(i2, I.n2, 1);
+        } else {
+            nb[0] = make_nbr(i0, I.n0, I.n1);
+            nb[ND - 1] = make_nbr(i1, I.n1, 1);
+        }
     }
     const T ih = (T)I.inv_h;
     const T* u = beta + I.foff + cl;
@@ -595,19 +606,17 @@ __device__ __forceinline__ void gather_cell(const InstDev& I, long long y, const
                                             const Axpy<T>& ax, T* out) {
     const long long cells = I.cells;
     Nbr nb[ND];
-    if (ND == 3) {
-        int i2 = (int)(y % I.n2);
-        long long r = y / I.n2;
-        int i1 = (int)(r % I.n1);
-        int i0 = (int)(r / I.n1);
-        nb[0] = make_nbr(i0, I.n0, (long long)I.n1 * I.n2);
-        nb[1] = make_nbr(i1, I.n1, I.n2);
-        nb[ND - 1] = make_nbr(i2, I.n2, 1);
-    } else {
-        int i1 = (int)(y % I.n1);
-        int i0 = (int)(y / I.n1);
-        nb[0] = make_nbr(i0, I.n0, I.n1);
-        nb[ND - 1] = make_nbr(i1, I.n1, 1);
+    {
+        int i0, i1, i2;
+        cell_coords(y, ND, I.n1, I.n2, i0, i1, i2);
+        if (ND == 3) {
+            nb[0] = make_nbr(i0, I.n0, (long long)I.n1 * I.n2);
+            nb[1] = make_nbr(i1, I.n1, I.n2);
+            nb[ND - 1] = make_nbr(i2, I.n2, 1);
+        } else {
+            nb[0] = make_nbr(i0, I.n0, I.n1);
+            nb[ND - 1] = make_nbr(i1, I.n1, 1);
+        }
     }
     const T ih = (T)I.inv_h;
     const T* ub = ubar + 54 * I.coff + y;
