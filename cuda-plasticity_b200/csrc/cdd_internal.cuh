@@ -246,6 +246,12 @@ template <> struct VecOf<double> { typedef double2 type; };
 
 template <typename V> __device__ __forceinline__ V vadd(V a, V b) { V r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
 template <typename V> __device__ __forceinline__ V vsub(V a, V b) { V r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+// FP32 complex add / subtract as one packed instruction (each lane rounded as the scalar operation;
+// a + (-1) b is a - b exactly rounded once)
+template <> __device__ __forceinline__ float2 vadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 vsub<float2>(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
 template <typename V> __device__ __forceinline__ V vmul(V a, V b) {
     V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
 }
