@@ -1147,11 +1147,37 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
     if (!clk[ii].active) return;
     const T dt = (T)clk[ii].dt;
     const long long n = 9 * I.cells;
-    const long long i0 = (long long)(blockIdx.x - pre[ii]) * blockDim.x * 4 + threadIdx.x;
+    const long long b0 = (long long)(blockIdx.x - pre[ii]) * blockDim.x * 4;   // 4 elements per thread
+    const T* uu = u + I.foff;
+    T* ff = f0 + I.foff;
+    if (blockDim.x == 256 && b0 + 1024 <= n && ((((uintptr_t)uu) | ((uintptr_t)ff)) & 15) == 0) {
+        // 16-byte vectors: one float4 (FP32) or two double2 (FP64) per thread
+        if constexpr (sizeof(T) == 4) {
+            const long long i = b0 + 4 * threadIdx.x;
+            const float4 a = *reinterpret_cast<const float4*>(uu + i);
+            float4 r = *reinterpret_cast<const float4*>(ff + i);
+            r.x = a.x + dt * r.x;
+            r.y = a.y + dt * r.y;
+            r.z = a.z + dt * r.z;
+            r.w = a.w + dt * r.w;
+            *reinterpret_cast<float4*>(ff + i) = r;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const long long i = b0 + 512 * k + 2 * threadIdx.x;
+                const double2 a = *reinterpret_cast<const double2*>(uu + i);
+                double2 r = *reinterpret_cast<const double2*>(ff + i);
+                r.x = a.x + dt * r.x;
+                r.y = a.y + dt * r.y;
+                *reinterpret_cast<double2*>(ff + i) = r;
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        long long i = i0 + (long long)k * blockDim.x;
-        if (i < n) f0[I.foff + i] = u[I.foff + i] + dt * f0[I.foff + i];
+        long long i = b0 + threadIdx.x + (long long)k * blockDim.x;
+        if (i < n) ff[i] = uu[i] + dt * ff[i];
     }
 }
 
