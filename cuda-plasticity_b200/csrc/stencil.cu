@@ -424,6 +424,7 @@ __device__ __forceinline__ void applied_load(const InstDev& I, double t, double*
 struct StageConst {
     double ld[3];
     double dt;
+    double cnu;   // nu / (1 + nu) of the elastic energy density (|sigma|^2 - cnu tr^2) / (4 mu)
     bool active;
 };
 
@@ -435,6 +436,7 @@ __device__ __forceinline__ StageConst stage_const(const InstDev& I, const InstCl
     const double tload = (MODE == M_FLUX) ? t_flux : ((MODE == M_STAGE1) ? ck.t : ck.t_stage);
     applied_load(I, tload, k.ld);
     k.dt = ck.dt;
+    k.cnu = I.nu / (1.0 + I.nu);
     k.active = ck.active != 0;
     return k;
 }
@@ -825,7 +827,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             double s3 = (double)sp[3 * cells], s4 = (double)sp[4 * cells], s5 = (double)sp[5 * cells];
             double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
             double tr = s0 + s3 + s5;
-            esum += (sq - I.nu / (1.0 + I.nu) * tr * tr) / (4.0 * I.mu);
+            esum += sq - kc.cnu * tr * tr;   // k_dt applies 1 / (4 mu) to the instance sum
             zsum += (double)tv.center(8);
         }
     } else if constexpr (UPD) {
@@ -1096,27 +1098,30 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
 // Per-instance time step: dt = cfl / (max(shape) * max speed), clamped to t_end
 // (FieldMover.py L94-111). Non-finite maxima raise ST_NONFINITE and skip the step.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_dt(const InstDev* __restrict__ insts,
+__global__ void __launch_bounds__(1024) k_dt(const InstDev* __restrict__ insts,
                                            const int* __restrict__ pre,
                                            const double* __restrict__ bmax,
                                            const double* __restrict__ bsum,
                                            InstClock* __restrict__ clk, double* __restrict__ obs,
                                            int* __restrict__ status, int fixed, double dt_fixed) {
-    __shared__ double red[8];
+    __shared__ double red[32];
     const int ii = blockIdx.x;
     const InstDev& I = insts[ii];
     const int b0 = pre[ii], b1 = pre[ii + 1];
     double m = 0.0, es = 0.0, zs = 0.0;
+    // one pass over the block partials, unrolled so that several loads are in flight; observable
+    // sums: fixed-order strided partial sums, then a fixed tree (deterministic)
+#pragma unroll 8
     for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
         m = fmax(m, bmax[b]);
+        es += bsum[2 * b];
+        zs += bsum[2 * b + 1];
     }
     m = block_reduce_max(m, red);
-    // observable sums: fixed-order strided partial sums, then a fixed tree (deterministic)
-    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) { es += bsum[2 * b]; zs += bsum[2 * b + 1]; }
     es = block_reduce_sum(es, red);
     zs = block_reduce_sum(zs, red);
     if (threadIdx.x == 0) {
-        obs[2 * ii] = es;
+        obs[2 * ii] = es / (4.0 * I.mu);
         obs[2 * ii + 1] = zs * I.inv_cells;
         InstClock c = clk[ii];
         c.vmax = m;
@@ -1399,7 +1404,7 @@ cudaError_t launch_set_clock(const PlanCore& P, double t, cudaStream_t st) {
 }
 
 cudaError_t launch_dt(const PlanCore& P, int fixed, double dt_fixed, cudaStream_t st) {
-    k_dt<<<P.n_inst, 256, 0, st>>>(P.d_inst, P.stencil.d_pre, P.d_bmax, P.d_bsum, P.d_clock, P.d_obs,
+    k_dt<<<P.n_inst, 1024, 0, st>>>(P.d_inst, P.stencil.d_pre, P.d_bmax, P.d_bsum, P.d_clock, P.d_obs,
                                    P.d_status, fixed, dt_fixed);
     return cudaGetLastError();
 }

@@ -112,7 +112,6 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
                                             typename VecOf<T>::type* __restrict__ dst, double* __restrict__ rowsum,
                                             long long nrows, long long npairs, int tid, int nt) {
     typedef typename VecOf<T>::type V;
-    constexpr int N = R0 * R1;
     const T half = (T)0.5;
     // stage 0 (span 1): butterfly (l, j) takes elements j + R1 r of pair line l
 #pragma unroll 1
@@ -683,6 +682,18 @@ __global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restri
 // Fused k-space pass along axis 0: forward FFT of the 9 components, Green contraction to the 6
 // stress components (scaled by 1 / cells), inverse FFT of the 6. In place on the spectrum.
 // ------------------------------------------------------------------------------------------
+// Complex value times a real scalar (plus a complex value): one packed instruction in FP32.
+template <typename V, typename T> __device__ __forceinline__ V csc(V a, T s) { a.x *= s; a.y *= s; return a; }
+template <typename V, typename T> __device__ __forceinline__ V cfma(V a, T s, V c) {
+    V r; r.x = a.x * s + c.x; r.y = a.y * s + c.y; return r;
+}
+template <> __device__ __forceinline__ float2 csc<float2, float>(float2 a, float s) {
+    return __fmul2_rn(a, make_float2(s, s));
+}
+template <> __device__ __forceinline__ float2 cfma<float2, float>(float2 a, float s, float2 c) {
+    return __ffma2_rn(a, make_float2(s, s), c);
+}
+
 template <typename T, typename V>
 __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz, bool kzero,
                                             T lam, T mu, T A, T B, T scale, bool drop_k0, V* phi_out) {
@@ -694,44 +705,29 @@ __device__ __forceinline__ void green_point(const V* b, V* out, T kx, T ky, T kz
     V p[3], q[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        p[j].x = k[0] * b[j].x + k[1] * b[3 + j].x + k[2] * b[6 + j].x;
-        p[j].y = k[0] * b[j].y + k[1] * b[3 + j].y + k[2] * b[6 + j].y;
-        q[j].x = b[3 * j].x * k[0] + b[3 * j + 1].x * k[1] + b[3 * j + 2].x * k[2];
-        q[j].y = b[3 * j].y * k[0] + b[3 * j + 1].y * k[1] + b[3 * j + 2].y * k[2];
+        p[j] = cfma(b[6 + j], k[2], cfma(b[3 + j], k[1], csc(b[j], k[0])));
+        q[j] = cfma(b[3 * j + 2], k[2], cfma(b[3 * j + 1], k[1], csc(b[3 * j], k[0])));
     }
-    V r;
-    r.x = k[0] * q[0].x + k[1] * q[1].x + k[2] * q[2].x;
-    r.y = k[0] * q[0].y + k[1] * q[1].y + k[2] * q[2].y;
-    V cc;
-    cc.x = A * s1.x * ikse - B * r.x * ikqe;
-    cc.y = A * s1.y * ikse - B * r.y * ikqe;
+    const V r = cfma(q[2], k[2], cfma(q[1], k[1], csc(q[0], k[0])));
+    const V cc = vsub(csc(s1, A * ikse), csc(r, B * ikqe));
     const T mask = kzero ? (T)0 : (T)1;
     if (phi_out) {
         // phi = s1 / kSq - r / kSqSq: g_j depends on nu only through k_j (dA s1 / kSq - dB r / kSqSq)
         // with dA = dB, so d sigma / d nu at this k point is a multiple of phi (minus the lambda term)
-        phi_out->x = mask * (s1.x * ikse - r.x * ikqe);
-        phi_out->y = mask * (s1.y * ikse - r.y * ikqe);
+        *phi_out = csc(vsub(csc(s1, ikse), csc(r, ikqe)), mask);
     }
     V g[3];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        g[j].x = mask * (k[j] * cc.x + (p[j].x + q[j].x) * ikse);
-        g[j].y = mask * (k[j] * cc.y + (p[j].y + q[j].y) * ikse);
-    }
-    V tr;
-    tr.x = k[0] * g[0].x + k[1] * g[1].x + k[2] * g[2].x - s1.x;
-    tr.y = k[0] * g[0].y + k[1] * g[1].y + k[2] * g[2].y - s1.y;
+    for (int j = 0; j < 3; ++j) g[j] = csc(cfma(vadd(p[j], q[j]), ikse, csc(cc, k[j])), mask);
+    const V tr = vsub(cfma(g[2], k[2], cfma(g[1], k[1], csc(g[0], k[0]))), s1);
     const int ia[6] = {0, 0, 0, 1, 1, 2};
     const int ja[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
     for (int o = 0; o < 6; ++o) {
         const int i = ia[o], j = ja[o];
-        V v;
-        v.x = mu * (k[i] * g[j].x + k[j] * g[i].x - b[3 * i + j].x - b[3 * j + i].x);
-        v.y = mu * (k[i] * g[j].y + k[j] * g[i].y - b[3 * i + j].y - b[3 * j + i].y);
-        if (i == j) { v.x += lam * tr.x; v.y += lam * tr.y; }
-        v.x *= scale;
-        v.y *= scale;
+        V v = csc(vsub(vsub(cfma(g[i], k[j], csc(g[j], k[i])), b[3 * i + j]), b[3 * j + i]), mu);
+        if (i == j) v = cfma(tr, lam, v);
+        v = csc(v, scale);
         if (drop_k0 && kzero) { v.x = 0; v.y = 0; }
         out[o] = v;
     }
