@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cdd.h"
@@ -325,11 +326,22 @@ template <typename V, bool INV> __device__ __forceinline__ void dft4(V* x) {
     V t0 = vadd(x[0], x[2]);
     V t1 = vsub(x[0], x[2]);
     V t2 = vadd(x[1], x[3]);
-    V t3 = vrot<V, INV>(vsub(x[1], x[3]));
-    x[0] = vadd(t0, t2);
-    x[2] = vsub(t0, t2);
-    x[1] = vadd(t1, t3);
-    x[3] = vsub(t1, t3);
+    if constexpr (std::is_same<V, float2>::value) {
+        // FP32: d = x1 - x3 formed with its halves swapped, so that t1 +- (-+i) d are one packed
+        // multiply-add each (by +-1: the same roundings as the scalar adds)
+        const float2 ds = make_float2(x[1].y - x[3].y, x[1].x - x[3].x);
+        const float2 sp = INV ? make_float2(-1.0f, 1.0f) : make_float2(1.0f, -1.0f);
+        x[0] = vadd(t0, t2);
+        x[2] = vsub(t0, t2);
+        x[1] = __ffma2_rn(ds, sp, t1);
+        x[3] = __ffma2_rn(ds, make_float2(-sp.x, -sp.y), t1);
+    } else {
+        V t3 = vrot<V, INV>(vsub(x[1], x[3]));
+        x[0] = vadd(t0, t2);
+        x[2] = vsub(t0, t2);
+        x[1] = vadd(t1, t3);
+        x[3] = vsub(t1, t3);
+    }
 }
 
 template <typename V, bool INV> __device__ __forceinline__ void dft5(V* x) {

@@ -24,6 +24,9 @@
 // adds it after the FP32 transforms (which carry a zero k = 0 mode).
 #include "cdd_internal.cuh"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace cdd {
 
 constexpr int ROW_THREADS = 256;
@@ -1142,28 +1145,35 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
 }
 
 // ------------------------------------------------------------------------------------------
-// FP32 plans: FP64 mean of each beta component from the row sums; block (instance, component),
-// fixed-order strided sums and a fixed tree, so the result is deterministic.
+// FP32 plans: FP64 mean of each beta component from the row sums. One cluster of MEAN_SPLIT blocks
+// per (instance, component): each block sums a contiguous share of the rows (fixed-order strided
+// sums and a fixed tree), block 0 of the cluster adds the shares from the blocks' shared memory
+// (distributed shared memory) in rank order, so the result is deterministic.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_mean_beta(const InstDev* __restrict__ insts,
-                                                    const double* __restrict__ rowsum,
-                                                    double* __restrict__ mean9) {
+constexpr int MEAN_SPLIT = 8;
+__global__ void __cluster_dims__(1, 1, MEAN_SPLIT) __launch_bounds__(1024)
+k_mean_beta(const InstDev* __restrict__ insts, const double* __restrict__ rowsum, double* __restrict__ mean9) {
     const InstDev& I = insts[blockIdx.x];
     const int c = blockIdx.y;
+    cg::cluster_group cl = cg::this_cluster();
+    const int part = (int)cl.block_rank();
     __shared__ double red[32];
+    __shared__ double share;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int chunk = (I.rows + MEAN_SPLIT - 1) / MEAN_SPLIT;
+    const int r0 = part * chunk, r1 = min(I.rows, r0 + chunk);
     const double* rs = rowsum + I.rsoff + (long long)c * I.rows;
     // four independent accumulators per thread keep several loads in flight; fixed order throughout
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     const int nt = blockDim.x;
-    int r = tid;
-    for (; r + 3 * nt < I.rows; r += 4 * nt) {
+    int r = r0 + tid;
+    for (; r + 3 * nt < r1; r += 4 * nt) {
         a0 += rs[r];
         a1 += rs[r + nt];
         a2 += rs[r + 2 * nt];
         a3 += rs[r + 3 * nt];
     }
-    for (; r < I.rows; r += nt) a0 += rs[r];
+    for (; r < r1; r += nt) a0 += rs[r];
     double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -1172,8 +1182,15 @@ __global__ void __launch_bounds__(1024) k_mean_beta(const InstDev* __restrict__ 
     if (tid == 0) {
         double s = 0.0;
         for (int w = 0; w < (nt >> 5); ++w) s += red[w];
+        share = s;
+    }
+    cl.sync();   // every block's share is written
+    if (part == 0 && tid == 0) {
+        double s = 0.0;
+        for (int k = 0; k < MEAN_SPLIT; ++k) s += *cl.map_shared_rank(&share, k);
         mean9[9 * blockIdx.x + c] = s * I.inv_cells;
     }
+    cl.sync();   // the shares stay in shared memory until block 0 has read them
 }
 
 
@@ -1190,7 +1207,7 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     if (f32) {
         k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM, 6);
-        k_mean_beta<<<dim3(P.n_inst, 6), 1024, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
+        k_mean_beta<<<dim3(P.n_inst, 6, MEAN_SPLIT), 1024, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, RS_SYM, 6);
