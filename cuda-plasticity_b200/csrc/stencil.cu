@@ -519,69 +519,46 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         T A[ND][2][3], Sd[ND][2], Pq[ND][2], trU[ND][2];
         constexpr int NP = (ND == 3) ? 3 : 1;
         T Cp[NP][2][2];
-    #pragma unroll
+#pragma unroll
         for (int d = 0; d < ND; ++d)
-    #pragma unroll
+#pragma unroll
             for (int s = 0; s < 2; ++s) {
                 Sd[d][s] = 0; Pq[d][s] = 0; trU[d][s] = 0;
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < 3; ++l) A[d][s][l] = 0;
             }
-    #pragma unroll
+#pragma unroll
         for (int p = 0; p < NP; ++p)
-    #pragma unroll
+#pragma unroll
             for (int a = 0; a < 2; ++a)
-    #pragma unroll
+#pragma unroll
                 for (int b = 0; b < 2; ++b) Cp[p][a][b] = 0;
 
-        // FP32 keeps all 54 one-sided derivatives in registers for pass 2; FP64 recomputes them
-        // from shared memory (register budget).
-        constexpr bool KEEPU = (sizeof(T) == 4);
-        T Ukeep[KEEPU ? ND : 1][2][9];
-        T Dv[(KEEPU || !GLIDE) ? 1 : ND][2][3];   // glide-only, FP64: (u_e)_{d e} per axis e and sign
-        if constexpr (KEEPU) {
-            // all derivatives first (shared memory only), so that the stress loads issued above have
-            // the whole derivative evaluation to arrive before the first use
-    #pragma unroll
-            for (int c = 0; c < 9; ++c)
-    #pragma unroll
-                for (int d = 0; d < ND; ++d) {
-                    T v5[5];
-                    tv.load5(c, d, v5);
-                    derivs5(v5, ih, Ukeep[d][0][c], Ukeep[d][1][c]);
-                }
-        }
-    #pragma unroll
+        // the 54 one-sided derivatives are recomputed from shared memory in each pass (register
+        // budget)
+        T Dv[GLIDE ? ND : 1][2][3];   // glide-only: (u_e)_{d e} per axis e and sign
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             T U[ND][2][3];
-            if constexpr (KEEPU) {
-    #pragma unroll
-                for (int d = 0; d < ND; ++d)
-    #pragma unroll
-                    for (int s = 0; s < 2; ++s)
-    #pragma unroll
-                        for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
-            } else {
-    #pragma unroll
-                for (int l = 0; l < 3; ++l) {
-    #pragma unroll
-                    for (int d = 0; d < ND; ++d) {
-                        T v5[5];
-                        tv.load5(3 * l + j, d, v5);
-                        derivs5(v5, ih, U[d][0][l], U[d][1][l]);
-                    }
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T v5[5];
+                    tv.load5(3 * l + j, d, v5);
+                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
                 }
             }
             T Sj[3], Sdj[3];
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < 3; ++l) { Sj[l] = (j == 0) ? S[l][0] : ((j == 1) ? S[l][1] : S[l][2]); }
-    #pragma unroll
+#pragma unroll
             for (int d = 0; d < ND; ++d) Sdj[d] = (j == 0) ? S[d][0] : ((j == 1) ? S[d][1] : S[d][2]);
-    #pragma unroll
+#pragma unroll
             for (int d = 0; d < ND; ++d)
-    #pragma unroll
+#pragma unroll
                 for (int s = 0; s < 2; ++s) {
-    #pragma unroll
+#pragma unroll
                     for (int l = 0; l < 3; ++l) {
                         T v = U[d][s][l];
                         A[d][s][l] += v * Sdj[d];
@@ -595,22 +572,22 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                     }
                     if (lam_on && j == d) {
                         // the -str (u_d)_{l d} terms
-    #pragma unroll
+#pragma unroll
                         for (int l = 0; l < 3; ++l) A[d][s][l] -= str * U[d][s][l];
                     }
                 }
-            if constexpr (!KEEPU && GLIDE) {
+            if constexpr (GLIDE) {
                 if (glide && j < ND) {
-    #pragma unroll
+#pragma unroll
                     for (int s = 0; s < 2; ++s)
-    #pragma unroll
+#pragma unroll
                         for (int l = 0; l < 3; ++l) Dv[j % ND][s][l] = U[j % ND][s][l];
                 }
             }
             // pair terms C_de[s_d][s_e] = sum_j (u_d)_ej (u_e)_dj
-    #pragma unroll
+#pragma unroll
             for (int a = 0; a < 2; ++a)
-    #pragma unroll
+#pragma unroll
                 for (int b = 0; b < 2; ++b) {
                     Cp[0][a][b] += U[0][a][1] * U[1][b][0];
                     if (ND == 3) {
@@ -619,9 +596,9 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                     }
                 }
         }
-    #pragma unroll
+#pragma unroll
         for (int d = 0; d < ND; ++d)
-    #pragma unroll
+#pragma unroll
             for (int s = 0; s < 2; ++s) {
                 T ad = (d == 0) ? A[d][s][0] : ((d == 1) ? A[d][s][1] : A[d][s][2]);
                 ad -= Sd[d][s];
@@ -632,7 +609,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         // ---------------- corners: V, speeds, weights, Q ----------------
         constexpr int NC = 1 << ND;
         T V[NC][3];
-    #pragma unroll
+#pragma unroll
         for (int c = 0; c < NC; ++c) {
             const int sx = (c >> (ND - 1)) & 1, sy = (c >> (ND - 2)) & 1;
             const int sz = (ND == 3) ? (c & 1) : 0;
@@ -644,7 +621,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                 rho2 = (T)ME + Pq[0][sx] + Pq[1][sy] - (T)2 * Cp[0][sx][sy];
             T inv = inv_sqrt(rho2);
             T av[3];
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < 3; ++l) {
                 T a = A[0][sx][l] + A[1][sy][l];
                 if (ND == 3) a += A[2 % ND][sz][l];
@@ -655,13 +632,12 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                 // g_d = tr(u_d) - sum_e (u_e)_{d e}, v += g (ME + v.g) / (ME + g.g), then v / |rho|
                 const int sgc[3] = {sx, sy, sz};
                 T gv[3];
-    #pragma unroll
+#pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     T Dd = (T)0;
-    #pragma unroll
+#pragma unroll
                     for (int e = 0; e < ND; ++e) {
-                        if constexpr (KEEPU) Dd += Ukeep[e][sgc[e]][3 * d + e];
-                        else if constexpr (GLIDE) Dd += Dv[e][sgc[e]][d];
+                        if constexpr (GLIDE) Dd += Dv[e][sgc[e]][d];
                     }
                     const T tr = (d < ND) ? trU[d % ND][sgc[d]] : (T)0;
                     gv[d] = tr - Dd;
@@ -669,66 +645,58 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                 const T rr = (T)ME + gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
                 const T rv = (T)ME + av[0] * gv[0] + av[1] * gv[1] + av[2] * gv[2];
                 const T f = fdiv(rv, rr);
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < 3; ++l) av[l] += gv[l] * f;
             }
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < 3; ++l) V[c][l] = av[l] * inv;
         }
         T pp[ND], pm[ND], tot[ND];
         T vsum = 0;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
-    #pragma unroll
+#pragma unroll
         for (int d = 0; d < ND; ++d) {
             T mx = (T)0, mn = (T)0;
-    #pragma unroll
+#pragma unroll
             for (int c = 0; c < NC; ++c) { mx = fmax(mx, V[c][d]); mn = fmin(mn, V[c][d]); vsum += V[c][d]; }
             pp[d] = mx;
             pm[d] = -mn;
             tot[d] = pp[d] + pm[d] + (T)ME;
         }
-        // FP32 normalises each axis' upwind weights by its total first (w_d / tot_d in [0, 1]): the
-        // product a_tot b_tot c_tot of a cell without gradients is ME^3, below the smallest FP32
-        // subnormal, and dividing by it would give 0 * inf. FP64 keeps the reference's order.
-        constexpr bool NORMW = (sizeof(T) == 4);
+        // the reference's order: the upwind weights a-_d, a+_d are divided by a_tot b_tot c_tot at
+        // the end (the FP32 form, flux_f32, normalises each axis first)
         T wm[ND], wp[ND];
-    #pragma unroll
+#pragma unroll
         for (int d = 0; d < ND; ++d) {
-            if constexpr (NORMW) {
-                const T it = fdiv((T)1, tot[d]);
-                wm[d] = pm[d] * it;
-                wp[d] = pp[d] * it;
-            } else {
-                wm[d] = pm[d];
-                wp[d] = pp[d];
-            }
+            wm[d] = pm[d];
+            wp[d] = pp[d];
         }
         T Q[ND][2][3];
-    #pragma unroll
+#pragma unroll
         for (int d = 0; d < ND; ++d)
-    #pragma unroll
+#pragma unroll
             for (int s = 0; s < 2; ++s)
-    #pragma unroll
+#pragma unroll
                 for (int l = 0; l < 3; ++l) Q[d][s][l] = 0;
-    #pragma unroll
+#pragma unroll
         for (int c = 0; c < NC; ++c) {
             int sg[3];
             sg[0] = (c >> (ND - 1)) & 1;
             sg[1] = (c >> (ND - 2)) & 1;
             sg[2] = (ND == 3) ? (c & 1) : 0;
             T w = (T)1;
-    #pragma unroll
+#pragma unroll
             for (int d = 0; d < ND; ++d) w *= (sg[d] == 0) ? wm[d] : wp[d];
-    #pragma unroll
+#pragma unroll
             for (int l = 0; l < 3; ++l) {
                 T wv = w * V[c][l];
-    #pragma unroll
+#pragma unroll
                 for (int d = 0; d < ND; ++d) Q[d][sg[d]][l] += wv;
             }
         }
-        const T inv_abc = NORMW ? (T)1 : fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
+        const T inv_abc = fdiv((T)1, ND == 3 ? tot[0] * tot[1] * tot[2 % ND] : tot[0] * tot[1]);
         T coef[ND];
-    #pragma unroll
-        for (int d = 0; d < ND; ++d) coef[d] = NORMW ? pm[d] * wp[d] : fdiv(pm[d] * pp[d], tot[d]);
+#pragma unroll
+        for (int d = 0; d < ND; ++d) coef[d] = fdiv(pm[d] * pp[d], tot[d]);
         spd = tot[0] + tot[1];
         if (ND == 3) spd += tot[2 % ND];
         if (vsum != vsum) spd = vsum;
@@ -736,39 +704,30 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         // ---------------- pass 2: rhs ----------------
         T Jp = 0;   // Lambda trace term, J = -Lambda/3 * Jp
         if (lam_on) {
-    #pragma unroll
+#pragma unroll
             for (int d = 0; d < ND; ++d)
-    #pragma unroll
+#pragma unroll
                 for (int s = 0; s < 2; ++s) {
                     T qdd = (d == 0) ? Q[d][s][0] : ((d == 1) ? Q[d][s][1] : Q[d][s][2]);
                     Jp += qdd * trU[d][s];
                 }
         }
-    #pragma unroll
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             T U[ND][2][3];
-            if constexpr (KEEPU) {
-    #pragma unroll
-                for (int d = 0; d < ND; ++d)
-    #pragma unroll
-                    for (int s = 0; s < 2; ++s)
-    #pragma unroll
-                        for (int l = 0; l < 3; ++l) U[d][s][l] = Ukeep[d][s][3 * l + j];
-            } else {
-    #pragma unroll
-                for (int l = 0; l < 3; ++l) {
-    #pragma unroll
-                    for (int d = 0; d < ND; ++d) {
-                        T v5[5];
-                        tv.load5(3 * l + j, d, v5);
-                        derivs5(v5, ih, U[d][0][l], U[d][1][l]);
-                    }
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T v5[5];
+                    tv.load5(3 * l + j, d, v5);
+                    derivs5(v5, ih, U[d][0][l], U[d][1][l]);
                 }
             }
-    #pragma unroll
+#pragma unroll
             for (int i = 0; i < 3; ++i) {
                 T hs = 0, vis = 0;
-    #pragma unroll
+#pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     T gp = (d == 0) ? Q[d][0][0] : ((d == 1) ? Q[d][0][1] : Q[d][0][2]);
                     T gm = (d == 0) ? Q[d][1][0] : ((d == 1) ? Q[d][1][1] : Q[d][1][2]);
@@ -776,9 +735,9 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                     vis += (U[d][0][i] - U[d][1][i]) * coef[d];
                 }
                 if (i < ND) {
-    #pragma unroll
+#pragma unroll
                     for (int s = 0; s < 2; ++s)
-    #pragma unroll
+#pragma unroll
                         for (int l = 0; l < 3; ++l) hs -= Q[i % ND][s][l] * U[i % ND][s][l];
                 }
                 T r = -hs * inv_abc + vis;
@@ -787,12 +746,12 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
                 else { if (i == 0) rhs[2] = r; else if (i == 1) rhs[5] = r; else rhs[8] = r; }
             }
             if (lam_on) {
-    #pragma unroll
+#pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     if (d != j) continue;
-    #pragma unroll
+#pragma unroll
                     for (int s = 0; s < 2; ++s)
-    #pragma unroll
+#pragma unroll
                         for (int l = 0; l < 3; ++l) Jp -= Q[d][s][l] * U[d][s][l];
                 }
             }

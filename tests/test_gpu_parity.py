@@ -379,3 +379,25 @@ def test_adjoint_rejects_glide_only():
     assert rc == _lib.CDD_ERR_UNSUPPORTED
     with pytest.raises(cdd.CDDError):
         cdd.Plan([cdd.Instance(shape, Lambda=1.0, glide_only=True)], "f64")
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_steps_are_deterministic(prec):
+    """Two runs of the same plan from the same state are bitwise equal: every reduction (speed
+    maxima, observable sums, the FP32 form's FP64 means, which one cluster of blocks per component
+    adds in rank order) has a fixed order."""
+    shapes = [(64, 64, 64), (48, 48), (16, 24, 80)]
+    fields = [cdd.gaussian_random_field(s, 0.05, 0.05, 500 + i) for i, s in enumerate(shapes)]
+    insts = [cdd.Instance(s, load_rate=(-0.025, -0.025, 0.05)) for s in shapes]
+    outs = []
+    for _ in range(2):
+        plan = cdd.Plan(insts, prec)
+        b = plan.pack(fields)
+        plan.set_time(0.0, 1e30)
+        plan.run(b, 3, graph=True)
+        e, m = plan.observables(b)
+        outs.append((b.clone(), np.asarray(e).copy(), np.asarray(m).copy(), plan.get_time()[0].copy()))
+        plan.check_status()
+    assert torch.equal(outs[0][0], outs[1][0])
+    for k in (1, 2, 3):
+        assert np.array_equal(outs[0][k], outs[1][k])
