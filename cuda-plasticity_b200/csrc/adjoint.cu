@@ -663,7 +663,7 @@ __device__ __forceinline__ void gather_cell(const InstDev& I, long long y, const
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_vjp_gather(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_vjp_gather(const InstDev* __restrict__ insts, int n_inst,
                                                     const int* __restrict__ pre, const T* __restrict__ ubar,
                                                     const uint32_t* __restrict__ flags,
                                                     const T* __restrict__ addend, const Axpy<T> ax,
