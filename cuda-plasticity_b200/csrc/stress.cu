@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_c2r_row
 // Block = (component, i0, column tile of W).
 // ------------------------------------------------------------------------------------------
 template <typename T, bool INV>
-__global__ void __launch_bounds__(ROW_THREADS) k_fft_mid(const InstDev* __restrict__ insts, int n_inst,
+__global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 2) k_fft_mid(const InstDev* __restrict__ insts, int n_inst,
                                                  const int* __restrict__ pre,
                                                  typename VecOf<T>::type* __restrict__ spec,
                                                  const typename VecOf<T>::type* __restrict__ tw,
