@@ -46,10 +46,17 @@ def parse():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=64, help="grid of the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=96,
+                    help="grid of the CPU baseline sample (one step on one core; 96^3 takes about 30 s, "
+                         "128^3 about 80 s)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
+    ap.add_argument("--precision-steps", type=int, default=200,
+                    help="steps of the FP32-vs-FP64 precision study (config 3: 200)")
+    ap.add_argument("--clocks-csv", default=os.environ.get("CDD_BENCH_CLOCKS_CSV"),
+                    help="file for the raw nvidia-smi samples of the timed region (default: none; "
+                         "the environment variable CDD_BENCH_CLOCKS_CSV may give it)")
     ap.add_argument("--only-flux", nargs="?", const="f32", default=None, choices=["f32", "f64"],
                     help="run three flux evaluations of the workload at the given precision and exit "
                          "(for profiling the stencil)")
@@ -195,11 +202,10 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu):
+    def __init__(self, gpu, path=None):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", "clocks_bench.csv") if os.path.isdir(
-            os.path.join(REPO, "gpurun_out")) else "/dev/null"
+        self.path = path or "/dev/null"   # raw samples are kept only when a path is given
         self.out = None
 
     def start(self):
@@ -283,8 +289,10 @@ def run_reference(args):
         mem_gb = psutil.virtual_memory().available / 2 ** 30
     except Exception:
         mem_gb = 16.0
-    sample = 48
-    workers = max(1, min(cores, int(mem_gb // 1.0), 64))
+    # one 64^3 grid per worker and step: a 256^3 step of the oracle takes about 10 minutes on one
+    # core (128^3: about 80 s), so the whole-job rate is sampled on independent 64^3 grids
+    sample = 64
+    workers = max(1, min(cores, int(mem_gb // 1.5), 64))
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
         for w in range(args.warmup):
@@ -331,7 +339,7 @@ def main():
     K, W = args.steps, max(3, args.warmup)
     shape, inst = workload(args.size, 100 + rank)
     cells = int(np.prod(shape))
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, args.clocks_csv)
 
     b0 = gaussian_random_field_torch(shape, 0.03, 0.05, 100 + rank, device=dev)   # FP64 on device
 
@@ -426,6 +434,7 @@ def main():
     # ---------------- FP64 plain form and FP32 error ----------------
     fp64 = None
     err = None
+    precision_study = None
     if not args.no_fp64:
         p64 = cdd.Plan([inst], "f64", tuning=tuning)
         beta64 = p64.empty_field()
@@ -436,22 +445,50 @@ def main():
         el64 = max_over_ranks(timed_run(p64, beta64, K64))
         rate64 = world * cells * 3 * K64 / el64
         fp64 = {"value": rate64, "unit": UNIT, "ms_per_step": 1e3 * el64 / K64, "steps": K64}
-        # error of the FP32 form after 10 steps from the same state
+        # config-3 precision study: the FP32 form against FP64 from the same field over
+        # --precision-steps adaptive steps (each form takes its own CFL steps); per-field rel-L2 at
+        # checkpoints, and the energy / mean-strain curves (observables after every step)
         beta64.copy_(b0.reshape(-1))
         beta32.copy_(b0.reshape(-1).to(torch.float32))
         p64.set_time(0.0, 1e30)
         p32.set_time(0.0, 1e30)
-        p64.run(beta64, 10, graph=True)
-        p32.run(beta32, 10, graph=True)
-        torch.cuda.synchronize()
-        a = beta64.view(9, -1)
-        b = beta32.view(9, -1).to(torch.float64)
-        rels = ((a - b).norm(dim=1) / a.norm(dim=1)).cpu().numpy()
+        n_prec = max(10, args.precision_steps)
+        marks = sorted({m for m in (10, 50, 100, 200, n_prec) if m <= n_prec})
         e64, m64 = p64.observables(beta64)
         e32, m32 = p32.observables(beta32)
-        err = {"per_field_rel_l2_max": float(rels.max()), "per_field_rel_l2": [float(x) for x in rels],
-               "energy_rel": float(abs(e32[0] - e64[0]) / abs(e64[0])),
-               "mean_zz_abs": float(abs(m32[0] - m64[0]))}
+        curve64, curve32 = [(e64[0], m64[0])], [(e32[0], m32[0])]
+        at_marks = {}
+        for n in range(1, n_prec + 1):
+            p64.run(beta64, 1, graph=True)
+            p32.run(beta32, 1, graph=True)
+            e64, m64 = p64.observables(beta64)
+            e32, m32 = p32.observables(beta32)
+            curve64.append((e64[0], m64[0]))
+            curve32.append((e32[0], m32[0]))
+            if n in marks:
+                a = beta64.view(9, -1)
+                b = beta32.view(9, -1).to(torch.float64)
+                rels = ((a - b).norm(dim=1) / a.norm(dim=1)).cpu().numpy()
+                at_marks[str(n)] = {"per_field_rel_l2_max": float(rels.max()),
+                                    "per_field_rel_l2": [float(x) for x in rels],
+                                    "energy_rel": float(abs(e32[0] - e64[0]) / abs(e64[0])),
+                                    "mean_zz_abs": float(abs(m32[0] - m64[0]))}
+        p64.check_status()
+        p32.check_status()
+        t64, _, _ = p64.get_time()
+        t32, _, _ = p32.get_time()
+        c64 = np.array(curve64)
+        c32 = np.array(curve32)
+        err = dict(at_marks["10"])
+        precision_study = {
+            "steps": n_prec, "grid": list(shape),
+            "per_field_rel_l2_at_step": at_marks,
+            "energy_curve_max_rel": float(np.max(np.abs(c32[:, 0] - c64[:, 0]) / np.abs(c64[:, 0]))),
+            "mean_zz_curve_max_abs": float(np.max(np.abs(c32[:, 1] - c64[:, 1]))),
+            "mean_zz_curve_max_rel": float(np.max(np.abs(c32[:, 1] - c64[:, 1])) / np.max(np.abs(c64[:, 1]))),
+            "t_final_fp64": float(t64[0]), "t_final_fp32": float(t32[0]),
+            "note": "each form takes its own CFL steps (FP64 speed maximum in both), so the curves are "
+                    "compared step by step and the times differ by the accumulated dt difference"}
         del p64, beta64
 
     # ---------------- end to end: host buffers through the public API ----------------
@@ -548,6 +585,7 @@ def main():
         "fp64_plain": fp64,
         "fp32_over_fp64": (rate32 / fp64["value"]) if fp64 else None,
         "fp32_error_10_steps": err,
+        "precision_study": precision_study,
         "adj_over_fwd": adj["value"] if adj else None,
         "adjoint": adj,
         "ensemble_96": ens,

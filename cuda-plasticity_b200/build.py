@@ -45,8 +45,16 @@ def up_to_date():
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
-def compile_one(src, verbose):
+def headers():
+    return [d for d in deps() if not d.endswith(".cu")]
+
+
+def compile_one(src, verbose, force=False):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+    if not force and not verbose and os.path.exists(obj):
+        t = os.path.getmtime(obj)
+        if all(os.path.getmtime(d) <= t for d in [src] + headers()):
+            return obj, ""
     cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
@@ -62,7 +70,7 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        results = list(ex.map(lambda s: compile_one(s, verbose), sources()))
+        results = list(ex.map(lambda s: compile_one(s, verbose, force), sources()))
     objs = [o for o, _ in results]
     if verbose:
         for _, log in results:

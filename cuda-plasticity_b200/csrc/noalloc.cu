@@ -2,9 +2,9 @@
 // cannot allocate device memory.
 //
 // Who needs it: code that runs where cudaMalloc is not allowed or not wanted -- a host framework
-// that owns all device memory through its own allocator and forbids libraries from allocating,
-// code running inside a region that is being captured into a CUDA graph (where allocation is
-// illegal), or long-running services that must not grow their memory after start-up. Such a
+// that owns all device memory through its own allocator and forbids libraries from allocating
+// behind its back, or a long-running service that must not grow its device memory after start-up
+// (an allocation there can fail late, or stall every stream while the driver maps memory). Such a
 // caller cannot create a cdd_plan (plan creation allocates its scratch), so this entry point
 // keeps its scratch in a fixed array inside the library instead.
 //
@@ -12,8 +12,11 @@
 // loads the library holds it until the process exits. Host code may not use the array's name as a
 // device address (on the host it only names a stand-in), so the first call on each device, with that
 // device current, looks the address up once with cudaGetSymbolAddress and caches it; that first
-// call should come before any stream capture. Nothing here calls cudaMalloc, cudaFree or any
-// allocating library routine.
+// call should come before any stream capture. The cached address belongs to the device's primary
+// context: after a cudaDeviceReset in the same process it is stale, as every other device pointer
+// is. Nothing here calls cudaMalloc, cudaFree or any allocating library routine. Each call copies
+// its small tables (FFT twiddles, k tables, launch description) from a host buffer of the call
+// into the front of the scratch with one cudaMemcpyAsync.
 //
 // Every call shares the one array and it keeps the last call's contents; calls that overlap on
 // the GPU (different streams or threads) race on it and must be serialised by the caller. Each
@@ -273,7 +276,9 @@ extern "C" int cdd_stress_noalloc(const cdd_instance* d, int precision, const vo
         base = g_scratch_ptr[dev];
     }
     int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess)
+        return err(CDD_ERR_CUDA, std::string("cudaDeviceGetAttribute(shared memory): ") + cudaGetErrorString(e));
     if (smem_need > (size_t)optin) return err(CDD_ERR_SHAPE, "cdd_stress_noalloc: shared memory need exceeds the device limit");
     // raise (never lower) the kernels' dynamic shared-memory limit: plans launch the same kernels
     e = stress_set_attributes(precision, (size_t)optin);

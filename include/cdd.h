@@ -253,13 +253,13 @@ int cdd_check_status(cdd_plan* plan);
 
 /* Internal stress of ONE instance, like cdd_stress, without allocating any device memory.
  * No counterpart in the reference: it exists for callers that cannot call cudaMalloc (and so
- * cannot create a plan) -- hosts that own all device memory through their own allocator, code
- * inside a region being captured into a CUDA graph, services that must not allocate after
- * start-up. The scratch (k-space spectra, FFT and k tables, FP64 row sums) is a fixed
+ * cannot create a plan) -- hosts that own all device memory through their own allocator and
+ * forbid libraries from allocating, services that must not allocate after start-up. The scratch (k-space spectra, FFT and k tables, FP64 row sums) is a fixed
  * CDD_STRESS_NOALLOC_MAX_BYTES array inside the library; a grid that needs more is rejected with
  * CDD_ERR_SHAPE and a message giving both sizes (e.g. FP64 64^3 and FP32 80^3 fit, 128^3 does
  * not). The first call on a device looks the array's device address up (once per device, with
- * that device current); make that first call before any stream capture. All calls share the
+ * that device current); make that first call before any stream capture. A cudaDeviceReset makes
+ * the looked-up address stale, like every other device pointer. All calls share the
  * array: calls that overlap on the GPU race and must be serialised by the caller. Each call
  * writes every scratch byte it reads, so nothing needs clearing between calls.
  * inst: one instance (shape, mu, nu); precision: CDD_F64 or CDD_F32; beta: 9 * cells elements

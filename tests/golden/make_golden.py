@@ -20,12 +20,20 @@ CentralUpwindHJBetaPDynamics.py (2-D, the module RunPython.py imports), and
 ``TVDRungeKutta_FieldMover.CalculateOneAdaptiveTimeStep`` -- on seeded inputs from
 ``cdd.initial.gaussian_random_field`` and writes ``*.npz`` fixtures next to this file.
 
+``initializer.npz`` holds states of the reference's GaussianRandomInitializer (``run_initializer_case``).
 ``observables.npz`` holds the field observables of PlasticityState (beta^E, rotation, Rodrigues
 vector, Nye density) of seeded fields. ``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
 LoadStateRaw run from their source text (``run_io_case``).
 
-Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only NAME]``.
-Only this script reads the reference tree; tests read the committed ``.npz`` files.
+``c2_3d_64`` and ``c2_3d_128`` are compact fixtures of 10 steps at the config-2 sizes (sigma 0.04, the
+applied strain rate diag(-0.025, -0.025, 0.05)): instead of whole fields they hold the dt sequence,
+the energy and mean-strain curves, per-component sums and sums of squares after steps 1 and 10, and
+the 9 components of 4096 seeded sample cells after steps 1 and 10 (``run_case`` with ``samples``).
+
+Usage: ``python tests/golden/make_golden.py --reference PATH [--only NAME]`` (PATH is the reference
+checkout; the environment variable CDD_REFERENCE may give it instead; CDD_REFPY_DIR may move the
+patched copy elsewhere, e.g. to run two cases at once). Only this script reads the reference tree;
+tests read the committed ``.npz`` files.
 """
 import argparse
 import os
@@ -38,7 +46,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-PATCHED = os.path.join(REPO, "oracle", "_refpy")
+PATCHED = os.environ.get("CDD_REFPY_DIR") or os.path.join(REPO, "oracle", "_refpy")
 
 MODULES = [
     "__init__.py", "Constants.py", "NumericalMethods.py", "PlasticitySystem.py",
@@ -100,7 +108,11 @@ def _import_reference():
 
 
 def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.25,
-             load_rate=None, store_fields=True, t_end=1e30, glide=False):
+             load_rate=None, store_fields=True, t_end=1e30, glide=False, samples=0):
+    """One reference run. ``samples`` > 0 makes a compact fixture: no whole
+    fields, but the 9 components of that many seeded sample cells and per-component sums and sums
+    of squares after the first and the last step, plus the initial field's sums as a check that
+    the generator reproduces it."""
     PlasticityState, GridArray, FieldMover, Dyn3, Dyn2, Glide = _import_reference()
     sys.path.insert(0, os.path.join(REPO, "cuda-plasticity_b200"))
     from cdd.initial import gaussian_random_field
@@ -144,6 +156,19 @@ def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.
     out = {"shape": np.array(shape), "sigma_f": sigma_f, "seed": seed, "mu": mu, "nu": nu,
            "Lambda": Lambda, "cfl": cfl, "glide": int(glide),
            "load_rate": np.zeros(3) if load_rate is None else np.asarray(load_rate, float)}
+    if samples:
+        rs = np.random.default_rng(10_000 + seed)
+        n_cells = int(np.prod(shape))
+        idx = np.sort(rs.choice(n_cells, size=samples, replace=False))
+        out["sample_idx"] = idx
+        out["beta0_sum"] = beta0.reshape(9, -1).sum(axis=1)
+        out["beta0_sumsq"] = (beta0.reshape(9, -1) ** 2).sum(axis=1)
+
+        def record(tag, arr):
+            flat = arr.reshape(9, -1)
+            out["sample_" + tag] = flat[:, idx].copy()
+            out["sum_" + tag] = flat.sum(axis=1)
+            out["sumsq_" + tag] = (flat ** 2).sum(axis=1)
     state = make_state(beta0)
     t0 = time.time()
     sig = state.CalculateSigma()
@@ -168,7 +193,12 @@ def run_case(name, shape, sigma_f, seed, steps, mu=1.0, nu=0.3, Lambda=0, cfl=0.
         means.append(m)
         if store_fields and n == 0:
             out["beta1"] = to_array(state)
+        if samples and n == 0:
+            record("step1", to_array(state))
+        print("  %s step %d dt=%.6e %.0fs" % (name, n + 1, dt, time.time() - t0), flush=True)
     final = to_array(state)
+    if samples:
+        record("final", final)
     if store_fields:
         out["beta_final"] = final
     out["steps"] = steps
@@ -313,6 +343,39 @@ def run_vacancy_case(name="vacancy"):
     print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
 
 
+def run_initializer_case(reference, name="initializer"):
+    """The reference's random initial condition, GaussianRandomInitializer (FieldInitializer.py
+    L153-209) with its ResizeState / ResampleArray (L421-442), run from their source text (the
+    module imports state classes that are not part of the time-step path). Names the module takes
+    from old scipy (random, sqrt, pi, exp) are numpy's, which is what those scipy names were."""
+    PlasticityState, GridArray = _import_reference()[:2]
+    sys.path.insert(0, PATCHED)
+    from Plasticity.PlasticityStates import VacancyState
+    from Plasticity.GridArray import FourierSpaceTools
+    import copy as copy_module
+    ns = {"numpy": np, "random": np.random, "fft": np.fft, "sqrt": np.sqrt, "pi": np.pi, "exp": np.exp,
+          "copy": copy_module, "PlasticityState": PlasticityState, "VacancyState": VacancyState,
+          "FourierSpaceTools": FourierSpaceTools, "GridArray": GridArray}
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "ReformatState"), ns)
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "ResampleArray"), ns)
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "ResizeState"), ns)
+    exec(_reference_function(reference, "FieldInitializers/FieldInitializer.py", "GaussianRandomInitializer"), ns)
+    out = {}
+    for key, shape, sigma, seed, vac in (("r3", (16, 16, 16), 0.2, 3, None), ("n2", (128, 128), 0.2, 5, None),
+                                         ("r2", (64, 64), 0.1, 7, None), ("v2", (16, 16), 0.2, 9, 0.5)):
+        st = ns["GaussianRandomInitializer"](shape, sigma, seed, vacancy=vac)
+        field = st.GetOrderParameterField()
+        out["shape_" + key] = np.array(shape)
+        out["sigma_" + key] = sigma
+        out["seed_" + key] = seed
+        out["vacancy_" + key] = -1.0 if vac is None else vac
+        out["components_" + key] = np.array(["".join(c) for c in field.components])
+        out["field_" + key] = np.stack([np.asarray(field[c]) for c in field.components])
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))
+
+
 CASES = {
     # one flux, one step and 10 steps of 3-D glide+climb dynamics
     "g3d_16": dict(shape=(16, 16, 16), sigma_f=0.05, seed=1, steps=10),
@@ -336,14 +399,22 @@ CASES = {
     # config-2 style curves at reduced size: 3-D 32^3, sigma 0.04, applied strain rate, 40 steps
     "c2_3d_32": dict(shape=(32, 32, 32), sigma_f=0.04, seed=12, steps=40, store_fields=False,
                      load_rate=(-0.025, -0.025, 0.05)),
+    # config-2 fields at 64^3 and 128^3 (sigma 0.04, applied strain rate), 10 steps, compact
+    "c2_3d_64": dict(shape=(64, 64, 64), sigma_f=0.04, seed=13, steps=10, store_fields=False,
+                     load_rate=(-0.025, -0.025, 0.05), samples=4096),
+    "c2_3d_128": dict(shape=(128, 128, 128), sigma_f=0.04, seed=14, steps=10, store_fields=False,
+                      load_rate=(-0.025, -0.025, 0.05), samples=4096),
 }
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("CDD_REFERENCE"),
+                    help="path of the reference checkout (or set CDD_REFERENCE)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference PATH (the reference checkout) or set CDD_REFERENCE")
     build_patched_copy(args.reference)
     if args.only in (None, "io_formats"):
         run_io_case(args.reference)
@@ -351,6 +422,8 @@ def main():
         run_observables_case()
     if args.only in (None, "vacancy"):
         run_vacancy_case()
+    if args.only in (None, "initializer"):
+        run_initializer_case(args.reference)
     for name, kw in CASES.items():
         if args.only and name != args.only:
             continue

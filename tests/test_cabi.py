@@ -107,3 +107,27 @@ def test_tuned_plan_rejects_bad_tuning_before_device_work():
         rc = lib.cdd_plan_create_tuned(ctypes.byref(inst), 1, _lib.CDD_F64, ctypes.byref(t), ctypes.byref(h))
         assert rc == _lib.CDD_ERR_ARG, bad
         assert "tuning" in lib.cdd_last_error().decode()
+
+
+def test_documented_binding_struct_matches_header(tmp_path):
+    """The ctypes cdd_instance a maintainer copies from INTEGRATION.md section 2 has every field of
+    include/cdd.h at gcc's offsets, and the same size, so the library never reads past its end."""
+    text = open(os.path.join(REPO, "INTEGRATION.md")).read()
+    block = re.search(r"^class cdd_instance\(ctypes\.Structure\):.*?\]\n", text, flags=re.M | re.S)
+    assert block, "INTEGRATION.md has no ctypes cdd_instance"
+    ns = {"ctypes": ctypes}
+    exec(block.group(0), ns)
+    S = ns["cdd_instance"]
+    names = [f[0] for f in S._fields_]
+    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct cdd_instance \{(.*?)\} cdd_instance;", hdr, flags=re.S).group(1)
+    declared = re.findall(r"(\w+)(?:\[\d+\])?\s*[,;]", body)
+    assert names == declared
+    src = tmp_path / "doc_layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(void){\n'
+                   'printf("%%zu\\n", sizeof(cdd_instance));\n%s return 0;}\n'
+                   % (HEADER, "".join('printf("%%zu\\n", offsetof(cdd_instance, %s));\n' % n for n in names)))
+    exe = tmp_path / "doc_layout"
+    subprocess.run(["gcc", "-std=c99", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert got == [ctypes.sizeof(S)] + [getattr(S, n).offset for n in names]

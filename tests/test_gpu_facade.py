@@ -121,3 +121,22 @@ def test_glide_only_system_run_matches_reference():
                                                dyn, [recall])
     system.Run(startTime=0.0, endTime=float(g["t_final"]) * (1.0 - 1e-12))
     assert rel(recall.state.betaP.stack(), g["beta_final"]) < 1e-10
+
+
+def test_runpython_style_start_from_gaussian_random_initializer():
+    """A RunPython.py-style run (L141-161, L181-186, L216-255): the state comes from
+    FieldInitializer.GaussianRandomInitializer(gridShape, lengthscale 0.2, seed) with the state
+    class's default mu = 0.5, nu = 0.3, the 'gcd' method's 2-D module dynamics (Lambda = 0) and mover
+    (CFL 0.1), and PlasticitySystem.Run over RunPython's first output interval [0, 0.01]; the result
+    equals the oracle's steps of the same initial field."""
+    from Plasticity.FieldInitializers import FieldInitializer
+    gridShape = (32, 32)
+    state = FieldInitializer.GaussianRandomInitializer(gridShape, 0.2, 3)
+    b0 = state.betaP.stack()
+    obs = Observer.RecallStateObserver()
+    system = PlasticitySystem.PlasticitySystem(gridShape, state, FieldMover.TVDRungeKutta_FieldMover(CFLsafeFactor=0.1),
+                                               CentralUpwindHJBetaPDynamics.BetaPDynamics(Lambda=0), [obs])
+    system.Run(startTime=0.0, endTime=0.01)
+    ref, t = O.run(b0, 0.0, 0.01, O.Params(mu=0.5, nu=0.3, cfl=0.1))
+    assert abs(t - 0.01) < 1e-15
+    assert rel(obs.state.betaP.stack(), ref) < 1e-10
