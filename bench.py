@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--only-flux", nargs="?", const="f32", default=None, choices=["f32", "f64"],
                     help="run three flux evaluations of the workload at the given precision and exit "
                          "(for profiling the stencil)")
+    ap.add_argument("--only-step", nargs="?", const="f32", default=None, choices=["f32", "f64"],
+                    help="run three adaptive steps of the workload (eager launches) at the given precision and "
+                         "exit (for the per-kernel launch list)")
     ap.add_argument("--only-vjp", action="store_true",
                     help="run three FP32 flux VJPs (cdd_flux_vjp) of the workload and exit (for profiling "
                          "the adjoint kernels)")
@@ -83,35 +86,39 @@ def ensemble_instances(seed):
     return out
 
 
-def run_ensemble(dev, K, W, seed, tuning):
-    """Batched FP32 ensemble through one plan: every stage is one launch per kernel over all
-    instances, per-instance dt, the whole step in a CUDA graph."""
+def run_ensemble(dev, K, W, seed, tuning, barrier, max_over_ranks):
+    """The 96-instance FP32 ensemble, sharded over the ranks (cdd.ensemble.ShardedEnsemble: greedy
+    bin packing on cells, one batched plan per rank, no data-path collective; N = 1 is one plan
+    over all instances). Each rank's stage is one launch per kernel over its instances, with
+    per-instance dt and the whole step in a CUDA graph. value = all instances' cell-stages / the
+    slowest rank's time (CUDA events on the launching stream)."""
     import torch
-    import cdd
+    from cdd.ensemble import ShardedEnsemble
     from cdd.initial import gaussian_random_field_torch
     spec = ensemble_instances(seed)
-    plan = cdd.Plan([s[3] for s in spec], "f32", tuning=tuning)
-    beta = plan.empty_field()
-    for i, (sh, sig, sd, _inst) in enumerate(spec):
-        plan.field_view(beta, i).copy_(gaussian_random_field_torch(sh, sig, 0.05, sd, device=dev))
-    plan.set_time(0.0, 1e30)
-    plan.run(beta, W, graph=True)
+    ens = ShardedEnsemble([s[3] for s in spec], "f32", tuning=tuning)
+    ens.load(lambda i: gaussian_random_field_torch(spec[i][0], spec[i][1], 0.05, spec[i][2], device=dev))
+    ens.set_time(0.0)
+    ens.run(W)
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    barrier()
     e0.record(st)
-    plan.run(beta, K, graph=True)
+    ens.run(K)
     e1.record(st)
-    torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) / 1e3
-    plan.check_status()
-    t, dt, act = plan.get_time()
-    cells = plan.total_cells
+    barrier()
+    el = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    ens.check_status()
+    table = ens.observables()            # (t, energy, mean_zz) of all 96 instances, one all-reduce
+    cells = ens.total_cells
+    dts = table[:, 0] / (W + K)
     return {"value": cells * 3 * K / el, "unit": UNIT, "ms_per_step": 1e3 * el / K, "steps": K,
             "instances": len(spec), "cells_per_stage": cells, "dtype": "f32",
-            "dt_range": [float(dt.min()), float(dt.max())],
+            "ranks": ens.world, "cells_per_rank_max": int(max_over_ranks(float(ens.local_cells))),
+            "dt_range": [float(dts.min()), float(dts.max())],
             "workload": "96 instances: 16 each of 256^2, 512^2, 48^3, 64^3, 96^3, 128^3; sigma U[0.02,0.08] L, "
-                        "rate_zz U[0,0.1] traceless; one plan, one CUDA graph per step"}
+                        "rate_zz U[0,0.1] traceless; sharded over the ranks, one plan and one CUDA graph per "
+                        "step per rank"}
 
 
 def run_adjoint(dev, seed, tuning):
@@ -289,10 +296,11 @@ def run_reference(args):
         mem_gb = psutil.virtual_memory().available / 2 ** 30
     except Exception:
         mem_gb = 16.0
-    # one 64^3 grid per worker and step: a 256^3 step of the oracle takes about 10 minutes on one
-    # core (128^3: about 80 s), so the whole-job rate is sampled on independent 64^3 grids
-    sample = 64
-    workers = max(1, min(cores, int(mem_gb // 1.5), 64))
+    # one 48^3 grid per worker and step: a 256^3 step of the oracle takes about 10 minutes on one
+    # core (128^3: about 80 s), so the whole-job rate is sampled on independent 48^3 grids (about
+    # 3 s per step with 16 workers), which keeps a 25-step run near a minute
+    sample = 48
+    workers = max(1, min(cores, int(mem_gb // 1.0), 64))
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
         for w in range(args.warmup):
@@ -384,6 +392,17 @@ def main():
         print(json.dumps({"only_vjp": "f32", "grid": list(shape)}))
         return
 
+    if args.only_step:
+        p = cdd.Plan([inst], args.only_step, tuning=None if args.no_tune else "auto")
+        b = p.empty_field()
+        b.copy_(b0.reshape(-1).to(p.dtype))
+        p.set_time(0.0, 1e30)
+        p.run(b, 3, graph=False)
+        p.check_status()
+        torch.cuda.synchronize()
+        print(json.dumps({"only_step": args.only_step, "grid": list(shape), "launch_shapes": p.tuning(0)}))
+        return
+
     if args.only_flux:
         p = cdd.Plan([inst], args.only_flux, tuning=None if args.no_tune else "auto")
         b = p.empty_field()
@@ -452,6 +471,14 @@ def main():
         beta32.copy_(b0.reshape(-1).to(torch.float32))
         p64.set_time(0.0, 1e30)
         p32.set_time(0.0, 1e30)
+        # the conditioning of the dynamics itself: FP64 from the same field with every value
+        # perturbed by a relative 1e-7 (about FP32 rounding), compared with the unperturbed FP64 run
+        p64b = cdd.Plan([inst], "f64", tuning=tuning)
+        beta64b = p64b.empty_field()
+        gen = torch.Generator(dev).manual_seed(11)
+        beta64b.copy_(b0.reshape(-1) * (1.0 + 1e-7 * torch.randn(b0.numel(), dtype=torch.float64, device=dev,
+                                                                   generator=gen)))
+        p64b.set_time(0.0, 1e30)
         n_prec = max(10, args.precision_steps)
         marks = sorted({m for m in (10, 50, 100, 200, n_prec) if m <= n_prec})
         e64, m64 = p64.observables(beta64)
@@ -461,6 +488,7 @@ def main():
         for n in range(1, n_prec + 1):
             p64.run(beta64, 1, graph=True)
             p32.run(beta32, 1, graph=True)
+            p64b.run(beta64b, 1, graph=True)
             e64, m64 = p64.observables(beta64)
             e32, m32 = p32.observables(beta32)
             curve64.append((e64[0], m64[0]))
@@ -469,12 +497,16 @@ def main():
                 a = beta64.view(9, -1)
                 b = beta32.view(9, -1).to(torch.float64)
                 rels = ((a - b).norm(dim=1) / a.norm(dim=1)).cpu().numpy()
+                relp = ((a - beta64b.view(9, -1)).norm(dim=1) / a.norm(dim=1)).cpu().numpy()
                 at_marks[str(n)] = {"per_field_rel_l2_max": float(rels.max()),
+                                    "fp64_perturbed_1e-7_rel_l2_max": float(relp.max()),
                                     "per_field_rel_l2": [float(x) for x in rels],
                                     "energy_rel": float(abs(e32[0] - e64[0]) / abs(e64[0])),
                                     "mean_zz_abs": float(abs(m32[0] - m64[0]))}
         p64.check_status()
         p32.check_status()
+        p64b.check_status()
+        del p64b, beta64b
         t64, _, _ = p64.get_time()
         t32, _, _ = p32.get_time()
         c64 = np.array(curve64)
@@ -488,7 +520,9 @@ def main():
             "mean_zz_curve_max_rel": float(np.max(np.abs(c32[:, 1] - c64[:, 1])) / np.max(np.abs(c64[:, 1]))),
             "t_final_fp64": float(t64[0]), "t_final_fp32": float(t32[0]),
             "note": "each form takes its own CFL steps (FP64 speed maximum in both), so the curves are "
-                    "compared step by step and the times differ by the accumulated dt difference"}
+                    "compared step by step and the times differ by the accumulated dt difference; "
+                    "fp64_perturbed_1e-7 is the FP64 run from the field perturbed by a relative 1e-7 per value, "
+                    "the growth the dynamics gives any rounding-sized difference"}
         del p64, beta64
 
     # ---------------- end to end: host buffers through the public API ----------------
@@ -526,8 +560,8 @@ def main():
     ens = None
     if world == 1 and not args.no_adjoint:
         adj = run_adjoint(dev, 5, tuning)
-    if world == 1 and not args.no_ensemble:
-        ens = run_ensemble(dev, max(3, min(K, 5)), W, 2024, tuning)
+    if not args.no_ensemble:
+        ens = run_ensemble(dev, max(3, min(K, 5)), W, 2024, tuning, barrier, max_over_ranks)
 
     if world > 1:
         dist.barrier()
@@ -543,7 +577,10 @@ def main():
     issue_ach = FLUX_WARP_INST_PER_CELL * cells / t_stencil / 1e9
     stage_s = el32 / K / 3
     achieved = WORDS_PER_CELL_STAGE * 4 * cells / stage_s / 1e9
-    launches_per_step = 3 * 6 + 3 + 2
+    # per stage: the stress solve (fused plane passes: forward, mean, k-space, inverse; else six
+    # passes incl. the mean) and the stencil; per step: k_dt and the F0 axpy
+    stress_launches = 4 if p32_tuning.get("plane_fft") == 1 else 6
+    launches_per_step = 3 * (stress_launches + 1) + 2
     line = {
         "metric": METRIC, "value": rate32, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

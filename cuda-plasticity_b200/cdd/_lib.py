@@ -63,9 +63,10 @@ class cdd_tuning(ctypes.Structure):
         ("mid_cols", ctypes.c_int),
         ("green_cols", ctypes.c_int),
         ("stencil_planes", ctypes.c_int),
+        ("plane_fft", ctypes.c_int),
     ]
 
-    KEYS = ("fft_radix", "rows_lines", "mid_cols", "green_cols", "stencil_planes")
+    KEYS = ("fft_radix", "rows_lines", "mid_cols", "green_cols", "stencil_planes", "plane_fft")
 
     @classmethod
     def from_dict(cls, d):

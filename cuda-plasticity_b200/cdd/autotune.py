@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib
 
-KNOBS = ("stencil_planes", "fft_radix", "green_cols", "mid_cols", "rows_lines")
+KNOBS = ("stencil_planes", "fft_radix", "green_cols", "mid_cols", "rows_lines", "plane_fft")
 
 
 def cache_path():
@@ -39,7 +39,7 @@ def load_cache(path=None):
 def save_cache(d, path=None):
     path = path or cache_path()
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
-    tmp = path + ".tmp"
+    tmp = "%s.%d.tmp" % (path, os.getpid())   # ranks of one job may save at the same time
     with open(tmp, "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
     os.replace(tmp, path)
@@ -57,6 +57,9 @@ def candidates(knob, shape, current):
         return sorted({p for p in (2, 4, 8, 16, 32, 64) if p <= shape[0]} | ({v} if v else set()))
     if knob == "mid_cols" and nd != 3:
         return []
+    if knob == "plane_fft":
+        # fused plane passes (1) or separate row and axis-1 passes (-1); 0: not applicable
+        return [1, -1] if v else []
     if v <= 0:
         return []
     return sorted({max(1, v // 2), v, v * 2})

@@ -214,6 +214,7 @@ struct InstDev {
     PassTile tile[NUM_PASSES];
     int stencil_blocks;
     int st_zc;              // planes per stencil block along axis 0 (3-D)
+    int plane;              // 1: the stress solve runs the fused plane passes (k_plane_fwd / k_plane_inv)
     int tma_slot;           // index of this instance's tensor map, -1: threads stage the planes
     int tma_sub;            // index of this instance in its map's run of same-shape instances
     double mu, nu, lamb, Lambda, cfl, nmax;
@@ -808,6 +809,8 @@ struct PlanCore {
     int* d_status = nullptr;
     LaunchShape pass[NUM_PASSES];
     LaunchShape pass9[NUM_PASSES];   // the k-space observables: 9-component row / axis-1 passes, 12-slot k-space pass
+    LaunchShape plane;               // stress solve: fused plane passes of the instances with plane set
+    LaunchShape rest[NUM_PASSES];    // stress solve: the row and axis-1 passes of the other instances
     bool obs_ok = false;             // pass9 fits the device (shared memory of the 12-slot k-space pass)
     LaunchShape stencil;
     LaunchShape cellwise;            // elementwise kernels over cells
@@ -832,6 +835,10 @@ struct StencilMapSet {
 // stress.cu
 // phi (optional): per k point of the input, s1 / kSq - r / kSqSq (see k_green), for the nu gradient.
 cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st, void* phi = nullptr);
+// The second RK3 stage's stress: rhs_f0 holds the stage-1 rhs on entry and F0 = u + dt rhs on
+// return (dt from the instances' clocks); sigma = stress(F0).
+cudaError_t launch_stress_f0(const PlanCore& P, const void* u, void* rhs_f0, void* sigma, cudaStream_t st,
+                             void* phi = nullptr);
 // phi / part (optional): phi of the state, per-green-block partials of the Parseval nu sum.
 cudaError_t launch_stress_adjoint(const PlanCore& P, const void* sigbar6, void* betabar9, cudaStream_t st,
                                   const void* phi = nullptr, double* part = nullptr);
@@ -889,5 +896,10 @@ inline cudaError_t set_dyn_smem_limit(F* fn, size_t smem) {
 size_t stencil_smem_bytes(int precision, bool any3d);
 void stencil_geometry(InstDev& I, int planes = 0);
 cudaError_t stress_set_attributes(int precision, size_t max_smem);
+// Fused plane passes of the stress solve (stress.cu): whether instance I can take them and their
+// shared memory per block.
+bool plane_eligible(const InstDev& I, int precision, size_t smem_limit);
+size_t plane_smem_bytes(const InstDev& I);
+constexpr int PLANE_CLUSTER = 8;   // blocks per (component, plane) cluster
 
 }  // namespace cdd

@@ -169,6 +169,17 @@ int build_shapes(cdd_plan* p, size_t elt) {
     std::vector<int> pre9[NUM_PASSES];   // the observables' launch shapes (9 components)
     for (int k = 0; k < NUM_PASSES; ++k) pre9[k].push_back(0);
     size_t smem_green12 = 0;
+    // the fused plane passes of the stress solve (3-D FP32 shapes that allow them) and the separate
+    // row / axis-1 passes of the other instances
+    std::vector<int> pre_plane(1, 0), pre_rest[NUM_PASSES];
+    for (int k = 0; k < NUM_PASSES; ++k) pre_rest[k].push_back(0);
+    size_t smem_plane = 0;
+    int optin_dev = 0;
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin_dev, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
     for (int i = 0; i < n; ++i) {
         InstDev& I = p->inst[i];
         // rows kernels (R2C: 9 components, C2R: 6); ping-pong buffers of P padded rows
@@ -247,6 +258,17 @@ int build_shapes(cdd_plan* p, size_t elt) {
             const size_t sm = ((size_t)12 * (I.n0 * W + W) + 1) / 2 * 2 * velt + (size_t)I.lp_first.twspan * velt;
             if (sm > smem_green12) smem_green12 = sm;
         }
+        {
+            const bool ok = plane_eligible(I, C.precision, (size_t)optin_dev);
+            if (p->tune[i].plane_fft == 1 && !ok)
+                return fail(CDD_ERR_ARG, "instance %d: tuning plane_fft 1, but the shape or precision does not allow "
+                                         "the fused plane passes", i);
+            I.plane = (ok && p->tune[i].plane_fft >= 0) ? 1 : 0;
+            p->tune[i].plane_fft = (I.nd == 3 && C.precision == CDD_F32) ? (I.plane ? 1 : -1) : 0;
+            pre_plane.push_back(pre_plane.back() + (I.plane ? 6 * I.n0 * PLANE_CLUSTER : 0));
+            for (int k = 0; k < NUM_PASSES; ++k) pre_rest[k].push_back(pre_rest[k].back() + (I.plane ? 0 : I.tile[k].blocks));
+            if (I.plane && plane_smem_bytes(I) > smem_plane) smem_plane = plane_smem_bytes(I);
+        }
         stencil_geometry(I, p->tune[i].stencil_planes);
         // effective launch shapes of this instance
         p->tune[i].rows_lines = I.tile[PASS_R2C].lines;
@@ -294,6 +316,19 @@ int build_shapes(cdd_plan* p, size_t elt) {
         if (L9.smem > smem_all) smem_all = L9.smem;
         CDD_CUDA(dalloc(p, (void**)&L9.d_pre, sizeof(int) * (n + 1)));
         CDD_CUDA(cudaMemcpy(L9.d_pre, pre9[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
+    C.plane.blocks = pre_plane.back();
+    C.plane.threads = 256;
+    C.plane.smem = smem_plane;
+    CDD_CUDA(dalloc(p, (void**)&C.plane.d_pre, sizeof(int) * (n + 1)));
+    CDD_CUDA(cudaMemcpy(C.plane.d_pre, pre_plane.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    for (int k = 0; k < NUM_PASSES; ++k) {
+        LaunchShape& L = C.rest[k];
+        L.blocks = pre_rest[k].back();
+        L.threads = C.pass[k].threads;
+        L.smem = C.pass[k].smem;
+        CDD_CUDA(dalloc(p, (void**)&L.d_pre, sizeof(int) * (n + 1)));
+        CDD_CUDA(cudaMemcpy(L.d_pre, pre_rest[k].data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     }
     {
         int dev = 0, optin = 0;
@@ -351,8 +386,7 @@ int record_step(cdd_plan* p, void* beta, cudaStream_t st, int fixed, double dt_f
     CDD_CUDA(launch_stress(C, beta, C.d_sigma, st));
     CDD_CUDA(launch_stencil(C, M_STAGE1, beta, beta, C.d_f0, nullptr, 0.0, mu, st));
     CDD_CUDA(launch_dt(C, fixed, dt_fixed, st));
-    CDD_CUDA(launch_axpy_f0(C, beta, C.d_f0, st));
-    CDD_CUDA(launch_stress(C, C.d_f0, C.d_sigma, st));
+    CDD_CUDA(launch_stress_f0(C, beta, C.d_f0, C.d_sigma, st));
     CDD_CUDA(launch_stencil(C, M_STAGE2, C.d_f0, beta, C.d_f1, nullptr, 0.0, p->maps_f0, st));
     CDD_CUDA(launch_stress(C, C.d_f1, C.d_sigma, st));
     CDD_CUDA(launch_stencil(C, M_STAGE3, C.d_f1, beta, beta, nullptr, 0.0, p->maps_f1, st));
@@ -395,12 +429,13 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
             (t.rows_lines && t.rows_lines > 1024) ||
             (t.mid_cols && (!pow2(t.mid_cols) || t.mid_cols > 64)) ||
             (t.green_cols && (!pow2(t.green_cols) || t.green_cols > 64)) || t.stencil_planes < 0 ||
-            t.fft_radix < 0 || t.rows_lines < 0 || t.mid_cols < 0 || t.green_cols < 0)
+            t.fft_radix < 0 || t.rows_lines < 0 || t.mid_cols < 0 || t.green_cols < 0 ||
+            t.plane_fft < -1 || t.plane_fft > 1)
             return fail(CDD_ERR_ARG, "instance %d: bad tuning (radix 4/8/16; lines <= 1024; columns: powers of "
-                                     "two <= 64; planes >= 0)", i);
+                                     "two <= 64; planes >= 0; plane_fft -1, 0 or 1)", i);
     }
     cdd_plan* p = new cdd_plan();
-    p->tune.assign(n_inst, cdd_tuning{0, 0, 0, 0, 0});
+    p->tune.assign(n_inst, cdd_tuning{0, 0, 0, 0, 0, 0});
     if (tune) p->tune.assign(tune, tune + n_inst);
     for (auto& t : p->tune)
         if (!t.fft_radix) t.fft_radix = 16;
@@ -1059,8 +1094,7 @@ int cdd_step_record(cdd_plan* p, void* beta, double t, double dt, void* rec, voi
     K.d_sigma = s_u;
     CDD_CUDA(launch_stencil(K, M_STAGE1, beta, beta, f0, nullptr, 0.0, user_maps(p, beta), st));
     CDD_CUDA(launch_dt(C, 1, dt, st));
-    CDD_CUDA(launch_axpy_f0(C, beta, f0, st));
-    CDD_CUDA(launch_stress(C, f0, s_f0, st, r + L.pf0 * elt));
+    CDD_CUDA(launch_stress_f0(C, beta, f0, s_f0, st, r + L.pf0 * elt));
     K.d_sigma = s_f0;
     StencilMapSet m0, m1;
     encode_stencil_maps(C, p->inst.data(), f0, m0);

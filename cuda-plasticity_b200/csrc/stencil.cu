@@ -126,6 +126,18 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+// One element (4 or 8 bytes) global -> shared without a register round trip; each thread waits for
+// its own copies only (cp.async.wait_all), so no block barrier is needed when a thread reads back
+// what it copied.
+__device__ __forceinline__ void cp_async_elem(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_own() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // u+ and u- from the five values u_{-2} .. u_{+2} along one axis. The limiter arguments D1, D2
 // of FindDerivatives all carry 1/h^2; minmod is positively homogeneous, so the kernel limits the
 // undivided second differences and applies 1/h once: u+ = (d_0 - mm/2) / h, u- = (d_-1 + mm_-1/2) / h.
@@ -455,12 +467,16 @@ template <typename T> struct CellCtx {
     bool has_load, lam_on, glide;
 };
 
+// ssm: this thread's 6 shared-memory stress slots (component c at ssm[c * ST_THREADS]), filled by
+// asynchronous copies issued one cell earlier; sig_next: the stress of the thread's cell in the
+// next plane (its copies are issued as soon as this cell's values are read), or null.
 template <typename T, int ND, int MODE, int VAR>
 __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>& cx, bool valid,
                                              const TileView<T, ND>& tv,
                                              const StageConst& kc_block, const InstClock& ck, double t_flux,
                                              double& vmax, double& esum, double& zsum,
-                                             const T* __restrict__ sig0, const T* __restrict__ vac) {
+                                             const T* __restrict__ sig0, const T* __restrict__ vac,
+                                             T* ssm, const T* sig_next) {
     // compile-time variant: bit 0 carries the glide-only projection, bit 1 the vacancy term
     constexpr bool GLIDE = (VAR & 1) != 0;
     constexpr bool VAC = (VAR & 2) != 0;
@@ -483,12 +499,26 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
     }
     const double* ld = kc.ld;
     // total stress at the cell: internal + applied load (FP64), symmetric
-    const T* sp = cx.sig;
     T S[3][3];
     {
         T s6[6];
+        cp_async_wait_own();
 #pragma unroll
-        for (int c = 0; c < 6; ++c) s6[c] = sp[c * cells];
+        for (int c = 0; c < 6; ++c) s6[c] = ssm[c * ST_THREADS];
+        if (sig_next) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) cp_async_elem(ssm + c * ST_THREADS, sig_next + c * cells);
+            cp_async_commit();
+        }
+        if (MODE == M_STAGE1 && valid) {
+            // observables of the step-start state: elastic energy of the internal stress (k_dt
+            // applies 1 / (4 mu) to the instance sum)
+            const double s0 = (double)s6[0], s1 = (double)s6[1], s2 = (double)s6[2];
+            const double s3 = (double)s6[3], s4 = (double)s6[4], s5 = (double)s6[5];
+            const double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
+            const double tr = s0 + s3 + s5;
+            esum += sq - kc.cnu * tr * tr;
+        }
         S[0][0] = (T)((double)s6[0] + ld[0]);
         S[1][1] = (T)((double)s6[3] + ld[1]);
         S[2][2] = (T)((double)s6[5] + ld[2]);
@@ -781,13 +811,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             double v = (double)spd;
             if (!(v <= 1.0e300)) v = __longlong_as_double(0x7ff0000000000000LL);   // NaN/Inf -> +Inf
             vmax = fmax(vmax, v);
-            // observables of the step-start state: elastic energy of the internal stress, mean b_zz
-            double s0 = (double)sp[0], s1 = (double)sp[cells], s2 = (double)sp[2 * cells];
-            double s3 = (double)sp[3 * cells], s4 = (double)sp[4 * cells], s5 = (double)sp[5 * cells];
-            double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
-            double tr = s0 + s3 + s5;
-            esum += sq - kc.cnu * tr * tr;   // k_dt applies 1 / (4 mu) to the instance sum
-            zsum += (double)tv.center(8);
+            zsum += (double)tv.center(8);   // mean b_zz of the step-start state
         }
     } else if constexpr (UPD) {
         if (valid && kc.active) {
@@ -965,6 +989,11 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     TileView<T, ND> tv;
     tv.sm = sm;
     tv.idx = (ty + 2) * RX + tx + OX;
+    // the stress of the thread's cell, one plane ahead, in shared memory after the ring
+    T* ssm = sm + NS * 9 * PP + tid;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) cp_async_elem(ssm + c * ST_THREADS, cx.sig + c * cells);
+    cp_async_commit();
 #pragma unroll 1
     for (int z = z0, k = 0; ok && z < z1; ++z, ++k) {
         const bool more = (z + 1 < z1);
@@ -990,7 +1019,8 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         } else {
             tv.so[2] = 0;
         }
-        stencil_cell<T, ND, MODE, VAR>(I, cx, own, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac);
+        stencil_cell<T, ND, MODE, VAR>(I, cx, own, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac, ssm,
+                                       more ? cx.sig + plane : nullptr);
         cx.sig += plane;
         if (cx.bn) cx.bn += plane;
         cx.out += plane;
@@ -1010,9 +1040,13 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
                 __syncthreads();
                 load_box((k + 5) % NS, wrapz(z + 3), true);   // plane pr = k + 5 lives in slot pr % NS
             }
-            __syncthreads();
+            // arrive's block-wide vote already orders this cell's reads before the next copy into
+            // the ring; a barrier is left only for plain shared-memory stores (edge patches, thread
+            // staging) to become visible
+            if (!use_tma || edge) __syncthreads();
         }
     }
+    cp_async_wait_own();   // no stress copy in flight past here
     if (!ok) {
         // a copy did not land in time: let every copy this block issued finish (bounded), then leave
         for (int pr = max(0, issued - NS + 1); pr <= issued; ++pr)
@@ -1101,14 +1135,15 @@ __global__ void __launch_bounds__(1024) k_dt(const InstDev* __restrict__ insts,
     }
 }
 
-// F0 = u + dt * rhs, in place on the rhs buffer, for active instances.
+// F0 = u + dt * rhs, in place on the rhs buffer, for active instances (one fused multiply-add per
+// value). Instances with the fused plane passes form F0 in their forward pass instead.
 template <typename T>
 __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ insts, int n_inst,
                                                  const int* __restrict__ pre, const T* __restrict__ u,
                                                  T* __restrict__ f0, const InstClock* __restrict__ clk) {
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
-    if (!clk[ii].active) return;
+    if (!clk[ii].active || I.plane) return;
     const T dt = (T)clk[ii].dt;
     const long long n = 9 * I.cells;
     const long long b0 = (long long)(blockIdx.x - pre[ii]) * blockDim.x * 4;   // 4 elements per thread
@@ -1120,10 +1155,10 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
             const long long i = b0 + 4 * threadIdx.x;
             const float4 a = *reinterpret_cast<const float4*>(uu + i);
             float4 r = *reinterpret_cast<const float4*>(ff + i);
-            r.x = a.x + dt * r.x;
-            r.y = a.y + dt * r.y;
-            r.z = a.z + dt * r.z;
-            r.w = a.w + dt * r.w;
+            r.x = __fmaf_rn(dt, r.x, a.x);
+            r.y = __fmaf_rn(dt, r.y, a.y);
+            r.z = __fmaf_rn(dt, r.z, a.z);
+            r.w = __fmaf_rn(dt, r.w, a.w);
             *reinterpret_cast<float4*>(ff + i) = r;
         } else {
 #pragma unroll
@@ -1131,8 +1166,8 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
                 const long long i = b0 + 512 * k + 2 * threadIdx.x;
                 const double2 a = *reinterpret_cast<const double2*>(uu + i);
                 double2 r = *reinterpret_cast<const double2*>(ff + i);
-                r.x = a.x + dt * r.x;
-                r.y = a.y + dt * r.y;
+                r.x = __fma_rn(dt, r.x, a.x);
+                r.y = __fma_rn(dt, r.y, a.y);
                 *reinterpret_cast<double2*>(ff + i) = r;
             }
         }
@@ -1141,7 +1176,7 @@ __global__ void __launch_bounds__(256) k_axpy_f0(const InstDev* __restrict__ ins
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         long long i = b0 + threadIdx.x + (long long)k * blockDim.x;
-        if (i < n) ff[i] = uu[i] + dt * ff[i];
+        if (i < n) ff[i] = fma(dt, ff[i], uu[i]);
     }
 }
 
@@ -1411,10 +1446,11 @@ cudaError_t stencil_set_attributes(int precision, size_t smem) {
     return precision == CDD_F32 ? st_attr<float>(smem) : st_attr<double>(smem);
 }
 
+// The plane ring plus the 6 stress slots of every thread.
 size_t stencil_smem_bytes(int precision, bool any3d) {
     if (precision == CDD_F32)
-        return (size_t)(any3d ? TileGeom<float>::NS : 1) * 9 * tile_pp<float>() * sizeof(float);
-    return (size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() * sizeof(double);
+        return ((size_t)(any3d ? TileGeom<float>::NS : 1) * 9 * tile_pp<float>() + 6 * ST_THREADS) * sizeof(float);
+    return ((size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() + 6 * ST_THREADS) * sizeof(double);
 }
 
 // Blocks of the stencil: (x, y) tiles times chunks of planes along axis 0. Built-in rule: about

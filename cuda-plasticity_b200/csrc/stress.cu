@@ -108,14 +108,41 @@ __device__ __forceinline__ void src_rows(const InstDev& I, const T* base, int mo
 // 32 (the block size is too): each warp takes part in a loop trip whole, as the shuffles need
 // (rows_io_plan).
 // ------------------------------------------------------------------------------------------
-template <typename T, bool MEAN64, int R0, int R1>
+// The half spectra of pair p's two rows go to dst + 2 (p - p0) dld and one row (dld) further:
+// the plan's spectrum (p0 = 0, dld = nhp) or a block's shared tile (the plane passes).
+// F0 (the second RK3 stage's stress): the rows are formed as F0 = u + dt rhs from the rows of u and
+// of rhs (held in f0w, the buffer rt points into) and written back over rhs, so the stage input is
+// made in the same sweep that transforms it.
+template <typename T> __device__ __forceinline__ T fma_t(T a, T b, T c);
+template <> __device__ __forceinline__ float fma_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <> __device__ __forceinline__ double fma_t<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <typename T, bool F0>
+__device__ __forceinline__ T row_value(const T* __restrict__ beta, T* f0w, const T* __restrict__ u, T dt,
+                                       const RowPtr& e, int i) {
+    if constexpr (F0) {
+        const T xp = fma_t(dt, f0w[e.p + i], u[e.p + i]);
+        f0w[e.p + i] = xp;
+        T xq = xp;
+        if (e.q != e.p) {
+            xq = fma_t(dt, f0w[e.q + i], u[e.q + i]);
+            f0w[e.q + i] = xq;
+        }
+        return (T)0.5 * (xp + xq);
+    } else {
+        return (T)0.5 * (beta[e.p + i] + beta[e.q + i]);
+    }
+}
+
+template <typename T, bool MEAN64, int R0, int R1, bool F0 = false>
 __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int ld, const RowPtr* __restrict__ rt,
                                             const T* __restrict__ beta, typename VecOf<T>::type* s,
                                             const typename VecOf<T>::type* __restrict__ tw1,
                                             typename VecOf<T>::type* __restrict__ dst, double* __restrict__ rowsum,
-                                            long long nrows, long long npairs, int tid, int nt) {
+                                            long long nrows, long long npairs, int tid, int nt,
+                                            long long p0, int dld, T* f0w = nullptr, const T* u = nullptr,
+                                            T dt = 0) {
     typedef typename VecOf<T>::type V;
-    const T half = (T)0.5;
     // stage 0 (span 1): butterfly (l, j) takes elements j + R1 r of pair line l
 #pragma unroll 1
     for (int g = tid; g < P * R1; g += nt) {
@@ -127,8 +154,8 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
         for (int r = 0; r < R0; ++r) {
             const int i = j + R1 * r;
             T a = 0, b = 0;
-            if (ea.p >= 0) a = half * (beta[ea.p + i] + beta[ea.q + i]);
-            if (eb.p >= 0) b = half * (beta[eb.p + i] + beta[eb.q + i]);
+            if (ea.p >= 0) a = row_value<T, F0>(beta, f0w, u, dt, ea, i);
+            if (eb.p >= 0) b = row_value<T, F0>(beta, f0w, u, dt, eb, i);
             if (MEAN64) { sa += (double)a; sb += (double)b; }
             v[r].x = a;
             v[r].y = b;
@@ -168,7 +195,7 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
         const long long p = (long long)lb * P + l;
         const bool valid = p < npairs;
         const bool hasb = 2 * p + 1 < nrows;
-        V* da = dst + 2 * p * I.nhp;
+        V* da = dst + 2 * (p - p0) * dld;
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
             V zs;
@@ -184,7 +211,7 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
                 b.x = (T)0.5 * (zk.y + zm.y);
                 b.y = (T)-0.5 * (zk.x - zm.x);
                 da[k] = a;
-                if (hasb) da[I.nhp + k] = b;
+                if (hasb) da[dld + k] = b;
             }
         }
     }
@@ -243,7 +270,7 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_r2c_row
 #define CDD_R2C_IO(A, B)                                                                                      \
         if (io && lq.radix[0] == A && lq.radix[1] == B) {                                                     \
             r2c_rows_io<T, MEAN64, A, B>(I, lb, P, ld, rt, beta, s, tw1, spec + I.spoff, rowsum, nrows, npairs,  \
-                                          tid, nt);                                                           \
+                                          tid, nt, 0, I.nhp);                                                 \
             return;                                                                                           \
         }
         CDD_ROWIO_SEQS(CDD_R2C_IO)
@@ -404,15 +431,15 @@ __device__ __forceinline__ void c2r_rows_io(const InstDev& I, int lb, int P, int
                                             typename VecOf<T>::type* s,
                                             const typename VecOf<T>::type* __restrict__ tw1, T* __restrict__ out,
                                             const T* __restrict__ beta, int epi, long long nrows, long long npairs,
-                                            int tid, int nt) {
+                                            int tid, int nt, long long p0, int sld) {
     typedef typename VecOf<T>::type V;
     constexpr int N = R0 * R1;
 #pragma unroll 1
     for (int g = tid; g < P * R1; g += nt) {
         const int l = g / R1, j = g - l * R1;
         const long long p = (long long)lb * P + l;
-        const V* sa = (p < npairs) ? src + 2 * p * I.nhp : nullptr;
-        const V* sb = (p < npairs && 2 * p + 1 < nrows) ? sa + I.nhp : nullptr;
+        const V* sa = (p < npairs) ? src + 2 * (p - p0) * sld : nullptr;
+        const V* sb = (p < npairs && 2 * p + 1 < nrows) ? sa + sld : nullptr;
         V v[R0];
 #pragma unroll
         for (int r = 0; r < R0; ++r) {
@@ -529,7 +556,7 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_c2r_row
 #define CDD_C2R_IO(A, B)                                                                                      \
         if (io && lq.radix[0] == A && lq.radix[1] == B) {                                                     \
             c2r_rows_io<T, MEAN64, A, B>(I, lb, P, ld, rt, re, rmean, src, s, tw1, out, beta, epi, nrows, npairs, \
-                                          tid, nt);                                                           \
+                                          tid, nt, 0, I.nhp);                                                 \
             return;                                                                                           \
         }
         CDD_ROWIO_SEQS(CDD_C2R_IO)
@@ -1145,6 +1172,272 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
 }
 
 // ------------------------------------------------------------------------------------------
+// Plane passes (3-D FP32 instances that plane_layout accepts): the transforms along the contiguous
+// axis and along axis 1 of one z-plane of one component in one kernel, so the spectrum crosses HBM
+// once between them instead of twice. One cluster of PLANE_C blocks per (component o, plane z):
+//   forward: block r runs the R2C of rows [r Rc, (r+1) Rc) of the plane (two real rows per complex
+//     FFT, as k_r2c_rows) into its shared tile S_own (Rc rows of nh half-spectrum values); after a
+//     cluster barrier it gathers spectrum columns [r W, (r+1) W) of all n1 rows from the blocks'
+//     tiles through distributed shared memory into S_col, transforms them along axis 1 and writes
+//     them to the plan's spectrum, which the k-space pass (k_green) reads as before;
+//   inverse: the mirror image: block r loads columns [r W, (r+1) W) of the plane's spectrum,
+//     inverts the axis-1 transform, gathers rows [r Rc, (r+1) Rc) of all columns from the blocks'
+//     tiles and runs the C2R of those rows (plus the FP64 mean stress) into sigma.
+// Columns 0 and nl/2 of a row's half spectrum are real (the R2C split makes their imaginary parts
+// exactly zero), so block 0 carries them as one complex column X0 + i X_{nl/2}; its axis-1
+// transform F = F0 + i FN is split again by Hermitian symmetry, F0(ky) = (F(ky) + conj F(-ky)) / 2,
+// FN(ky) = (F(ky) - conj F(-ky)) / (2i). The inverse packs the Hermitian parts H(G)(ky) =
+// (G(ky) + conj G(-ky)) / 2 of the two columns as H(G0) + i H(GN): the inverse transform of H(G) is
+// the real part of that of G, which is what the C2R keeps of those bins (numpy's irfft semantics).
+// That keeps W = nl / (2 PLANE_C) columns per block, a power of two. Same codelets, twiddles and
+// row tables as the separate passes; results agree with them to rounding.
+// Shared memory (V = complex): region A = S_own (Rc x ldo) or the axis-1 scratch tile (n1 x W);
+// region B = the row pass's line buffer (P x rows_ld(nl)) or S_col (n1 x W); the row twiddles;
+// the row tables. Regions are reused only across block or cluster barriers.
+// ------------------------------------------------------------------------------------------
+constexpr int PLANE_C = PLANE_CLUSTER;
+
+struct PlaneGeom {
+    int Rc, P, W, lgw, ldo, ld;
+    size_t a, b, tw, tab, total;   // region sizes in bytes (16-byte multiples) and the sum
+};
+
+__host__ __device__ inline PlaneGeom plane_geom(const InstDev& I, size_t velt) {
+    PlaneGeom g;
+    g.Rc = I.n1 / PLANE_C;
+    g.P = g.Rc / 2;
+    g.W = (I.nl / 2) / PLANE_C;
+    g.lgw = 0;
+    while ((1 << g.lgw) < g.W) ++g.lgw;
+    g.ldo = (I.nh + 1) & ~1;   // even: 16-byte aligned FP32 rows
+    g.ld = rows_ld(I.nl);
+    auto r16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    const size_t colt = (size_t)I.n1 * g.W * velt;
+    const size_t own = (size_t)g.Rc * g.ldo * velt, line = (size_t)g.P * g.ld * velt;
+    g.a = r16(own > colt ? own : colt);
+    g.b = r16(line > colt ? line : colt);
+    g.tw = r16((size_t)I.lp_last.twspan * velt);
+    g.tab = r16(rows_table_bytes(g.P));
+    g.total = g.a + g.b + g.tw + g.tab;
+    return g;
+}
+
+// Whether instance I runs its stress transforms through the plane passes (FP32 plans): n1 and nl
+// powers of two with Rc = n1 / PLANE_C an even number of rows, at least two columns per block, the
+// register-resident two-stage row codelets (rows_io_plan) and a two-stage compile-time axis-1 plan.
+bool plane_eligible(const InstDev& I, int precision, size_t smem_limit) {
+    if (precision != CDD_F32 || I.nd != 3) return false;
+    auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+    if (!pow2(I.n1) || !pow2(I.nl)) return false;
+    if (I.n1 % (2 * PLANE_C) != 0 || (I.nl / 2) % (2 * PLANE_C) != 0) return false;
+    const PlaneGeom g = plane_geom(I, sizeof(float2));
+    if (!rows_io_plan(I.lp_last, g.P)) return false;
+    if (!(line_plan_io(I.lp_mid) && I.lp_mid.nst == 2)) return false;
+    return g.total + 1024 <= smem_limit;
+}
+
+size_t plane_smem_bytes(const InstDev& I) { return plane_geom(I, sizeof(float2)).total; }
+
+// F0: beta holds the stage-1 rhs; the kernel forms F0 = u + dt rhs row by row (dt from the
+// instance's clock), writes it back over rhs and transforms it (see r2c_rows_io).
+template <typename T, bool F0>
+__global__ void __cluster_dims__(PLANE_C, 1, 1) __launch_bounds__(ROW_THREADS, 3)
+k_plane_fwd(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre, const T* beta,
+            typename VecOf<T>::type* __restrict__ spec, const typename VecOf<T>::type* __restrict__ tw,
+            double* __restrict__ rowsum, T* f0w, const T* __restrict__ u, const InstClock* __restrict__ clk) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    const int lb = blockIdx.x - pre[ii];
+    const int rank = (int)cl.block_rank();
+    const int q = lb / PLANE_C;              // o * n0 + z
+    const int o = q / I.n0, z = q - o * I.n0;
+    const PlaneGeom g = plane_geom(I, sizeof(V));
+    const int N = I.nl, n1 = I.n1, W = g.W, lgw = g.lgw, ldo = g.ldo, P = g.P;
+    V* s_own = reinterpret_cast<V*>(smem_raw);
+    V* s_col = reinterpret_cast<V*>(smem_raw + g.a);
+    V* tws = reinterpret_cast<V*>(smem_raw + g.a + g.b);
+    RowPtr* rt = reinterpret_cast<RowPtr*>(smem_raw + g.a + g.b + g.tw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long nrows = 6LL * I.rows, npairs = nrows / 2;
+    const long long plane_row = (long long)o * I.rows + (long long)z * n1;   // first row of the plane
+    const long long row0 = plane_row + (long long)rank * g.Rc;
+    const long long p0 = row0 / 2;
+    const int lbv = (int)(p0 / P);           // the row pass's block index of these rows
+    for (int r = tid; r < 2 * P; r += nt) {
+        const T *pa, *qa;
+        src_rows(I, beta, RS_SYM, row0 + r, pa, qa);
+        RowPtr e;
+        e.p = pa - beta;
+        e.q = qa - beta;
+        rt[r] = e;
+    }
+    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
+    __syncthreads();
+    {
+        const LinePlan& lq = I.lp_last;
+        const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
+        constexpr bool MEAN64 = sizeof(T) == 4;
+        const T dt = F0 ? (T)clk[ii].dt : (T)0;
+        if (lq.radix[0] == 16 && lq.radix[1] == 16)
+            r2c_rows_io<T, MEAN64, 16, 16, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
+                                               tid, nt, p0, ldo, f0w, u, dt);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 8)
+            r2c_rows_io<T, MEAN64, 16, 8, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
+                                              tid, nt, p0, ldo, f0w, u, dt);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 4)
+            r2c_rows_io<T, MEAN64, 16, 4, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
+                                              tid, nt, p0, ldo, f0w, u, dt);
+        else
+            r2c_rows_io<T, MEAN64, 8, 4, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
+                                             tid, nt, p0, ldo, f0w, u, dt);
+    }
+    cl.sync();   // every block's half spectra are in its S_own
+    {
+        const int lrc = 31 - __clz(g.Rc);   // Rc is a power of two
+        for (int e = tid; e < n1 * W; e += nt) {
+            const int y = e >> lgw, w = e & (W - 1);
+            const int src = y >> lrc, ly = y - (src << lrc);
+            const V* so = cl.map_shared_rank(s_own, src) + ly * ldo;
+            V v;
+            if (rank == 0 && w == 0) {
+                v.x = so[0].x;
+                v.y = so[N / 2].x;
+            } else {
+                v = so[rank * W + w];
+            }
+            s_col[e] = v;
+        }
+    }
+    cl.sync();   // no block reads another's S_own from here on
+    SColT<V, 1> col{s_col, lgw, 0}, scr{s_own, lgw, 0};
+    fft_io<V, false, 1>(col, scr, scr, col, lgw, I.lp_mid, tw, tid, nt, 0);
+    V* dst = spec + I.spoff + plane_row * I.nhp;
+    for (int e = tid; e < n1 * W; e += nt) {
+        const int ky = e >> lgw, w = e & (W - 1);
+        const V v = s_col[e];
+        V* d = dst + (long long)ky * I.nhp;
+        if (rank == 0 && w == 0) {
+            const int km = (ky == 0) ? 0 : n1 - ky;
+            const V zm = s_col[km << lgw];
+            V a, b;
+            a.x = (T)0.5 * (v.x + zm.x);
+            a.y = (T)0.5 * (v.y - zm.y);
+            b.x = (T)0.5 * (v.y + zm.y);
+            b.y = (T)-0.5 * (v.x - zm.x);
+            d[0] = a;
+            d[N / 2] = b;
+        } else {
+            d[rank * W + w] = v;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __cluster_dims__(PLANE_C, 1, 1) __launch_bounds__(ROW_THREADS, 3)
+k_plane_inv(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre,
+            const typename VecOf<T>::type* __restrict__ spec, T* __restrict__ out,
+            const typename VecOf<T>::type* __restrict__ tw, const double* __restrict__ sbar) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    const int lb = blockIdx.x - pre[ii];
+    const int rank = (int)cl.block_rank();
+    const int q = lb / PLANE_C;
+    const int o = q / I.n0, z = q - o * I.n0;
+    const PlaneGeom g = plane_geom(I, sizeof(V));
+    const int N = I.nl, n1 = I.n1, W = g.W, lgw = g.lgw, ldo = g.ldo, P = g.P;
+    V* s_own = reinterpret_cast<V*>(smem_raw);
+    V* s_col = reinterpret_cast<V*>(smem_raw + g.a);
+    V* tws = reinterpret_cast<V*>(smem_raw + g.a + g.b);
+    RowPtr* rt = reinterpret_cast<RowPtr*>(smem_raw + g.a + g.b + g.tw);
+    RowPtr* re = rt + 2 * P;
+    double* rmean = reinterpret_cast<double*>(re + 2 * P);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const long long nrows = 6LL * I.rows, npairs = nrows / 2;
+    const long long plane_row = (long long)o * I.rows + (long long)z * n1;
+    const long long row0 = plane_row + (long long)rank * g.Rc;
+    const long long p0 = row0 / 2;
+    const int lbv = (int)(p0 / P);
+    constexpr bool MEAN64 = sizeof(T) == 4;
+    for (int r = tid; r < 2 * P; r += nt) {
+        T *pd, *qd;
+        dst_rows(I, out, RD_STRESS, row0 + r, pd, qd);
+        RowPtr e, ep;
+        e.p = pd - out;
+        e.q = qd - out;
+        ep.p = ep.q = -1;
+        rt[r] = e;
+        re[r] = ep;
+        rmean[r] = MEAN64 ? mean_stress(I, sbar + 9 * ii, o) : 0.0;
+    }
+    stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
+    const V* src = spec + I.spoff + plane_row * I.nhp;
+    for (int e = tid; e < n1 * W; e += nt) {
+        const int ky = e >> lgw, w = e & (W - 1);
+        const V* sr = src + (long long)ky * I.nhp;
+        V v;
+        if (rank == 0 && w == 0) {
+            // the Hermitian parts of columns 0 and nl/2 along axis 1: their inverse transforms are
+            // the real parts the C2R keeps (the k tables' positive Nyquist values make the k-space
+            // operator's output not exactly Hermitian on the axis-1 Nyquist line)
+            const V* sm = src + (long long)((ky == 0) ? 0 : n1 - ky) * I.nhp;
+            const V f0 = sr[0], f0m = sm[0], fn = sr[N / 2], fnm = sm[N / 2];
+            const T ax = (T)0.5 * (f0.x + f0m.x), ay = (T)0.5 * (f0.y - f0m.y);
+            const T bx = (T)0.5 * (fn.x + fnm.x), by = (T)0.5 * (fn.y - fnm.y);
+            v.x = ax - by;
+            v.y = ay + bx;
+        } else {
+            v = sr[rank * W + w];
+        }
+        s_col[e] = v;
+    }
+    __syncthreads();
+    SColT<V, 1> col{s_col, lgw, 0}, scr{s_own, lgw, 0};
+    fft_io<V, true, 1>(col, scr, scr, col, lgw, I.lp_mid, tw, tid, nt, 0);
+    cl.sync();   // every block's columns are transformed
+    {
+        const int lh = 31 - __clz(N / 2);    // N / 2 is a power of two
+        for (int e = tid; e < g.Rc * (N / 2); e += nt) {
+            const int ly = e >> lh, kx = e & (N / 2 - 1);
+            const int srcb = kx >> lgw, w = kx & (W - 1);
+            const V v = cl.map_shared_rank(s_col, srcb)[((rank * g.Rc + ly) << lgw) + w];
+            V* d = s_own + ly * ldo;
+            if (kx == 0) {
+                V a, b;
+                a.x = v.x; a.y = 0;
+                b.x = v.y; b.y = 0;
+                d[0] = a;
+                d[N / 2] = b;
+            } else {
+                d[kx] = v;
+            }
+        }
+    }
+    cl.sync();   // no block reads another's S_col from here on; S_own is complete
+    {
+        const LinePlan& lq = I.lp_last;
+        const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
+        if (lq.radix[0] == 16 && lq.radix[1] == 16)
+            c2r_rows_io<T, MEAN64, 16, 16>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
+                                           nrows, npairs, tid, nt, p0, ldo);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 8)
+            c2r_rows_io<T, MEAN64, 16, 8>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
+                                          nrows, npairs, tid, nt, p0, ldo);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 4)
+            c2r_rows_io<T, MEAN64, 16, 4>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
+                                          nrows, npairs, tid, nt, p0, ldo);
+        else
+            c2r_rows_io<T, MEAN64, 8, 4>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
+                                         nrows, npairs, tid, nt, p0, ldo);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // FP32 plans: FP64 mean of each beta component from the row sums. One cluster of MEAN_SPLIT blocks
 // per (instance, component): each block sums a contiguous share of the rows (fixed-order strided
 // sums and a fixed tree), block 0 of the cluster adds the shares from the blocks' shared memory
@@ -1197,37 +1490,65 @@ k_mean_beta(const InstDev* __restrict__ insts, const double* __restrict__ rowsum
 // ------------------------------------------------------------------------------------------
 // Host launch sequence
 // ------------------------------------------------------------------------------------------
+// u != null: beta holds the stage-1 rhs and the stress is that of F0 = u + dt rhs, which is formed
+// in place first (the plane instances' forward pass forms it while transforming; the others by the
+// axpy kernel, which skips the plane instances).
 template <typename T>
-static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, void* phi, cudaStream_t st) {
+static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, void* phi, cudaStream_t st,
+                              const void* u = nullptr) {
     typedef typename VecOf<T>::type V;
     const bool f32 = (P.precision == CDD_F32);
     V* spec = (V*)P.d_spec;
     const V* tw = (const V*)P.d_tw;
     const LaunchShape* L = P.pass;
+    // instances with the fused plane passes (FP32 only) skip the separate row and axis-1 passes
+    const bool plane = std::is_same<T, float>::value && P.plane.blocks > 0;
+    const LaunchShape* LR = plane ? P.rest : P.pass;
+    if (u && LR[PASS_R2C].blocks > 0) {   // some instance forms F0 by the axpy kernel
+        cudaError_t e = launch_axpy_f0(P, u, const_cast<void*>(beta), st);
+        if (e != cudaSuccess) return e;
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        if (plane && u)
+            k_plane_fwd<T, true><<<P.plane.blocks, P.plane.threads, P.plane.smem, st>>>(
+                P.d_inst, P.n_inst, P.plane.d_pre, (const T*)beta, spec, tw, P.d_rowsum, (T*)beta, (const T*)u,
+                P.d_clock);
+        else if (plane)
+            k_plane_fwd<T, false><<<P.plane.blocks, P.plane.threads, P.plane.smem, st>>>(
+                P.d_inst, P.n_inst, P.plane.d_pre, (const T*)beta, spec, tw, P.d_rowsum, nullptr, nullptr, nullptr);
+    }
     if (f32) {
-        k_r2c_rows<T, true><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM, 6);
+        if (LR[PASS_R2C].blocks > 0)
+            k_r2c_rows<T, true><<<LR[PASS_R2C].blocks, LR[PASS_R2C].threads, LR[PASS_R2C].smem, st>>>(
+                P.d_inst, P.n_inst, LR[PASS_R2C].d_pre, (const T*)beta, spec, tw, P.d_rowsum, RS_SYM, 6);
         k_mean_beta<<<dim3(P.n_inst, 6, MEAN_SPLIT), 1024, 0, st>>>(P.d_inst, P.d_rowsum, P.d_sbar);
     } else {
         k_r2c_rows<T, false><<<L[PASS_R2C].blocks, L[PASS_R2C].threads, L[PASS_R2C].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_R2C].d_pre, (const T*)beta, spec, tw, nullptr, RS_SYM, 6);
     }
-    if (L[PASS_MID_F].blocks > 0)
-        k_fft_mid<T, false><<<L[PASS_MID_F].blocks, L[PASS_MID_F].threads, L[PASS_MID_F].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6, 0);
+    if (LR[PASS_MID_F].blocks > 0)
+        k_fft_mid<T, false><<<LR[PASS_MID_F].blocks, LR[PASS_MID_F].threads, LR[PASS_MID_F].smem, st>>>(
+            P.d_inst, P.n_inst, LR[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, 6, 0);
     if (f32)
         k_green<T, true, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr, nullptr);
     else
         k_green<T, false, 0><<<L[PASS_GREEN].blocks, L[PASS_GREEN].threads, L[PASS_GREEN].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_GREEN].d_pre, spec, tw, (const T*)P.d_k, (V*)phi, nullptr, nullptr);
-    if (L[PASS_MID_I].blocks > 0)
-        k_fft_mid<T, true><<<L[PASS_MID_I].blocks, L[PASS_MID_I].threads, L[PASS_MID_I].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6, 0);
-    if (f32)
-        k_c2r_rows<T, true><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
-            P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS, 6, nullptr, EPI_NONE, nullptr);
-    else
+    if (LR[PASS_MID_I].blocks > 0)
+        k_fft_mid<T, true><<<LR[PASS_MID_I].blocks, LR[PASS_MID_I].threads, LR[PASS_MID_I].smem, st>>>(
+            P.d_inst, P.n_inst, LR[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, 6, 0);
+    if constexpr (std::is_same<T, float>::value) {
+        if (plane)
+            k_plane_inv<T><<<P.plane.blocks, P.plane.threads, P.plane.smem, st>>>(
+                P.d_inst, P.n_inst, P.plane.d_pre, spec, (T*)sigma, tw, P.d_sbar);
+    }
+    if (f32) {
+        if (LR[PASS_C2R].blocks > 0)
+            k_c2r_rows<T, true><<<LR[PASS_C2R].blocks, LR[PASS_C2R].threads, LR[PASS_C2R].smem, st>>>(
+                P.d_inst, P.n_inst, LR[PASS_C2R].d_pre, spec, (T*)sigma, tw, P.d_sbar, RD_STRESS, 6, nullptr,
+                EPI_NONE, nullptr);
+    } else
         k_c2r_rows<T, false><<<L[PASS_C2R].blocks, L[PASS_C2R].threads, L[PASS_C2R].smem, st>>>(
             P.d_inst, P.n_inst, L[PASS_C2R].d_pre, spec, (T*)sigma, tw, nullptr, RD_STRESS, 6, nullptr, EPI_NONE, nullptr);
     return cudaGetLastError();
@@ -1350,9 +1671,20 @@ cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cuda
     return run_stress<double>(P, beta, sigma, phi, st);
 }
 
+cudaError_t launch_stress_f0(const PlanCore& P, const void* u, void* rhs_f0, void* sigma, cudaStream_t st,
+                             void* phi) {
+    if (P.precision == CDD_F32) return run_stress<float>(P, rhs_f0, sigma, phi, st, u);
+    return run_stress<double>(P, rhs_f0, sigma, phi, st, u);
+}
+
 template <typename T>
 static cudaError_t set_attr_t(size_t smem) {
     cudaError_t e;
+    if constexpr (std::is_same<T, float>::value) {
+        if ((e = set_dyn_smem_limit(k_plane_fwd<T, false>, smem))) return e;
+        if ((e = set_dyn_smem_limit(k_plane_fwd<T, true>, smem))) return e;
+        if ((e = set_dyn_smem_limit(k_plane_inv<T>, smem))) return e;
+    }
     if ((e = set_dyn_smem_limit(k_r2c_rows<T, true>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_r2c_rows<T, false>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_c2r_rows<T, true>, smem))) return e;

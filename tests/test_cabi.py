@@ -83,13 +83,14 @@ def test_tuning_struct_layout_matches_ctypes(tmp_path):
     from cdd import _lib
     src = tmp_path / "tlayout.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\n'
-                   'int main(void){printf("%%zu %%zu %%zu\\n", sizeof(cdd_tuning),'
-                   'offsetof(cdd_tuning, green_cols), offsetof(cdd_tuning, stencil_planes)); return 0;}\n' % HEADER)
+                   'int main(void){printf("%%zu %%zu %%zu %%zu\\n", sizeof(cdd_tuning),'
+                   'offsetof(cdd_tuning, green_cols), offsetof(cdd_tuning, stencil_planes),'
+                   'offsetof(cdd_tuning, plane_fft)); return 0;}\n' % HEADER)
     exe = tmp_path / "tlayout"
     subprocess.run(["gcc", "-std=c99", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     S = _lib.cdd_tuning
-    assert got == [ctypes.sizeof(S), S.green_cols.offset, S.stencil_planes.offset]
+    assert got == [ctypes.sizeof(S), S.green_cols.offset, S.stencil_planes.offset, S.plane_fft.offset]
 
 
 def test_tuned_plan_rejects_bad_tuning_before_device_work():
@@ -101,7 +102,7 @@ def test_tuned_plan_rejects_bad_tuning_before_device_work():
         inst.shape[a] = 16
     inst.mu, inst.nu, inst.cfl = 1.0, 0.3, 0.25
     for bad in [dict(fft_radix=32), dict(fft_radix=2), dict(mid_cols=12), dict(green_cols=128),
-                dict(rows_lines=5000), dict(stencil_planes=-1)]:
+                dict(rows_lines=5000), dict(stencil_planes=-1), dict(plane_fft=2), dict(plane_fft=-2)]:
         t = _lib.cdd_tuning.from_dict(bad)
         h = ctypes.c_void_p()
         rc = lib.cdd_plan_create_tuned(ctypes.byref(inst), 1, _lib.CDD_F64, ctypes.byref(t), ctypes.byref(h))
