@@ -263,7 +263,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (p->tune[i].plane_fft == 1 && !ok)
                 return fail(CDD_ERR_ARG, "instance %d: tuning plane_fft 1, but the shape or precision does not allow "
                                          "the fused plane passes", i);
-            I.plane = (ok && p->tune[i].plane_fft >= 0) ? 1 : 0;
+            I.plane = (ok && p->tune[i].plane_fft == 1) ? 1 : 0;   // built-in: the separate passes (faster)
             p->tune[i].plane_fft = (I.nd == 3 && C.precision == CDD_F32) ? (I.plane ? 1 : -1) : 0;
             pre_plane.push_back(pre_plane.back() + (I.plane ? 6 * I.n0 * PLANE_CLUSTER : 0));
             for (int k = 0; k < NUM_PASSES; ++k) pre_rest[k].push_back(pre_rest[k].back() + (I.plane ? 0 : I.tile[k].blocks));

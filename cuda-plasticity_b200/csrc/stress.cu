@@ -43,6 +43,15 @@ __device__ __forceinline__ void load4(const double* p, double* v) {
     double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
+// The same through the coherent path (data the kernel also writes).
+__device__ __forceinline__ void load4c(const float* p, float* v) {
+    float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void load4c(const double* p, double* v) {
+    double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
 __device__ __forceinline__ void store4(float* p, const float* v) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
@@ -134,14 +143,25 @@ __device__ __forceinline__ T row_value(const T* __restrict__ beta, T* f0w, const
     }
 }
 
-template <typename T, bool MEAN64, int R0, int R1, bool F0 = false>
+// Where the row pass puts the two half spectra a (row 2q) and b (row 2q + 1) at bin k of the q-th
+// line pair of the block (q = p - p0): rows of dst, dld apart.
+template <typename V> struct RowSink {
+    V* dst;
+    int dld;
+    __device__ __forceinline__ void operator()(long long q, int k, const V& a, const V& b, bool hasb) const {
+        V* da = dst + 2 * q * dld;
+        da[k] = a;
+        if (hasb) da[dld + k] = b;
+    }
+};
+
+template <typename T, bool MEAN64, int R0, int R1, bool F0, class Sink>
 __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int ld, const RowPtr* __restrict__ rt,
                                             const T* __restrict__ beta, typename VecOf<T>::type* s,
                                             const typename VecOf<T>::type* __restrict__ tw1,
-                                            typename VecOf<T>::type* __restrict__ dst, double* __restrict__ rowsum,
+                                            const Sink& out, double* __restrict__ rowsum,
                                             long long nrows, long long npairs, int tid, int nt,
-                                            long long p0, int dld, T* f0w = nullptr, const T* u = nullptr,
-                                            T dt = 0) {
+                                            long long p0, T* f0w = nullptr, const T* u = nullptr, T dt = 0) {
     typedef typename VecOf<T>::type V;
     // stage 0 (span 1): butterfly (l, j) takes elements j + R1 r of pair line l
 #pragma unroll 1
@@ -195,7 +215,6 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
         const long long p = (long long)lb * P + l;
         const bool valid = p < npairs;
         const bool hasb = 2 * p + 1 < nrows;
-        V* da = dst + 2 * (p - p0) * dld;
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
             V zs;
@@ -210,8 +229,7 @@ __device__ __forceinline__ void r2c_rows_io(const InstDev& I, int lb, int P, int
                 a.y = (T)0.5 * (zk.y - zm.y);
                 b.x = (T)0.5 * (zk.y + zm.y);
                 b.y = (T)-0.5 * (zk.x - zm.x);
-                da[k] = a;
-                if (hasb) da[dld + k] = b;
+                out(p - p0, k, a, b, hasb);
             }
         }
     }
@@ -269,8 +287,8 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_r2c_row
         const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
 #define CDD_R2C_IO(A, B)                                                                                      \
         if (io && lq.radix[0] == A && lq.radix[1] == B) {                                                     \
-            r2c_rows_io<T, MEAN64, A, B>(I, lb, P, ld, rt, beta, s, tw1, spec + I.spoff, rowsum, nrows, npairs,  \
-                                          tid, nt, 0, I.nhp);                                                 \
+            r2c_rows_io<T, MEAN64, A, B, false>(I, lb, P, ld, rt, beta, s, tw1, RowSink<V>{spec + I.spoff, I.nhp}, \
+                                                 rowsum, nrows, npairs, tid, nt, 0);                          \
             return;                                                                                           \
         }
         CDD_ROWIO_SEQS(CDD_R2C_IO)
@@ -287,18 +305,18 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_r2c_row
             const RowPtr ea = rt[2 * pl], eb = rt[2 * pl + 1];
             T a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
             if (ea.p >= 0) {
-                T u[4], v[4];
-                load4(beta + ea.p + idx, u);
-                load4(beta + ea.q + idx, v);
+                T x[4], y[4];
+                load4(beta + ea.p + idx, x);
+                load4(beta + ea.q + idx, y);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = half * (u[q] + v[q]);
+                for (int q = 0; q < 4; ++q) a[q] = half * (x[q] + y[q]);
             }
             if (eb.p >= 0) {
-                T u[4], v[4];
-                load4(beta + eb.p + idx, u);
-                load4(beta + eb.q + idx, v);
+                T x[4], y[4];
+                load4(beta + eb.p + idx, x);
+                load4(beta + eb.q + idx, y);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) b[q] = half * (u[q] + v[q]);
+                for (int q = 0; q < 4; ++q) b[q] = half * (x[q] + y[q]);
             }
             V* d = s + pl * ld + row_pad(idx);
 #pragma unroll
@@ -399,14 +417,6 @@ __device__ __forceinline__ void dst_rows(const InstDev& I, T* base, int mode, lo
 }
 
 // out -= coef (beta[e.p + idx ..] - beta[e.q + idx ..]) for four (epilogue4) or one value.
-__device__ __forceinline__ void load4c(const float* p, float* v) {
-    float4 q = *reinterpret_cast<const float4*>(p);
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-}
-__device__ __forceinline__ void load4c(const double* p, double* v) {
-    double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
 template <typename T>
 __device__ __forceinline__ void epilogue4(const T* beta, const RowPtr& e, T coef, int idx, T* v) {
     T a[4], b[4] = {0, 0, 0, 0};
@@ -1172,28 +1182,36 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
 }
 
 // ------------------------------------------------------------------------------------------
-// Plane passes (3-D FP32 instances that plane_layout accepts): the transforms along the contiguous
-// axis and along axis 1 of one z-plane of one component in one kernel, so the spectrum crosses HBM
-// once between them instead of twice. One cluster of PLANE_C blocks per (component o, plane z):
-//   forward: block r runs the R2C of rows [r Rc, (r+1) Rc) of the plane (two real rows per complex
-//     FFT, as k_r2c_rows) into its shared tile S_own (Rc rows of nh half-spectrum values); after a
-//     cluster barrier it gathers spectrum columns [r W, (r+1) W) of all n1 rows from the blocks'
-//     tiles through distributed shared memory into S_col, transforms them along axis 1 and writes
-//     them to the plan's spectrum, which the k-space pass (k_green) reads as before;
-//   inverse: the mirror image: block r loads columns [r W, (r+1) W) of the plane's spectrum,
-//     inverts the axis-1 transform, gathers rows [r Rc, (r+1) Rc) of all columns from the blocks'
-//     tiles and runs the C2R of those rows (plus the FP64 mean stress) into sigma.
+// Plane passes (3-D FP32 instances that plane_eligible accepts): the transforms along the
+// contiguous axis and along axis 1 of one z-plane of one component in one kernel each way, so the
+// spectrum crosses HBM once between them instead of twice. One cluster of PLANE_C blocks per
+// (component o, plane z); block r owns rows [r Rc, (r+1) Rc) of the plane (Rc = n1 / PLANE_C) and
+// spectrum columns [r W, (r+1) W) (W = nl / (2 PLANE_C)). Data moves between the blocks of a
+// cluster by stores into the owner's shared memory (distributed shared memory), which do not stall
+// the storing thread:
+//   forward: block r runs the R2C of its rows (two real rows per complex FFT, as k_r2c_rows); the
+//     last FFT stage stores each half-spectrum bin straight into the shared column tile S_col of
+//     the block that owns its column; after a cluster barrier every block transforms its W columns
+//     along axis 1 and writes them to the plan's spectrum, which the k-space pass (k_green) reads
+//     as before;
+//   inverse: block r runs the inverse axis-1 transform of its W columns, the first stage reading
+//     them from the spectrum and the last stage storing each value into the shared row tile S_own
+//     of the block that owns its row; after a cluster barrier every block runs the C2R of its rows
+//     (plus the FP64 mean stress) into sigma.
+// Every kernel starts with a cluster barrier, so no block stores into a block that has not started.
 // Columns 0 and nl/2 of a row's half spectrum are real (the R2C split makes their imaginary parts
 // exactly zero), so block 0 carries them as one complex column X0 + i X_{nl/2}; its axis-1
 // transform F = F0 + i FN is split again by Hermitian symmetry, F0(ky) = (F(ky) + conj F(-ky)) / 2,
 // FN(ky) = (F(ky) - conj F(-ky)) / (2i). The inverse packs the Hermitian parts H(G)(ky) =
 // (G(ky) + conj G(-ky)) / 2 of the two columns as H(G0) + i H(GN): the inverse transform of H(G) is
-// the real part of that of G, which is what the C2R keeps of those bins (numpy's irfft semantics).
-// That keeps W = nl / (2 PLANE_C) columns per block, a power of two. Same codelets, twiddles and
-// row tables as the separate passes; results agree with them to rounding.
-// Shared memory (V = complex): region A = S_own (Rc x ldo) or the axis-1 scratch tile (n1 x W);
-// region B = the row pass's line buffer (P x rows_ld(nl)) or S_col (n1 x W); the row twiddles;
-// the row tables. Regions are reused only across block or cluster barriers.
+// the real part of that of G, which is what the C2R keeps of those bins (numpy's irfft semantics;
+// the k tables' positive Nyquist values make the k-space operator's output not exactly Hermitian
+// on the axis-1 Nyquist line). That keeps W columns per block, a power of two. Same codelets,
+// twiddles and row tables as the separate passes; results agree with them to rounding.
+// Shared memory (V = complex): forward: the row pass's line buffer (P x rows_ld(nl); then the
+// axis-1 scratch tile, n1 x W) and S_col (n1 x W); inverse: S_own (Rc x ldo) and a buffer of
+// max(n1 x W, P x rows_ld(nl)) (the axis-1 scratch tile, then the C2R line buffer); both: the row
+// twiddles and the row tables.
 // ------------------------------------------------------------------------------------------
 constexpr int PLANE_C = PLANE_CLUSTER;
 
@@ -1214,8 +1232,12 @@ __host__ __device__ inline PlaneGeom plane_geom(const InstDev& I, size_t velt) {
     auto r16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
     const size_t colt = (size_t)I.n1 * g.W * velt;
     const size_t own = (size_t)g.Rc * g.ldo * velt, line = (size_t)g.P * g.ld * velt;
-    g.a = r16(own > colt ? own : colt);
-    g.b = r16(line > colt ? line : colt);
+    // region a: forward line buffer / axis-1 scratch, inverse S_own; region b: forward S_col,
+    // inverse axis-1 scratch / C2R line buffer
+    const size_t fa = line > colt ? line : colt, ia = own;
+    const size_t fb = colt, ib = line > colt ? line : colt;
+    g.a = r16(fa > ia ? fa : ia);
+    g.b = r16(fb > ib ? fb : ib);
     g.tw = r16((size_t)I.lp_last.twspan * velt);
     g.tab = r16(rows_table_bytes(g.P));
     g.total = g.a + g.b + g.tw + g.tab;
@@ -1238,6 +1260,97 @@ bool plane_eligible(const InstDev& I, int precision, size_t smem_limit) {
 
 size_t plane_smem_bytes(const InstDev& I) { return plane_geom(I, sizeof(float2)).total; }
 
+// Forward: bin k of rows y0 + 2q and y0 + 2q + 1 of the plane goes to the column tile S_col of the
+// block owning column k (element (y, w) at (y << lgw) + w); bins 0 and nl/2 (real) to the real and
+// imaginary parts of block 0's column 0.
+template <typename V> struct PlaneColSink {
+    V* s_col;   // this block's S_col (the same offset in every block of the cluster)
+    int y0, lgw, half;
+    __device__ __forceinline__ void operator()(long long q, int k, const V& a, const V& b, bool) const {
+        cg::cluster_group cl = cg::this_cluster();
+        const int y = y0 + 2 * (int)q;
+        if (k == 0 || k == half) {
+            V* d = cl.map_shared_rank(s_col, 0);
+            if (k == 0) {
+                d[y << lgw].x = a.x;
+                d[(y + 1) << lgw].x = b.x;
+            } else {
+                d[y << lgw].y = a.x;
+                d[(y + 1) << lgw].y = b.x;
+            }
+        } else {
+            const int w = k & ((1 << lgw) - 1);
+            V* d = cl.map_shared_rank(s_col, k >> lgw);
+            d[(y << lgw) + w] = a;
+            d[((y + 1) << lgw) + w] = b;
+        }
+    }
+};
+
+// Inverse, first axis-1 stage: element ky of column w of this block read from the spectrum; block
+// 0's column 0 is H(G0) + i H(GN) of spectrum columns 0 and nl/2.
+template <typename V> struct PlaneSpecIn {
+    const V* src;   // the plane's first spectrum row, at this block's first column
+    long long nhp;
+    int n1, half;
+    bool packed;    // block 0: column 0 carries bins 0 and nl/2
+    struct Walk {
+        const V* p;       // element i0 of the column
+        const V* base;    // row 0 of the plane at column 0 (packed column)
+        long long stride, nhp;
+        int i0, step, n1, half;
+        bool packed;
+        __device__ __forceinline__ V ld(int r) const {
+            if (!packed) return p[r * stride];
+            typedef decltype(V().x) T;
+            const int ky = i0 + r * step, km = ky == 0 ? 0 : n1 - ky;
+            const V* sr = base + (long long)ky * nhp;
+            const V* sm = base + (long long)km * nhp;
+            const V f0 = sr[0], f0m = sm[0], fn = sr[half], fnm = sm[half];
+            const T ax = (T)0.5 * (f0.x + f0m.x), ay = (T)0.5 * (f0.y - f0m.y);
+            const T bx = (T)0.5 * (fn.x + fnm.x), by = (T)0.5 * (fn.y - fnm.y);
+            V v;
+            v.x = ax - by;
+            v.y = ay + bx;
+            return v;
+        }
+    };
+    __device__ __forceinline__ Walk walk(int l, int i0, int step) const {
+        return {src + (long long)i0 * nhp + l, src, (long long)step * nhp, nhp, i0, step, n1, half, packed && l == 0};
+    }
+};
+
+// Inverse, last axis-1 stage: element y of column w stored into the row tile S_own of the block
+// owning row y (row ly at ly * ldo); block 0's column 0 is unpacked into bins 0 and nl/2 (real).
+template <typename V> struct PlaneRowOut {
+    V* s_own;
+    int col0, lrc, ldo, half;
+    bool packed;
+    struct Walk {
+        V* s_own;
+        int i0, step, kx, lrc, ldo, half;
+        bool packed;
+        __device__ __forceinline__ void st(int r, V v) const {
+            cg::cluster_group cl = cg::this_cluster();
+            const int y = i0 + r * step;
+            const int q = y >> lrc, ly = y & ((1 << lrc) - 1);
+            V* d = cl.map_shared_rank(s_own, q) + ly * ldo;
+            if (packed) {
+                V a, b;
+                a.x = v.x; a.y = 0;
+                b.x = v.y; b.y = 0;
+                d[0] = a;
+                d[half] = b;
+            } else {
+                d[kx] = v;
+            }
+        }
+    };
+    __device__ __forceinline__ Walk walk(int l, int i0, int step) const {
+        return {s_own, i0, step, col0 + l, lrc, ldo, half, packed && l == 0};
+    }
+};
+
 // F0: beta holds the stage-1 rhs; the kernel forms F0 = u + dt rhs row by row (dt from the
 // instance's clock), writes it back over rhs and transforms it (see r2c_rows_io).
 template <typename T, bool F0>
@@ -1248,6 +1361,7 @@ k_plane_fwd(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cl = cg::this_cluster();
+    cl.sync();   // every block of the cluster runs before any stores into another
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
@@ -1255,8 +1369,8 @@ k_plane_fwd(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
     const int q = lb / PLANE_C;              // o * n0 + z
     const int o = q / I.n0, z = q - o * I.n0;
     const PlaneGeom g = plane_geom(I, sizeof(V));
-    const int N = I.nl, n1 = I.n1, W = g.W, lgw = g.lgw, ldo = g.ldo, P = g.P;
-    V* s_own = reinterpret_cast<V*>(smem_raw);
+    const int N = I.nl, n1 = I.n1, W = g.W, lgw = g.lgw, P = g.P;
+    V* s_line = reinterpret_cast<V*>(smem_raw);            // line buffer, then the axis-1 scratch tile
     V* s_col = reinterpret_cast<V*>(smem_raw + g.a);
     V* tws = reinterpret_cast<V*>(smem_raw + g.a + g.b);
     RowPtr* rt = reinterpret_cast<RowPtr*>(smem_raw + g.a + g.b + g.tw);
@@ -1281,38 +1395,18 @@ k_plane_fwd(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
         const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
         constexpr bool MEAN64 = sizeof(T) == 4;
         const T dt = F0 ? (T)clk[ii].dt : (T)0;
-        if (lq.radix[0] == 16 && lq.radix[1] == 16)
-            r2c_rows_io<T, MEAN64, 16, 16, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
-                                               tid, nt, p0, ldo, f0w, u, dt);
-        else if (lq.radix[0] == 16 && lq.radix[1] == 8)
-            r2c_rows_io<T, MEAN64, 16, 8, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
-                                              tid, nt, p0, ldo, f0w, u, dt);
-        else if (lq.radix[0] == 16 && lq.radix[1] == 4)
-            r2c_rows_io<T, MEAN64, 16, 4, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
-                                              tid, nt, p0, ldo, f0w, u, dt);
-        else
-            r2c_rows_io<T, MEAN64, 8, 4, F0>(I, lbv, P, g.ld, rt, beta, s_col, tw1, s_own, rowsum, nrows, npairs,
-                                             tid, nt, p0, ldo, f0w, u, dt);
+        const PlaneColSink<V> sink{s_col, rank * g.Rc, lgw, N / 2};
+#define CDD_PLANE_R2C(A, B)                                                                                 \
+        r2c_rows_io<T, MEAN64, A, B, F0>(I, lbv, P, g.ld, rt, beta, s_line, tw1, sink, rowsum, nrows, npairs, \
+                                         tid, nt, p0, f0w, u, dt)
+        if (lq.radix[0] == 16 && lq.radix[1] == 16) CDD_PLANE_R2C(16, 16);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 8) CDD_PLANE_R2C(16, 8);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 4) CDD_PLANE_R2C(16, 4);
+        else CDD_PLANE_R2C(8, 4);
+#undef CDD_PLANE_R2C
     }
-    cl.sync();   // every block's half spectra are in its S_own
-    {
-        const int lrc = 31 - __clz(g.Rc);   // Rc is a power of two
-        for (int e = tid; e < n1 * W; e += nt) {
-            const int y = e >> lgw, w = e & (W - 1);
-            const int src = y >> lrc, ly = y - (src << lrc);
-            const V* so = cl.map_shared_rank(s_own, src) + ly * ldo;
-            V v;
-            if (rank == 0 && w == 0) {
-                v.x = so[0].x;
-                v.y = so[N / 2].x;
-            } else {
-                v = so[rank * W + w];
-            }
-            s_col[e] = v;
-        }
-    }
-    cl.sync();   // no block reads another's S_own from here on
-    SColT<V, 1> col{s_col, lgw, 0}, scr{s_own, lgw, 0};
+    cl.sync();   // every half-spectrum bin of the plane is in its owner's S_col
+    SColT<V, 1> col{s_col, lgw, 0}, scr{s_line, lgw, 0};
     fft_io<V, false, 1>(col, scr, scr, col, lgw, I.lp_mid, tw, tid, nt, 0);
     V* dst = spec + I.spoff + plane_row * I.nhp;
     for (int e = tid; e < n1 * W; e += nt) {
@@ -1343,6 +1437,7 @@ k_plane_inv(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
     typedef typename VecOf<T>::type V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cg::cluster_group cl = cg::this_cluster();
+    cl.sync();   // every block of the cluster runs before any stores into another
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
     const int lb = blockIdx.x - pre[ii];
@@ -1350,9 +1445,9 @@ k_plane_inv(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
     const int q = lb / PLANE_C;
     const int o = q / I.n0, z = q - o * I.n0;
     const PlaneGeom g = plane_geom(I, sizeof(V));
-    const int N = I.nl, n1 = I.n1, W = g.W, lgw = g.lgw, ldo = g.ldo, P = g.P;
+    const int N = I.nl, n1 = I.n1, lgw = g.lgw, ldo = g.ldo, P = g.P;
     V* s_own = reinterpret_cast<V*>(smem_raw);
-    V* s_col = reinterpret_cast<V*>(smem_raw + g.a);
+    V* s_buf = reinterpret_cast<V*>(smem_raw + g.a);      // axis-1 scratch tile, then the C2R line buffer
     V* tws = reinterpret_cast<V*>(smem_raw + g.a + g.b);
     RowPtr* rt = reinterpret_cast<RowPtr*>(smem_raw + g.a + g.b + g.tw);
     RowPtr* re = rt + 2 * P;
@@ -1376,64 +1471,24 @@ k_plane_inv(const InstDev* __restrict__ insts, int n_inst, const int* __restrict
         rmean[r] = MEAN64 ? mean_stress(I, sbar + 9 * ii, o) : 0.0;
     }
     stage_tw_to_smem(I.lp_last, tw, tws, tid, nt);
-    const V* src = spec + I.spoff + plane_row * I.nhp;
-    for (int e = tid; e < n1 * W; e += nt) {
-        const int ky = e >> lgw, w = e & (W - 1);
-        const V* sr = src + (long long)ky * I.nhp;
-        V v;
-        if (rank == 0 && w == 0) {
-            // the Hermitian parts of columns 0 and nl/2 along axis 1: their inverse transforms are
-            // the real parts the C2R keeps (the k tables' positive Nyquist values make the k-space
-            // operator's output not exactly Hermitian on the axis-1 Nyquist line)
-            const V* sm = src + (long long)((ky == 0) ? 0 : n1 - ky) * I.nhp;
-            const V f0 = sr[0], f0m = sm[0], fn = sr[N / 2], fnm = sm[N / 2];
-            const T ax = (T)0.5 * (f0.x + f0m.x), ay = (T)0.5 * (f0.y - f0m.y);
-            const T bx = (T)0.5 * (fn.x + fnm.x), by = (T)0.5 * (fn.y - fnm.y);
-            v.x = ax - by;
-            v.y = ay + bx;
-        } else {
-            v = sr[rank * W + w];
-        }
-        s_col[e] = v;
-    }
-    __syncthreads();
-    SColT<V, 1> col{s_col, lgw, 0}, scr{s_own, lgw, 0};
-    fft_io<V, true, 1>(col, scr, scr, col, lgw, I.lp_mid, tw, tid, nt, 0);
-    cl.sync();   // every block's columns are transformed
     {
-        const int lh = 31 - __clz(N / 2);    // N / 2 is a power of two
-        for (int e = tid; e < g.Rc * (N / 2); e += nt) {
-            const int ly = e >> lh, kx = e & (N / 2 - 1);
-            const int srcb = kx >> lgw, w = kx & (W - 1);
-            const V v = cl.map_shared_rank(s_col, srcb)[((rank * g.Rc + ly) << lgw) + w];
-            V* d = s_own + ly * ldo;
-            if (kx == 0) {
-                V a, b;
-                a.x = v.x; a.y = 0;
-                b.x = v.y; b.y = 0;
-                d[0] = a;
-                d[N / 2] = b;
-            } else {
-                d[kx] = v;
-            }
-        }
+        const PlaneSpecIn<V> in{spec + I.spoff + plane_row * I.nhp + rank * g.W, I.nhp, n1, N / 2, rank == 0};
+        const PlaneRowOut<V> rows{s_own, rank * g.W, 31 - __clz(g.Rc), ldo, N / 2, rank == 0};
+        SColT<V, 1> scr{s_buf, lgw, 0};
+        fft_io<V, true, 1>(in, scr, scr, rows, lgw, I.lp_mid, tw, tid, nt, 0);
     }
-    cl.sync();   // no block reads another's S_col from here on; S_own is complete
+    cl.sync();   // every row of every block's S_own is complete; no block reads the scratch tiles
     {
         const LinePlan& lq = I.lp_last;
         const V* tw1 = tws + (lq.twst[1] - lq.twst[0]);
-        if (lq.radix[0] == 16 && lq.radix[1] == 16)
-            c2r_rows_io<T, MEAN64, 16, 16>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
-                                           nrows, npairs, tid, nt, p0, ldo);
-        else if (lq.radix[0] == 16 && lq.radix[1] == 8)
-            c2r_rows_io<T, MEAN64, 16, 8>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
-                                          nrows, npairs, tid, nt, p0, ldo);
-        else if (lq.radix[0] == 16 && lq.radix[1] == 4)
-            c2r_rows_io<T, MEAN64, 16, 4>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
-                                          nrows, npairs, tid, nt, p0, ldo);
-        else
-            c2r_rows_io<T, MEAN64, 8, 4>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_col, tw1, out, nullptr, EPI_NONE,
-                                         nrows, npairs, tid, nt, p0, ldo);
+#define CDD_PLANE_C2R(A, B)                                                                                   \
+        c2r_rows_io<T, MEAN64, A, B>(I, lbv, P, g.ld, rt, re, rmean, s_own, s_buf, tw1, out, nullptr, EPI_NONE, \
+                                     nrows, npairs, tid, nt, p0, ldo)
+        if (lq.radix[0] == 16 && lq.radix[1] == 16) CDD_PLANE_C2R(16, 16);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 8) CDD_PLANE_C2R(16, 8);
+        else if (lq.radix[0] == 16 && lq.radix[1] == 4) CDD_PLANE_C2R(16, 4);
+        else CDD_PLANE_C2R(8, 4);
+#undef CDD_PLANE_C2R
     }
 }
 
@@ -1490,9 +1545,10 @@ k_mean_beta(const InstDev* __restrict__ insts, const double* __restrict__ rowsum
 // ------------------------------------------------------------------------------------------
 // Host launch sequence
 // ------------------------------------------------------------------------------------------
-// u != null: beta holds the stage-1 rhs and the stress is that of F0 = u + dt rhs, which is formed
-// in place first (the plane instances' forward pass forms it while transforming; the others by the
-// axpy kernel, which skips the plane instances).
+// u != null: beta holds the stage-1 rhs and the stress is that of F0 = u + dt rhs, formed in place
+// first: by the plane instances' forward pass while it transforms the rows (fused), by the axpy
+// kernel for the others (it skips the plane instances). A fused F0 in the separate row pass was
+// measured slower: its write-back of F0 orders each row load after the previous store.
 template <typename T>
 static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, void* phi, cudaStream_t st,
                               const void* u = nullptr) {
@@ -1504,7 +1560,7 @@ static cudaError_t run_stress(const PlanCore& P, const void* beta, void* sigma, 
     // instances with the fused plane passes (FP32 only) skip the separate row and axis-1 passes
     const bool plane = std::is_same<T, float>::value && P.plane.blocks > 0;
     const LaunchShape* LR = plane ? P.rest : P.pass;
-    if (u && LR[PASS_R2C].blocks > 0) {   // some instance forms F0 by the axpy kernel
+    if (u && LR[PASS_R2C].blocks > 0) {   // the other instances form F0 with the axpy kernel first
         cudaError_t e = launch_axpy_f0(P, u, const_cast<void*>(beta), st);
         if (e != cudaSuccess) return e;
     }

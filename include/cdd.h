@@ -96,10 +96,10 @@ typedef struct cdd_tuning {
     int mid_cols;         /* axis-1 FFT pass (3-D): spectrum columns per block (power of two) */
     int green_cols;       /* fused axis-0 FFT + Green pass: spectrum columns per block (power of two) */
     int stencil_planes;   /* stencil (3-D): planes marched per block along axis 0 */
-    int plane_fft;        /* stress transforms of 3-D FP32 instances: 0 (built-in) or 1 fuse the
-                             contiguous-axis and axis-1 passes of each z-plane into one cluster
-                             kernel each way where the shape allows it (1: required, CDD_ERR_ARG
-                             when it does not), -1 keeps the separate passes */
+    int plane_fft;        /* stress transforms of 3-D FP32 instances: 1 fuses the contiguous-axis
+                             and axis-1 passes of each z-plane into one cluster kernel each way
+                             (CDD_ERR_ARG when the shape does not allow it); 0 (built-in) or -1
+                             keep the separate passes, which measure faster on B200 */
 } cdd_tuning;
 
 /* Create a plan for n_inst instances at the given precision on the current CUDA device.

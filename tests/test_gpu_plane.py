@@ -1,6 +1,7 @@
-"""The fused plane passes of the FP32 stress solve (k_plane_fwd / k_plane_inv: the contiguous-axis
-and axis-1 transforms of each z-plane in one cluster kernel each way, spectra exchanged through
-distributed shared memory) against the separate row / axis-1 passes and the CPU oracle."""
+"""The fused plane passes of the FP32 stress solve (tuning plane_fft = 1; k_plane_fwd / k_plane_inv:
+the contiguous-axis and axis-1 transforms of each z-plane in one cluster kernel each way, spectra
+exchanged through distributed shared memory) against the separate row / axis-1 passes (the
+built-in choice) and the CPU oracle, and the stage-2 forward pass that forms F0 = u + dt rhs in both."""
 import numpy as np
 import pytest
 
@@ -61,13 +62,14 @@ def test_mixed_plan_runs_each_instance_like_its_single_plan():
     shapes = [(16, 64, 128), (24, 24, 24), (64, 64), (8, 128, 64)]
     insts = [cdd.Instance(sh, mu=1.0, nu=0.3, cfl=0.25) for sh in shapes]
     fields = [cdd.gaussian_random_field(sh, 0.06, 0.05, 40 + i) for i, sh in enumerate(shapes)]
-    batch = cdd.Plan(insts, "f32")
+    tun = [{"plane_fft": 1}, {}, {}, {"plane_fft": 1}]
+    batch = cdd.Plan(insts, "f32", tuning=tun)
     assert [batch.tuning(i)["plane_fft"] for i in range(4)] == [1, -1, 0, 1]
     bb = batch.pack(fields)
     batch.set_time(0.0, 1e30)
     batch.run(bb, 2, graph=True)
     for i, inst in enumerate(insts):
-        single = cdd.Plan([inst], "f32")
+        single = cdd.Plan([inst], "f32", tuning=[tun[i]])
         bs = single.pack([fields[i]])
         single.set_time(0.0, 1e30)
         single.run(bs, 2, graph=True)
