@@ -63,6 +63,10 @@ __device__ __forceinline__ T mm_sel(T a, T c, int& sel) {
     return same ? (pa ? a : c) : (T)0;
 }
 
+// The limiter arguments in the reference's difference order. The FP32 forward stencil forms e0 and
+// em2 in a packed form that can differ from these in the last bit, so in an exact tie between two
+// limiter arguments the FP32 reverse may take the other branch (the FP32 gradient is checked
+// against the FP64 one, whose forward and reverse use the same differences).
 template <typename T>
 __device__ __forceinline__ void derivs_sel(const T* __restrict__ p, const Nbr& nb, T ih, T& up, T& um,
                                            int& sp, int& sm) {

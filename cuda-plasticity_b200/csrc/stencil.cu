@@ -174,12 +174,20 @@ __device__ __forceinline__ void derivs5(const T* v, T ih, T& up, T& um) {
 //                      + [i < ND] sum_{s,l} Q^s_il (u^s_i)_lj,
 // with c_d = a+_d a-_d / tot_d, i.e. -H / (a_tot b_tot c_tot) + the viscous term of the scalar form.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 derivs5_f2(const float* v, float2 ihh) {
-    const float dm2 = v[1] - v[0], dm1 = v[2] - v[1], d0 = v[3] - v[2], d1 = v[4] - v[3];
-    const float e0 = d1 - d0, em1 = d0 - dm1, em2 = dm1 - dm2;
+// The differences in packed form around the centre c = u_0: P = (u_1, u_-1) - (c, c) = (d0, -dm1),
+// Q = (u_2, u_-2) - (c, c), and the limiter's outer arguments (e0, em2) = Q - 2 P in one packed
+// multiply-add (e0 = d1 - d0 and em2 = dm1 - dm2 up to rounding); the middle one em1 = d0 - dm1 =
+// P.x + P.y and the one-sided derivatives (d0 - dd0 / 2, dm1 + ddm / 2) / h are formed as the
+// scalar form does.
+__device__ __forceinline__ float2 derivs5_f2(const float* v, float ih) {
+    const float2 c2 = f2(v[2], v[2]);
+    const float2 m1 = f2(-1.0f, -1.0f);
+    const float2 P = __ffma2_rn(c2, m1, f2(v[3], v[1]));
+    const float2 Q = __ffma2_rn(c2, m1, f2(v[4], v[0]));
+    const float2 E = __ffma2_rn(P, f2(-2.0f, -2.0f), Q);
     float dd0, ddm;
-    minmod_pair(e0, em1, em2, dd0, ddm);
-    return __fmul2_rn(__ffma2_rn(f2(dd0, ddm), f2(-0.5f, 0.5f), f2(d0, dm1)), ihh);
+    minmod_pair(E.x, P.x + P.y, E.y, dd0, ddm);
+    return __fmul2_rn(__ffma2_rn(f2(dd0, ddm), f2(-0.5f, -0.5f), P), f2(ih, -ih));
 }
 __device__ __forceinline__ float lane(const float2& v, int s) { return s ? v.y : v.x; }
 
@@ -196,7 +204,7 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
         for (int d = 0; d < ND; ++d) {
             float v5[5];
             tv.load5(c, d, v5);
-            U[d][c] = derivs5_f2(v5, f2(ih, ih));
+            U[d][c] = derivs5_f2(v5, ih);
         }
     const float str = lam_on ? (S[0][0] + S[1][1] + S[2][2]) / 3.0f * Lambda : 0.0f;
 
