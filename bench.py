@@ -32,9 +32,9 @@ FLUX_WORDS = 24                 # stencil, flux form: read beta 9 + sigma 6, wri
 FLUX_TRAFFIC_BYTES_PER_CELL = 93.2    # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
 # executed FP32 operations (add + mul + 2 fma, packed pairs counted per lane) and warp instructions
 # per cell of the FP32 flux-form stencil, from ncu's instruction counters at 192^3
-FLUX_FLOP_PER_CELL = 1176.2
-FLUX_WARP_INST_PER_CELL = 44.06
-FLUX_COUNTS_SOURCE = "profiles/k_stencil_flux_flops_192cube.md"
+FLUX_FLOP_PER_CELL = 1338.2
+FLUX_WARP_INST_PER_CELL = 42.23
+FLUX_COUNTS_SOURCE = "profiles/k_stencil_flux_192cube_fp32.md"
 
 
 def parse():

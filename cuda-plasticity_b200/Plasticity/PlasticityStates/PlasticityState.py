@@ -116,23 +116,26 @@ class PlasticityState:
         e = (sq - self.nu / (1.0 + self.nu) * tr * tr) / (4.0 * self.mu)
         return GridArray.GridArray(e.cpu().numpy())
 
-    def _observe(self, kind):
-        """A k-space observable of this state's beta^P on the GPU (cdd.Plan.observe), as host FP64."""
+    @staticmethod
+    def _sin_k(type):
+        if type not in ('k', 'sinK'):
+            raise ValueError("type must be 'k' or 'sinK'")
+        return type == 'sinK'
+
+    def _observe(self, kind, type='k'):
+        """A k-space observable of this state's beta^P on the GPU (cdd.Plan.observe), as host FP64;
+        type 'sinK' uses the sine k tables (FourierSpaceTools(gridShape, func=sin))."""
         plan = self._engine()
-        out = plan.observe(kind, plan.pack_state(self))
+        out = plan.observe(kind, plan.pack_state(self), sin_k=self._sin_k(type))
         return plan.observable_view(out, 0, kind).detach().to('cpu').double().numpy()
 
     def CalculateBetaElastic(self, type='k'):
         """beta^E = IFFT(kmask T beta^P^) - beta^P (PlasticityState.py L357-390), on the GPU."""
-        if type != 'k':
-            raise NotImplementedError("CalculateBetaElastic supports type='k' on the GPU")
-        return Fields.from_stack(self.gridShape, self._observe("beta_elastic"))
+        return Fields.from_stack(self.gridShape, self._observe("beta_elastic", type))
 
     def CalculateRotationField(self, type='k'):
         """rotE_ij = (beta^E_ij - beta^E_ji) / 2 (PlasticityState.py L435-446), on the GPU."""
-        if type != 'k':
-            raise NotImplementedError("CalculateRotationField supports type='k' on the GPU")
-        w = self._observe("rotation")   # xy, xz, yz
+        w = self._observe("rotation", type)   # xy, xz, yz
         full = numpy.zeros((9,) + tuple(self.gridShape))
         for c, (i, j) in enumerate(((0, 1), (0, 2), (1, 2))):
             full[3 * i + j] = w[c]
@@ -141,22 +144,27 @@ class PlasticityState:
 
     def CalculateRotationRodrigues(self, type='k', source='betaP'):
         """Rodrigues rotation vector (PlasticityState.py L447-494), on the GPU: source 'betaP' (the
-        reference's default) from beta^P's transform, 'betaE' from the rotation field."""
-        if type != 'k' or source not in ('betaP', 'betaE'):
-            raise NotImplementedError("CalculateRotationRodrigues supports type='k', source='betaP'/'betaE'")
+        reference's default) from beta^P's transform, 'betaE' from the rotation field, 'rho' from
+        the Nye density field (which loses the means, as in the reference)."""
+        sin_k = self._sin_k(type)
         if source == 'betaP':
-            rod = self._observe("rodrigues")
-        else:
-            w = self._observe("rotation")
+            rod = self._observe("rodrigues", type)
+        elif source == 'betaE':
+            w = self._observe("rotation", type)
             rod = numpy.stack([w[2], -w[1], w[0]])
+        elif source == 'rho':
+            plan = self._engine()
+            rho = plan.observe("rho", plan.pack_state(self), sin_k=sin_k)
+            out = plan.observe("rodrigues_rho", rho, sin_k=sin_k)
+            rod = plan.observable_view(out, 0, "rodrigues_rho").detach().to('cpu').double().numpy()
+        else:
+            raise ValueError("source must be 'betaP', 'betaE' or 'rho'")
         return Fields.from_stack(self.gridShape, rod, components=[x, y, z])
 
     def CalculateRhoFourier(self, type='k'):
         """Nye dislocation density rho_ij = -eps_ikl d_k betaP_lj by Fourier derivatives
         (PlasticityState.py L264-304), on the GPU."""
-        if type != 'k':
-            raise NotImplementedError("CalculateRhoFourier supports type='k' on the GPU")
-        return Fields.from_stack(self.gridShape, self._observe("rho"))
+        return Fields.from_stack(self.gridShape, self._observe("rho", type))
 
     # ---------------------------------------------------------------- state algebra
     def _combine(self, other, op):

@@ -22,6 +22,8 @@ CDD_OBS_BETA_ELASTIC = 0
 CDD_OBS_ROTATION = 1
 CDD_OBS_RODRIGUES = 2
 CDD_OBS_RHO = 3
+CDD_OBS_RODRIGUES_RHO = 4
+CDD_OBS_SINK = 0x100
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_SHAPE", 3: "ERR_CUDA", 4: "ERR_NONFINITE",
                 5: "ERR_TIMEOUT", 6: "ERR_UNSUPPORTED", 7: "ERR_ALLOC"}
 

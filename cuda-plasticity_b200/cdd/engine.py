@@ -264,15 +264,19 @@ class Plan:
     # ------------------------------------------------------------------ field observables
     # name -> (cdd_observable, components); see cdd_observe_field in include/cdd.h
     OBSERVABLES = {"beta_elastic": (_lib.CDD_OBS_BETA_ELASTIC, 9), "rotation": (_lib.CDD_OBS_ROTATION, 3),
-                   "rodrigues": (_lib.CDD_OBS_RODRIGUES, 3), "rho": (_lib.CDD_OBS_RHO, 9)}
+                   "rodrigues": (_lib.CDD_OBS_RODRIGUES, 3), "rho": (_lib.CDD_OBS_RHO, 9),
+                   "rodrigues_rho": (_lib.CDD_OBS_RODRIGUES_RHO, 3)}
 
-    def observe(self, kind, beta, out=None, stream=None):
+    def observe(self, kind, beta, out=None, stream=None, sin_k=False):
         """A k-space field observable of every instance of beta: "beta_elastic" (9 components),
         "rotation" (3: xy, xz, yz of the antisymmetric part of beta^E), "rodrigues" (3: x, y, z,
-        from beta^P) or "rho" (9: the Nye density). Returns a packed buffer; ``observable_view``
-        gives instance i."""
+        from beta^P), "rho" (9: the Nye density) or "rodrigues_rho" (3: the Rodrigues vector of
+        the Nye density field passed as beta, i.e. what "rho" returns). sin_k: the reference's
+        type 'sinK' k tables. Returns a packed buffer; ``observable_view`` gives instance i."""
         self._check_field(beta)
         code, nc = self.OBSERVABLES[kind]
+        if sin_k:
+            code |= _lib.CDD_OBS_SINK
         n = self.field_elems if nc == 9 else self.field_elems // 3
         if out is None:
             out = torch.empty(n, dtype=self.dtype, device=self.device)

@@ -796,7 +796,8 @@ struct PlanCore {
     InstDev* d_inst = nullptr;       // device copy of the instance table
     InstClock* d_clock = nullptr;
     void* d_tw = nullptr;            // twiddles (double2 or float2)
-    void* d_k = nullptr;             // k tables (double or float)
+    void* d_k = nullptr;             // k tables (double or float): the wrapped identity ones, then the sine ones
+    long long ksin_off = 0;          // offset (elements) of the sine k tables ('sinK') in d_k
     void* d_spec = nullptr;          // 9-component half spectra
     void* d_sigma = nullptr;         // 6-component internal stress
     void* d_f0 = nullptr;            // stage-1 rhs / F0
@@ -868,7 +869,8 @@ cudaError_t launch_vacancy_pre(const PlanCore& P, const void* beta, cudaStream_t
 cudaError_t launch_vacancy_post(const PlanCore& P, const void* beta, cudaStream_t st);
 cudaError_t launch_vacancy_diffusion(const PlanCore& P, cudaStream_t st);
 // k-space observables of beta (kind: cdd_observable); out in the packed 9- or 3-component layout.
-cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st);
+cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st,
+                              bool sin_k = false);
 // Convert 9 components between the plan layout (last axis contiguous) and the reference files'
 // layout (axis 0 fastest) of an n0 x n1 x n2 grid (2-D: n0 x 1 x n1); to_file selects the direction.
 cudaError_t launch_field_xpose(bool to_file, const void* src, int src_prec, void* dst, int dst_prec, int n0, int n1,

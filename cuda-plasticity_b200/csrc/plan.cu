@@ -110,6 +110,11 @@ double k_value(int n_scale, int n_axis, int i) {
     return (double)n_scale * a;
 }
 
+// The 'sinK' tables, FourierSpaceTools(gridShape, func=sin): n_scale * sin(2 pi i / n_axis).
+double k_value_sin(int n_scale, int n_axis, int i) {
+    return (double)n_scale * std::sin(2.0 * M_PI * (double)i / (double)n_axis);
+}
+
 struct DevBuf {
     void* p = nullptr;
     ~DevBuf() {}
@@ -447,7 +452,7 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
     p->inst.resize(n_inst);
     std::map<int, LinePlan> lp_done;   // line plans (with twiddle offsets) by (length, largest radix)
     std::vector<double> twre, twim;
-    std::vector<double> ktab;
+    std::vector<double> ktab, ksin;   // k tables: wrapped identity and sine ('sinK'), same layout
     long long foff = 0, soff = 0, coff = 0, spoff = 0, rsoff = 0;
     C.any3d = false;
     for (int i = 0; i < n_inst; ++i) {
@@ -531,17 +536,32 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
         // k tables (FourierSpaceTools.py L26-55)
         if (I.nd == 3) {
             I.koff0 = (int)ktab.size();
-            for (int a = 0; a < I.n0; ++a) ktab.push_back(k_value(I.n0, I.n0, a));
+            for (int a = 0; a < I.n0; ++a) {
+                ktab.push_back(k_value(I.n0, I.n0, a));
+                ksin.push_back(k_value_sin(I.n0, I.n0, a));
+            }
             I.koff1 = (int)ktab.size();
-            for (int a = 0; a < I.n1; ++a) ktab.push_back(k_value(I.n1, I.n1, a));
+            for (int a = 0; a < I.n1; ++a) {
+                ktab.push_back(k_value(I.n1, I.n1, a));
+                ksin.push_back(k_value_sin(I.n1, I.n1, a));
+            }
             I.koffh = (int)ktab.size();
-            for (int a = 0; a < I.nh; ++a) ktab.push_back(k_value(I.n2, I.n2, a));
+            for (int a = 0; a < I.nh; ++a) {
+                ktab.push_back(k_value(I.n2, I.n2, a));
+                ksin.push_back(k_value_sin(I.n2, I.n2, a));
+            }
         } else {
             I.koff0 = (int)ktab.size();
-            for (int a = 0; a < I.n0; ++a) ktab.push_back(k_value(I.n1, I.n0, a));
+            for (int a = 0; a < I.n0; ++a) {
+                ktab.push_back(k_value(I.n1, I.n0, a));
+                ksin.push_back(k_value_sin(I.n1, I.n0, a));
+            }
             I.koff1 = I.koff0;
             I.koffh = (int)ktab.size();
-            for (int a = 0; a < I.nh; ++a) ktab.push_back(k_value(I.n1, I.n1, a));
+            for (int a = 0; a < I.nh; ++a) {
+                ktab.push_back(k_value(I.n1, I.n1, a));
+                ksin.push_back(k_value_sin(I.n1, I.n1, a));
+            }
         }
         I.mu = d.mu;
         I.nu = d.nu;
@@ -608,6 +628,8 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
         for (size_t k = 0; k < ntw; ++k) tw[k] = make_double2(twre[k], twim[k]);
         ALLOC_OR_FAIL(C.d_tw, sizeof(double2) * ntw);
         COPY_OR_FAIL(C.d_tw, tw.data(), sizeof(double2) * ntw);
+        C.ksin_off = (long long)ktab.size();
+        ktab.insert(ktab.end(), ksin.begin(), ksin.end());
         ALLOC_OR_FAIL(C.d_k, sizeof(double) * ktab.size());
         COPY_OR_FAIL(C.d_k, ktab.data(), sizeof(double) * ktab.size());
     } else {
@@ -615,7 +637,9 @@ int cdd_plan_create_tuned(const cdd_instance* inst, int n_inst, int precision, c
         for (size_t k = 0; k < ntw; ++k) tw[k] = make_float2((float)twre[k], (float)twim[k]);
         ALLOC_OR_FAIL(C.d_tw, sizeof(float2) * ntw);
         COPY_OR_FAIL(C.d_tw, tw.data(), sizeof(float2) * ntw);
+        C.ksin_off = (long long)ktab.size();
         std::vector<float> kf(ktab.begin(), ktab.end());
+        kf.insert(kf.end(), ksin.begin(), ksin.end());
         ALLOC_OR_FAIL(C.d_k, sizeof(float) * kf.size());
         COPY_OR_FAIL(C.d_k, kf.data(), sizeof(float) * kf.size());
     }
@@ -883,11 +907,13 @@ int cdd_set_vacancy(cdd_plan* p, void* c) {
 int cdd_observe_field(cdd_plan* p, int kind, const void* beta, void* out, void* stream) {
     if (int rc = check_plan(p)) return rc;
     if (!beta || !out) return fail(CDD_ERR_ARG, "null buffer");
-    if (kind < CDD_OBS_BETA_ELASTIC || kind > CDD_OBS_RHO) return fail(CDD_ERR_ARG, "bad observable %d", kind);
+    const bool sin_k = (kind & CDD_OBS_SINK) != 0;
+    const int base = kind & ~CDD_OBS_SINK;
+    if (base < CDD_OBS_BETA_ELASTIC || base > CDD_OBS_RODRIGUES_RHO) return fail(CDD_ERR_ARG, "bad observable %d", kind);
     if (!p->core.obs_ok)
         return fail(CDD_ERR_SHAPE, "the k-space observables need more shared memory than the device has for this "
                                    "axis-0 length");
-    CDD_CUDA(launch_observable(p->core, kind, beta, out, (cudaStream_t)stream));
+    CDD_CUDA(launch_observable(p->core, base, beta, out, (cudaStream_t)stream, sin_k));
     return CDD_OK;
 }
 

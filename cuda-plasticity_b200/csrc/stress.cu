@@ -891,9 +891,9 @@ __device__ __forceinline__ void green_point_dnu(const V* b, V* out, T kx, T ky, 
 // ---- k-space observables (PlasticityState.py) ----
 // Component counts of the k-space pass per mode (see k_green) and its shared-memory slots (inputs
 // or outputs, whichever are more, plus three scratch slots).
-__host__ __device__ constexpr int green_nin(int gmode) { return gmode == 6 ? 9 : (gmode == 7 ? 1 : 6); }
+__host__ __device__ constexpr int green_nin(int gmode) { return (gmode == 6 || gmode == 8) ? 9 : (gmode == 7 ? 1 : 6); }
 __host__ __device__ constexpr int green_nout(int gmode) {
-    return (gmode == 3 || gmode == 6) ? 9 : ((gmode == 4 || gmode == 5) ? 3 : (gmode == 7 ? 1 : 6));
+    return (gmode == 3 || gmode == 6) ? 9 : ((gmode == 4 || gmode == 5 || gmode == 8) ? 3 : (gmode == 7 ? 1 : 6));
 }
 // transforms run on groups of three components, or one by one for the single-component mode
 __host__ __device__ constexpr int green_group(int gmode) { return gmode == 7 ? 1 : 3; }
@@ -911,12 +911,43 @@ __host__ __device__ constexpr int green_slots(int gmode) {
 //     kmask sum_jst k_j (e_ijt k_s + e_ijs k_t) b_st / (2 kSq) = kmask (k x q)_i / kSq;
 //  6: the Nye density rho_ai = -e_akl d_k b_li by Fourier derivatives (CalculateRhoFourier
 //     L264-304): rho_xi = i (kz b_yi - ky b_zi), rho_yi = i (kx b_zi - kz b_xi),
-//     rho_zi = i (ky b_xi - kx b_yi) (kz = 0 in 2-D), no mask.
-// Inputs: 6 symmetric components xx xy xz yy yz zz (3-5) or all 9 (6).
+//     rho_zi = i (ky b_xi - kx b_yi) (kz = 0 in 2-D), no mask;
+//  8: the Rodrigues vector from the Nye density b = rho (CalculateRotationRodrigues L472-494, source
+//     'rho'): kmask sum_mn D_imn b_mn, D_imn = i (2 k_n d_im - k_m d_in - k_i d_mn) / (2 kSq)
+//     + i k_i k_n k_m / (2 kSqSq), i.e. i [(2 q_i - p_i - k_i s) / kSq + k_i r / kSqSq] / 2 with
+//     q = b k, p = b^T k, s = tr b, r = k . b k.
+// Inputs: 6 symmetric components xx xy xz yy yz zz (3-5) or all 9 (6, 8). The k values are those of
+// the table the launch passes (the wrapped identity or, for 'sinK', the sine tables).
 template <typename T, typename V, int GMODE>
 __device__ __forceinline__ void obs_point(const V* b, V* o, T kx, T ky, T kz, bool kzero, T A, T B, T scale) {
     const T k[3] = {kx, ky, kz};
-    if constexpr (GMODE == 6) {
+    if constexpr (GMODE == 8) {
+        const T ksq = kx * kx + ky * ky + kz * kz;
+        const T ikse = (T)1 / (ksq + (T)ME);
+        const T ikqe = (T)1 / (ksq * ksq + (T)ME);
+        const T f = (kzero ? (T)0 : (T)1) * (T)0.5 * scale;
+        V q[3], p[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            q[i].x = b[3 * i].x * k[0] + b[3 * i + 1].x * k[1] + b[3 * i + 2].x * k[2];
+            q[i].y = b[3 * i].y * k[0] + b[3 * i + 1].y * k[1] + b[3 * i + 2].y * k[2];
+            p[i].x = k[0] * b[i].x + k[1] * b[3 + i].x + k[2] * b[6 + i].x;
+            p[i].y = k[0] * b[i].y + k[1] * b[3 + i].y + k[2] * b[6 + i].y;
+        }
+        const V s1 = vadd(vadd(b[0], b[4]), b[8]);
+        V r;
+        r.x = k[0] * q[0].x + k[1] * q[1].x + k[2] * q[2].x;
+        r.y = k[0] * q[0].y + k[1] * q[1].y + k[2] * q[2].y;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            V t;   // (2 q_i - p_i - k_i s) / kSq + k_i r / kSqSq, then times i f
+            t.x = ((T)2 * q[i].x - p[i].x - k[i] * s1.x) * ikse + k[i] * r.x * ikqe;
+            t.y = ((T)2 * q[i].y - p[i].y - k[i] * s1.y) * ikse + k[i] * r.y * ikqe;
+            o[i].x = -t.y * f;
+            o[i].y = t.x * f;
+        }
+        return;
+    } else if constexpr (GMODE == 6) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const V bx = b[i], by = b[3 + i], bz = b[6 + i];
@@ -1681,7 +1712,7 @@ cudaError_t launch_vacancy_diffusion(const PlanCore& P, cudaStream_t st) {
 // fused axis-0 pass, inverse transforms of its 9 or 3 components with the real-space epilogue.
 // No FP64 mean path: every operator's k = 0 mode is zero (kmask, or a factor k).
 template <typename T, int GMODE>
-static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out, cudaStream_t st) {
+static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out, cudaStream_t st, bool sin_k) {
     typedef typename VecOf<T>::type V;
     V* spec = (V*)P.d_spec;
     const V* tw = (const V*)P.d_tw;
@@ -1695,8 +1726,9 @@ static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out
     if (LI[PASS_MID_F].blocks > 0)
         k_fft_mid<T, false><<<LI[PASS_MID_F].blocks, LI[PASS_MID_F].threads, LI[PASS_MID_F].smem, st>>>(
             P.d_inst, P.n_inst, LI[PASS_MID_F].d_pre, spec, tw, PASS_MID_F, NIN, 0);
-    k_green<T, false, GMODE><<<LG.blocks, LG.threads, LG.smem, st>>>(P.d_inst, P.n_inst, LG.d_pre, spec, tw,
-                                                                      (const T*)P.d_k, nullptr, nullptr, nullptr);
+    const T* ktab = (const T*)P.d_k + (sin_k ? P.ksin_off : 0);
+    k_green<T, false, GMODE><<<LG.blocks, LG.threads, LG.smem, st>>>(P.d_inst, P.n_inst, LG.d_pre, spec, tw, ktab,
+                                                                      nullptr, nullptr, nullptr);
     if (LO[PASS_MID_I].blocks > 0)
         k_fft_mid<T, true><<<LO[PASS_MID_I].blocks, LO[PASS_MID_I].threads, LO[PASS_MID_I].smem, st>>>(
             P.d_inst, P.n_inst, LO[PASS_MID_I].d_pre, spec, tw, PASS_MID_I, NOUT, 0);
@@ -1707,19 +1739,22 @@ static cudaError_t run_observable(const PlanCore& P, const void* beta, void* out
 }
 
 template <typename T>
-static cudaError_t run_observable_t(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st) {
+static cudaError_t run_observable_t(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st,
+                                    bool sin_k) {
     switch (kind) {
-        case CDD_OBS_BETA_ELASTIC: return run_observable<T, 3>(P, beta, out, st);
-        case CDD_OBS_ROTATION: return run_observable<T, 4>(P, beta, out, st);
-        case CDD_OBS_RODRIGUES: return run_observable<T, 5>(P, beta, out, st);
-        case CDD_OBS_RHO: return run_observable<T, 6>(P, beta, out, st);
+        case CDD_OBS_BETA_ELASTIC: return run_observable<T, 3>(P, beta, out, st, sin_k);
+        case CDD_OBS_ROTATION: return run_observable<T, 4>(P, beta, out, st, sin_k);
+        case CDD_OBS_RODRIGUES: return run_observable<T, 5>(P, beta, out, st, sin_k);
+        case CDD_OBS_RHO: return run_observable<T, 6>(P, beta, out, st, sin_k);
+        case CDD_OBS_RODRIGUES_RHO: return run_observable<T, 8>(P, beta, out, st, sin_k);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st) {
-    if (P.precision == CDD_F32) return run_observable_t<float>(P, kind, beta, out, st);
-    return run_observable_t<double>(P, kind, beta, out, st);
+cudaError_t launch_observable(const PlanCore& P, int kind, const void* beta, void* out, cudaStream_t st,
+                              bool sin_k) {
+    if (P.precision == CDD_F32) return run_observable_t<float>(P, kind, beta, out, st, sin_k);
+    return run_observable_t<double>(P, kind, beta, out, st, sin_k);
 }
 
 cudaError_t launch_stress(const PlanCore& P, const void* beta, void* sigma, cudaStream_t st, void* phi) {
@@ -1756,6 +1791,7 @@ static cudaError_t set_attr_t(size_t smem) {
     if ((e = set_dyn_smem_limit(k_green<T, false, 5>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 6>, smem))) return e;
     if ((e = set_dyn_smem_limit(k_green<T, false, 7>, smem))) return e;
+    if ((e = set_dyn_smem_limit(k_green<T, false, 8>, smem))) return e;
     return cudaSuccess;
 }
 

@@ -294,7 +294,16 @@ int cdd_set_vacancy(cdd_plan* plan, void* c);
  *                        derivatives, 9 components (CalculateRhoFourier L264-304).
  * Uses the plan's spectrum scratch (stream-ordered with the other entry points). CDD_ERR_SHAPE when
  * the k-space pass of 12 component slots does not fit the device's shared memory. */
-enum cdd_observable { CDD_OBS_BETA_ELASTIC = 0, CDD_OBS_ROTATION = 1, CDD_OBS_RODRIGUES = 2, CDD_OBS_RHO = 3 };
+/*  CDD_OBS_RODRIGUES_RHO: the Rodrigues vector from the Nye density (CalculateRotationRodrigues L472-494,
+ *                        source 'rho'): `beta` holds the density field as CDD_OBS_RHO returns it (field
+ *                        layout, 9 components), transformed again and contracted with
+ *                        D_imn = i (2 k_n d_im - k_m d_in - k_i d_mn) / (2 kSq) + i k_i k_n k_m / (2 kSqSq);
+ *                        3 components, no real-space term (the means are lost, as in the reference).
+ * kind | CDD_OBS_SINK uses the k tables of FourierSpaceTools(gridShape, func=sin) (the reference's type
+ * 'sinK', n sin(2 pi i / n) per axis) instead of the wrapped identity ones; kmask is the same. */
+enum cdd_observable { CDD_OBS_BETA_ELASTIC = 0, CDD_OBS_ROTATION = 1, CDD_OBS_RODRIGUES = 2, CDD_OBS_RHO = 3,
+                      CDD_OBS_RODRIGUES_RHO = 4 };
+#define CDD_OBS_SINK 0x100
 int cdd_observe_field(cdd_plan* plan, int kind, const void* beta, void* out, void* stream);
 
 /* ---- The reference CUDA solver's on-disk formats ----

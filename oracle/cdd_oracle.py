@@ -37,23 +37,27 @@ def _identity(a):
     return a - 2 * np.pi * greater
 
 
-def k_axis(n_scale, n_axis, count):
-    """``n_scale * identity(2 pi i / n_axis)`` for i in [0, count) (FourierSpaceTools.py L29-49)."""
+def k_axis(n_scale, n_axis, count, sin_k=False):
+    """``n_scale * func(2 pi i / n_axis)`` for i in [0, count) (FourierSpaceTools.py L29-49), func the
+    identity wrap or, for the 'sinK' tools (PlasticityState.py L35-39, ``func=sin``), the sine."""
     i = np.arange(count, dtype=np.float64)
-    return n_scale * _identity(2. * np.pi * i / float(n_axis))
+    a = 2. * np.pi * i / float(n_axis)
+    return n_scale * (np.sin(a) if sin_k else _identity(a))
 
 
-def k_tables(shape):
+def k_tables(shape, sin_k=False):
     """Return (k, kSq, kSqSq, kmask) on the rfft half grid, as in FourierSpaceTools.py L26-55.
 
     ``k`` is a list of three broadcastable arrays (kx, ky, kz). In 2-D both wave vectors are
     scaled by ``gridShape[1]`` (L29-30) and kz is zero; in 3-D each axis uses its own size (L47-49).
+    ``sin_k``: the tables of ``FourierSpaceTools(gridShape, func=sin)`` (the observables' type
+    'sinK'); kmask is the same.
     """
     if len(shape) == 3:
         n0, n1, n2 = shape
-        kx = k_axis(n0, n0, n0).reshape(n0, 1, 1)
-        ky = k_axis(n1, n1, n1).reshape(1, n1, 1)
-        kz = k_axis(n2, n2, n2 // 2 + 1).reshape(1, 1, n2 // 2 + 1)
+        kx = k_axis(n0, n0, n0, sin_k).reshape(n0, 1, 1)
+        ky = k_axis(n1, n1, n1, sin_k).reshape(1, n1, 1)
+        kz = k_axis(n2, n2, n2 // 2 + 1, sin_k).reshape(1, 1, n2 // 2 + 1)
         full = (n0, n1, n2 // 2 + 1)
         kx, ky, kz = (np.broadcast_to(v, full) for v in (kx, ky, kz))
         kSq = kx * kx + ky * ky + kz * kz
@@ -61,8 +65,8 @@ def k_tables(shape):
         kmask[0, 0, 0] = 0.
     elif len(shape) == 2:
         n0, n1 = shape
-        kx = k_axis(n1, n0, n0).reshape(n0, 1)
-        ky = k_axis(n1, n1, n1 // 2 + 1).reshape(1, n1 // 2 + 1)
+        kx = k_axis(n1, n0, n0, sin_k).reshape(n0, 1)
+        ky = k_axis(n1, n1, n1 // 2 + 1, sin_k).reshape(1, n1 // 2 + 1)
         full = (n0, n1 // 2 + 1)
         kx, ky = (np.broadcast_to(v, full) for v in (kx, ky))
         kz = np.zeros(full)
@@ -79,12 +83,12 @@ def k_tables(shape):
 # Stress: PlasticityState.CalculateSigma(type='k', source='betaE') L85-127 and
 #         PlasticityState.CalculateBetaElastic L357-390
 # ----------------------------------------------------------------------------------------------
-def beta_elastic(beta, mu, nu):
+def beta_elastic(beta, mu, nu, sin_k=False):
     shape = beta.shape[1:]
     axes = tuple(range(-len(shape), 0))
     KbetaP = np.fft.rfftn(beta, axes=axes)
     lamb = 2. * mu * nu / (1. - 2 * nu)
-    k, kSq0, kSqSq0, kmask = k_tables(shape)
+    k, kSq0, kSqSq0, kmask = k_tables(shape, sin_k)
     kSq = kSq0 + ME
     kSqSq = kSqSq0 + ME
     KbetaE = np.zeros_like(KbetaP)
@@ -537,12 +541,12 @@ PERM[0, 1, 2] = PERM[1, 2, 0] = PERM[2, 0, 1] = 1.
 PERM[0, 2, 1] = PERM[2, 1, 0] = PERM[1, 0, 2] = -1.
 
 
-def rho_fourier(beta):
+def rho_fourier(beta, sin_k=False):
     """Nye density rho_ij = -eps_ikl d_k beta_lj with Fourier derivatives d_k -> i k_k (no kmask)."""
     shape = beta.shape[1:]
     axes = tuple(range(-len(shape), 0))
     Kb = np.fft.rfftn(beta, axes=axes)
-    k = k_tables(shape)[0]
+    k = k_tables(shape, sin_k)[0]
     D = [Kb * (1.0j * k[d]) for d in range(len(shape))]
     Kr = np.zeros_like(Kb)
     for i in range(3):
@@ -557,19 +561,19 @@ def rho_fourier(beta):
     return np.fft.irfftn(Kr, s=shape, axes=axes)
 
 
-def rotation_field(beta, mu, nu):
+def rotation_field(beta, mu, nu, sin_k=False):
     """rotE_ij = (betaE_ij - betaE_ji) / 2, 9 components."""
-    be = beta_elastic(beta, mu, nu)
+    be = beta_elastic(beta, mu, nu, sin_k)
     return np.stack([(be[ci(i, j)] - be[ci(j, i)]) / 2. for i in range(3) for j in range(3)])
 
 
-def rodrigues(beta):
+def rodrigues(beta, sin_k=False):
     """Rodrigues vector (x, y, z) from beta^P: IFFT(kmask sum k_j (e_ijt k_s + e_ijs k_t) b_st /
     kSq / 2) minus the antisymmetric part of beta^P."""
     shape = beta.shape[1:]
     axes = tuple(range(-len(shape), 0))
     Kb = np.fft.rfftn(beta, axes=axes)
-    k, kSq0, _, kmask = k_tables(shape)
+    k, kSq0, _, kmask = k_tables(shape, sin_k)
     kSq = kSq0 + ME
     Kr = np.zeros((3,) + Kb.shape[1:], dtype=complex)
     for i in range(3):
@@ -583,3 +587,26 @@ def rodrigues(beta):
     rod[1] -= (beta[ci(2, 0)] - beta[ci(0, 2)]) / 2.
     rod[2] -= (beta[ci(0, 1)] - beta[ci(1, 0)]) / 2.
     return rod
+
+
+def rodrigues_from_rho(beta, sin_k=False):
+    """Rodrigues vector from the Nye density (CalculateRotationRodrigues source 'rho',
+    PlasticityState.py L472-494): rho = rho_fourier(beta) as a real field, then
+    IFFT(kmask sum_mn D_imn FFT(rho)_mn) with D_imn = i (2 k_n d_im - k_m d_in - k_i d_mn) / (2 kSq)
+    + i k_i k_n k_m / (2 kSqSq), kSq = |k|^2 + ME, kSqSq = |k|^4 + ME."""
+    shape = beta.shape[1:]
+    axes = tuple(range(-len(shape), 0))
+    rho = rho_fourier(beta, sin_k)
+    KR = np.fft.rfftn(rho, axes=axes)
+    k, kSq0, kSqSq0, kmask = k_tables(shape, sin_k)
+    kSq = kSq0 + ME
+    kSqSq = kSqSq0 + ME
+    Kr = np.zeros((3,) + KR.shape[1:], dtype=complex)
+    for i in range(3):
+        for m in range(3):
+            for n in range(3):
+                D = ((1.j) / (2. * kSq)) * (2. * k[n] * (i == m) - k[m] * (i == n) - k[i] * (m == n)) + \
+                    (1.j) * k[i] * k[n] * k[m] / (2. * kSqSq)
+                Kr[i] += D * KR[ci(m, n)]
+        Kr[i] *= kmask
+    return np.fft.irfftn(Kr, s=shape, axes=axes)

@@ -22,7 +22,7 @@ CentralUpwindHJBetaPDynamics.py (2-D, the module RunPython.py imports), and
 
 ``initializer.npz`` holds states of the reference's GaussianRandomInitializer (``run_initializer_case``).
 ``observables.npz`` holds the field observables of PlasticityState (beta^E, rotation, Rodrigues
-vector, Nye density) of seeded fields. ``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
+vector from beta^P and from rho, Nye density; with the 'k' and the 'sinK' tables) of seeded fields. ``io_formats.npz`` pins the CUDA solver's file formats: the reference's convertStateToCUDA and
 LoadStateRaw run from their source text (``run_io_case``).
 
 ``c2_3d_64`` and ``c2_3d_128`` are compact fixtures of 10 steps at the config-2 sizes (sigma 0.04, the
@@ -302,6 +302,15 @@ def run_observables_case(name="observables"):
         rod = st.CalculateRotationRodrigues()
         out["rod_" + key] = np.stack([np.asarray(rod[a]) for a in "xyz"])
         out["rho_" + key] = stack9(st.CalculateRhoFourier())
+        # the 'sinK' tools (FourierSpaceTools with func=sin) and the Rodrigues vector from rho
+        out["betaE_sink_" + key] = stack9(st.CalculateBetaElastic(type='sinK'))
+        out["rot_sink_" + key] = stack9(st.CalculateRotationField(type='sinK'))
+        rod = st.CalculateRotationRodrigues(type='sinK')
+        out["rod_sink_" + key] = np.stack([np.asarray(rod[a]) for a in "xyz"])
+        out["rho_sink_" + key] = stack9(st.CalculateRhoFourier(type='sinK'))
+        for tag, typ in (("rodrho_", 'k'), ("rodrho_sink_", 'sinK')):
+            rod = st.CalculateRotationRodrigues(type=typ, source='rho')
+            out[tag + key] = np.stack([np.asarray(rod[a]) for a in "xyz"])
     path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **out)
     print("%-16s -> %s" % (name, os.path.relpath(path, REPO)))

@@ -84,3 +84,34 @@ def test_facade_observables():
     r9 = G["rot_c"]
     assert rel(np.stack([np.asarray(rodE[a]) for a in "xyz"]), np.stack([r9[5], r9[6], r9[1]])) < 1e-12
     assert rel(st.CalculateRhoFourier().stack(), G["rho_c"]) < 1e-12
+
+
+@pytest.mark.parametrize("key", KEYS)
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-12), ("f32", 1e-5)])
+def test_sink_tables_and_rodrigues_from_rho_match_reference(key, prec, tol):
+    """type 'sinK' (the sine k tables, CDD_OBS_SINK) for every observable, and the Rodrigues vector
+    from the Nye density field (CDD_OBS_RODRIGUES_RHO, source 'rho') with both tables."""
+    beta0 = G["beta_" + key]
+    plan = cdd.Plan([cdd.Instance(beta0.shape[1:], mu=1.0, nu=0.3)], prec)
+    beta = plan.pack([beta0])
+    view = lambda kind, buf: plan.observable_view(buf, 0, kind).cpu().numpy()
+    assert rel(view("beta_elastic", plan.observe("beta_elastic", beta, sin_k=True)), G["betaE_sink_" + key]) < tol
+    assert rel(view("rotation", plan.observe("rotation", beta, sin_k=True)), rot3(G["rot_sink_" + key])) < tol
+    assert rel(view("rodrigues", plan.observe("rodrigues", beta, sin_k=True)), G["rod_sink_" + key]) < tol
+    assert rel(view("rho", plan.observe("rho", beta, sin_k=True)), G["rho_sink_" + key]) < tol
+    for sink, tag in ((False, "rodrho_"), (True, "rodrho_sink_")):
+        rho = plan.observe("rho", beta, sin_k=sink)
+        got = view("rodrigues_rho", plan.observe("rodrigues_rho", rho, sin_k=sink))
+        assert rel(got, G[tag + key]) < tol, (sink, rel(got, G[tag + key]))
+
+
+def test_facade_sink_and_rho_source():
+    from Plasticity.PlasticityStates import PlasticityState
+    from Plasticity.Fields import Fields
+    beta0 = G["beta_c"]
+    st = PlasticityState.PlasticityState(beta0.shape[1:], mu=1.0, nu=0.3)
+    st.betaP = Fields.from_stack(beta0.shape[1:], beta0)
+    rod = st.CalculateRotationRodrigues(type='sinK', source='rho')
+    assert rel(np.stack([np.asarray(rod[a]) for a in "xyz"]), G["rodrho_sink_c"]) < 1e-12
+    rho = st.CalculateRhoFourier(type='sinK')
+    assert rel(rho.stack(), G["rho_sink_c"]) < 1e-12
