@@ -200,7 +200,9 @@ int build_shapes(cdd_plan* p, size_t elt) {
             if (P > npairs) P = (int)npairs;
             PassTile& t = I.tile[k];
             t.lines = P;
-            t.threads = (velt == 8) ? 256 : 128;
+            // one first-stage butterfly per thread for 16-point stages: 256 threads from 16 line pairs
+            // on (FP32), 128 below (and for FP64)
+            t.threads = (velt == 8 && P >= 16) ? 256 : 128;
             t.blocks = (int)((npairs + P - 1) / P);
             t.tiles_a = 1;
             size_t sm = (((size_t)rows_buffers(I.lp_last, P) * P * (line_bytes / velt) + 1) & ~(size_t)1) * velt +
@@ -309,7 +311,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
     for (int k = 0; k < NUM_PASSES; ++k) {
         LaunchShape& L = C.pass[k];
         L.blocks = pre[k].back();
-        L.threads = (k == PASS_R2C || k == PASS_C2R) ? (velt == 8 ? 256 : 128) : 256;
+        L.threads = (k == PASS_R2C || k == PASS_C2R) ? thr_max[k] : 256;
         L.smem = smem_max[k];
         if (L.smem > smem_all) smem_all = L.smem;
         CDD_CUDA(dalloc(p, (void**)&L.d_pre, sizeof(int) * (n + 1)));
