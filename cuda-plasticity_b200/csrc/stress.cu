@@ -657,30 +657,17 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 1) k_c2r_row
 // Complex FFT along axis 1 of a 3-D spectrum, in place, for `ncomp` components.
 // Block = (component, i0, column tile of W).
 // ------------------------------------------------------------------------------------------
+// One column tile: W = 2^lgw columns of N = n1 elements from base (row pitch nhp), wv of them valid.
+// The kernel calls it with lgw as a literal for the usual tile widths, so that every shared-memory
+// offset of the stages folds to a constant.
 template <typename T, bool INV>
-__global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 2) k_fft_mid(const InstDev* __restrict__ insts, int n_inst,
-                                                 const int* __restrict__ pre,
-                                                 typename VecOf<T>::type* __restrict__ spec,
-                                                 const typename VecOf<T>::type* __restrict__ tw,
-                                                 int pass, int ncomp, int vac_only) {
+__device__ __forceinline__ void fft_mid_tile(const InstDev& I, typename VecOf<T>::type* s,
+                                             typename VecOf<T>::type* base,
+                                             const typename VecOf<T>::type* __restrict__ tw, int lgw, int wv,
+                                             int tid, int nt) {
     typedef typename VecOf<T>::type V;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* s = reinterpret_cast<V*>(smem_raw);
-    const int ii = find_instance(pre, n_inst, blockIdx.x);
-    const InstDev& I = insts[ii];
-    int lb = blockIdx.x - pre[ii];
-    const PassTile& tl = I.tile[pass];
-    const int W = tl.lines, lgw = tl.lgw, ta_n = tl.tiles_a;
-    const int ta = lb % ta_n; lb /= ta_n;
-    const int i0 = lb % I.n0;
-    const int c = lb / I.n0;
-    if (c >= ncomp) return;   // launch sized for more components than this pass carries
-    if (vac_only && !I.vacancy) return;
-    const int N = I.n1, nhp = I.nhp, nh = I.nh;
-    const int col0 = ta * W;
-    const int wv = min(W, nh - col0);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+    const int W = 1 << lgw;
+    const int N = I.n1, nhp = I.nhp;
     if (line_plan_io(I.lp_mid)) {
         // first and last stage in global memory; one shared tile for two-stage plans
         V* tws = s + (I.lp_mid.nst == 2 ? 1 : 2) * N * W;
@@ -716,6 +703,35 @@ __global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 2) k_fft_mid
             if (w < wv) base[(long long)e * nhp + w] = s[i];
         }
     }
+}
+
+template <typename T, bool INV>
+__global__ void __launch_bounds__(ROW_THREADS, sizeof(T) == 4 ? 4 : 2) k_fft_mid(const InstDev* __restrict__ insts, int n_inst,
+                                                 const int* __restrict__ pre,
+                                                 typename VecOf<T>::type* __restrict__ spec,
+                                                 const typename VecOf<T>::type* __restrict__ tw,
+                                                 int pass, int ncomp, int vac_only) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    int lb = blockIdx.x - pre[ii];
+    const PassTile& tl = I.tile[pass];
+    const int W = tl.lines, lgw = tl.lgw, ta_n = tl.tiles_a;
+    const int ta = lb % ta_n; lb /= ta_n;
+    const int i0 = lb % I.n0;
+    const int c = lb / I.n0;
+    if (c >= ncomp) return;   // launch sized for more components than this pass carries
+    if (vac_only && !I.vacancy) return;
+    const int N = I.n1, nhp = I.nhp, nh = I.nh;
+    const int col0 = ta * W;
+    const int wv = min(W, nh - col0);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    V* base = spec + I.spoff + ((long long)c * I.n0 + i0) * (long long)N * nhp + col0;
+    if (lgw == 4) fft_mid_tile<T, INV>(I, s, base, tw, 4, wv, tid, nt);
+    else if (lgw == 3) fft_mid_tile<T, INV>(I, s, base, tw, 3, wv, tid, nt);
+    else fft_mid_tile<T, INV>(I, s, base, tw, lgw, wv, tid, nt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1035,25 +1051,20 @@ __device__ __forceinline__ void fft_group(V* s, int g, int lgw, int cs, const Li
 // sum_k w_k Re(conj(sigbar_hat) . (2 mu k k + lam kSq I) phi) / cells (w_k = 1 on the first and
 // the Nyquist half-axis column, 2 elsewhere): the A/B part of <sigbar, (d sigma / d nu) beta>
 // per unit dA.
+// One column tile of the k-space pass: W = 2^lgw spectrum columns from ta W of row i1 (3-D) of
+// instance ii. k_green calls it with lgw as a literal for the usual tile widths, so that the
+// shared-memory offsets of the transforms fold to constants.
 template <typename T, bool MEAN64, int GMODE>
-__global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green(const InstDev* __restrict__ insts, int n_inst,
-                                                         const int* __restrict__ pre,
-                                                         typename VecOf<T>::type* __restrict__ spec,
-                                                         const typename VecOf<T>::type* __restrict__ tw,
-                                                         const T* __restrict__ ktab,
-                                                         typename VecOf<T>::type* __restrict__ phi,
-                                                         double* __restrict__ part,
-                                                         const InstClock* __restrict__ clk) {
+__device__ __forceinline__ void green_tile(const InstDev& I, int ii, int ta, int i1, int lgw,
+                                           typename VecOf<T>::type* s,
+                                           typename VecOf<T>::type* __restrict__ spec,
+                                           const typename VecOf<T>::type* __restrict__ tw,
+                                           const T* __restrict__ ktab,
+                                           typename VecOf<T>::type* __restrict__ phi,
+                                           double* __restrict__ part,
+                                           const InstClock* __restrict__ clk) {
     typedef typename VecOf<T>::type V;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* s = reinterpret_cast<V*>(smem_raw);
-    const int ii = find_instance(pre, n_inst, blockIdx.x);
-    const InstDev& I = insts[ii];
-    int lb = blockIdx.x - pre[ii];
-    const PassTile& tl = I.tile[PASS_GREEN];
-    const int W = tl.lines, lgw = tl.lgw, ta_n = tl.tiles_a;
-    const int ta = lb % ta_n;
-    const int i1 = lb / ta_n;          // 0 in 2-D
+    const int W = 1 << lgw;
     const int N = I.n0, nhp = I.nhp, nh = I.nh;
     const int col0 = ta * W;
     const int wv = min(W, nh - col0);
@@ -1210,6 +1221,40 @@ __global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green
             }
         }
     }
+}
+
+template <typename T, bool MEAN64, int GMODE>
+__global__ void __launch_bounds__(GREEN_THREADS, sizeof(T) == 4 ? 3 : 2) k_green(const InstDev* __restrict__ insts, int n_inst,
+                                                         const int* __restrict__ pre,
+                                                         typename VecOf<T>::type* __restrict__ spec,
+                                                         const typename VecOf<T>::type* __restrict__ tw,
+                                                         const T* __restrict__ ktab,
+                                                         typename VecOf<T>::type* __restrict__ phi,
+                                                         double* __restrict__ part,
+                                                         const InstClock* __restrict__ clk) {
+    typedef typename VecOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s = reinterpret_cast<V*>(smem_raw);
+    const int ii = find_instance(pre, n_inst, blockIdx.x);
+    const InstDev& I = insts[ii];
+    int lb = blockIdx.x - pre[ii];
+    const PassTile& tl = I.tile[PASS_GREEN];
+    const int lgw = tl.lgw, ta_n = tl.tiles_a;
+    const int ta = lb % ta_n;
+    const int i1 = lb / ta_n;          // 0 in 2-D
+    // the FP32 stress solve (GMODE 0) at the built-in tile width (4 columns) and 8 (measured: 1.5%
+    // faster at 256^3, 3% at 96^3; FP64 kept the general form, which measured no slower)
+    if constexpr (GMODE == 0 && sizeof(T) == 4) {
+        if (lgw == 2) {
+            green_tile<T, MEAN64, GMODE>(I, ii, ta, i1, 2, s, spec, tw, ktab, phi, part, clk);
+            return;
+        }
+        if (lgw == 3) {
+            green_tile<T, MEAN64, GMODE>(I, ii, ta, i1, 3, s, spec, tw, ktab, phi, part, clk);
+            return;
+        }
+    }
+    green_tile<T, MEAN64, GMODE>(I, ii, ta, i1, lgw, s, spec, tw, ktab, phi, part, clk);
 }
 
 // ------------------------------------------------------------------------------------------
