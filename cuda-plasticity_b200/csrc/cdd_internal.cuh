@@ -896,7 +896,7 @@ inline cudaError_t set_dyn_smem_limit(F* fn, size_t smem) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v);
 }
 size_t stencil_smem_bytes(int precision, bool any3d);
-void stencil_geometry(InstDev& I, int planes = 0);
+void stencil_geometry(InstDev& I, int precision, int planes = 0);
 cudaError_t stress_set_attributes(int precision, size_t max_smem);
 // Fused plane passes of the stress solve (stress.cu): whether instance I can take them and their
 // shared memory per block.

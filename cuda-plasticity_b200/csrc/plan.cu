@@ -276,7 +276,7 @@ int build_shapes(cdd_plan* p, size_t elt) {
             for (int k = 0; k < NUM_PASSES; ++k) pre_rest[k].push_back(pre_rest[k].back() + (I.plane ? 0 : I.tile[k].blocks));
             if (I.plane && plane_smem_bytes(I) > smem_plane) smem_plane = plane_smem_bytes(I);
         }
-        stencil_geometry(I, p->tune[i].stencil_planes);
+        stencil_geometry(I, C.precision, p->tune[i].stencil_planes);
         // effective launch shapes of this instance
         p->tune[i].rows_lines = I.tile[PASS_R2C].lines;
         p->tune[i].mid_cols = (I.nd == 3) ? I.tile[PASS_MID_F].lines : 0;

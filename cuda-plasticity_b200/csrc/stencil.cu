@@ -56,12 +56,13 @@ __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 // contiguous) and walks along axis 0 (3-D). Each staged plane holds all 9 components of a box of
 // RY rows (2-row halo in y) by RX columns starting OX cells left of the tile: RX/OX keep the box's
 // x origin on a 16-byte boundary (TMA), i.e. 40/4 for FP32 and 36/2 for FP64.
-constexpr int TXS = 32, TYS = 4, RY = TYS + 4;
-constexpr int ST_THREADS = TXS * TYS;
+constexpr int TXS = 32;
 template <typename T> struct TileGeom;
-template <> struct TileGeom<float> { static constexpr int RX = 40, OX = 4, NS = 6; };
-template <> struct TileGeom<double> { static constexpr int RX = 36, OX = 2, NS = 5; };
-template <typename T> __host__ __device__ constexpr int tile_pp() { return RY * TileGeom<T>::RX; }   // per component
+template <> struct TileGeom<float> { static constexpr int RX = 40, OX = 4, NS = 6, TY = 8; };
+template <> struct TileGeom<double> { static constexpr int RX = 36, OX = 2, NS = 5, TY = 4; };
+template <typename T> __host__ __device__ constexpr int tile_ry() { return TileGeom<T>::TY + 4; }
+template <typename T> __host__ __device__ constexpr int st_threads() { return TXS * TileGeom<T>::TY; }
+template <typename T> __host__ __device__ constexpr int tile_pp() { return tile_ry<T>() * TileGeom<T>::RX; }   // per component
 
 template <typename T, int ND>
 struct TileView {
@@ -137,6 +138,8 @@ __device__ __forceinline__ void cp_async_elem(double* dst, const double* src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_own() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// Hint: bring the 128-byte line at p into L2 (no register result, no completion to wait for).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 
 // u+ and u- from the five values u_{-2} .. u_{+2} along one axis. The limiter arguments D1, D2
 // of FindDerivatives all carry 1/h^2; minmod is positively homogeneous, so the kernel limits the
@@ -475,14 +478,48 @@ template <typename T> struct CellCtx {
     bool has_load, lam_on, glide;
 };
 
+// Stage-1 observables of a thread's cells: the CFL speed maximum (NaN and Inf map to +Inf) and
+// the FP64 sums of the elastic energy density and of b_zz. FP64 keeps all three in registers.
+// FP32 (255 registers per thread would cost resident warps) keeps the maximum as a float (a
+// maximum of floats is exact) and the two FP64 sums in this thread's two shared-memory slots
+// (`acc`, `acc + ST_THREADS`), so that nothing of them stays in registers across the march.
+template <typename T> struct Stage1Acc {
+    double vmax = 0.0, esum = 0.0, zsum = 0.0;
+    __device__ __forceinline__ void start(double*, int) {}
+    __device__ __forceinline__ void speed(T s) {
+        double v = (double)s;
+        if (!(v <= 1.0e300)) v = __longlong_as_double(0x7ff0000000000000LL);   // NaN/Inf -> +Inf
+        vmax = fmax(vmax, v);
+    }
+    __device__ __forceinline__ void energy(double e, double*, int) { esum += e; }
+    __device__ __forceinline__ void bzz(double z, double*, int) { zsum += z; }
+    __device__ __forceinline__ double max_speed() const { return vmax; }
+    __device__ __forceinline__ double energy_sum(const double*) const { return esum; }
+    __device__ __forceinline__ double bzz_sum(const double*, int) const { return zsum; }
+};
+template <> struct Stage1Acc<float> {
+    float vmax = 0.0f;
+    __device__ __forceinline__ void start(double* acc, int nt) { acc[0] = 0.0; acc[nt] = 0.0; }
+    __device__ __forceinline__ void speed(float s) {
+        if (!(s <= 3.402823466e38f)) s = __int_as_float(0x7f800000);   // NaN/Inf -> +Inf
+        vmax = fmaxf(vmax, s);
+    }
+    __device__ __forceinline__ void energy(double e, double* acc, int) { acc[0] += e; }
+    __device__ __forceinline__ void bzz(double z, double* acc, int nt) { acc[nt] += z; }
+    __device__ __forceinline__ double max_speed() const { return (double)vmax; }
+    __device__ __forceinline__ double energy_sum(const double* acc) const { return acc[0]; }
+    __device__ __forceinline__ double bzz_sum(const double* acc, int nt) const { return acc[nt]; }
+};
+
 // ssm: this thread's 6 shared-memory stress slots (component c at ssm[c * ST_THREADS]), filled by
 // asynchronous copies issued one cell earlier; sig_next: the stress of the thread's cell in the
-// next plane (its copies are issued as soon as this cell's values are read), or null.
+// next plane (its copies are issued as soon as this cell's values are read), or null; acc: this
+// thread's FP64 sum slots (FP32 stage 1).
 template <typename T, int ND, int MODE, int VAR>
 __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>& cx, bool valid,
                                              const TileView<T, ND>& tv,
                                              const StageConst& kc_block, const InstClock& ck, double t_flux,
-                                             double& vmax, double& esum, double& zsum,
+                                             Stage1Acc<T>& sums, double* acc,
                                              const T* __restrict__ sig0, const T* __restrict__ vac,
                                              T* ssm, const T* sig_next) {
     // compile-time variant: bit 0 carries the glide-only projection, bit 1 the vacancy term
@@ -495,16 +532,9 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
     StageConst kc_cell;
     if constexpr (sizeof(T) == 8) kc_cell = stage_const<MODE>(I, ck, t_flux);
     const StageConst& kc = (sizeof(T) == 8) ? kc_cell : kc_block;
-    // beta_n of the stage update: in FP32 issued first so that the loads overlap the flux
-    // computation (FP64 loads them at the end: no registers to spare)
+    // beta_n of the stage update is loaded after the flux (no registers to hold it across; FP32
+    // requested its rows into L2 one plane ahead)
     constexpr bool UPD = (MODE == M_STAGE2 || MODE == M_STAGE3);
-    constexpr bool PRE = UPD && (sizeof(T) == 4);
-    T vn[UPD ? 9 : 1];
-    if constexpr (PRE) {
-        const T* un = cx.bn;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) vn[c] = (valid && kc.active) ? un[c * cells] : (T)0;
-    }
     const double* ld = kc.ld;
     // total stress at the cell: internal + applied load (FP64), symmetric
     T S[3][3];
@@ -512,10 +542,10 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         T s6[6];
         cp_async_wait_own();
 #pragma unroll
-        for (int c = 0; c < 6; ++c) s6[c] = ssm[c * ST_THREADS];
+        for (int c = 0; c < 6; ++c) s6[c] = ssm[c * st_threads<T>()];
         if (sig_next) {
 #pragma unroll
-            for (int c = 0; c < 6; ++c) cp_async_elem(ssm + c * ST_THREADS, sig_next + c * cells);
+            for (int c = 0; c < 6; ++c) cp_async_elem(ssm + c * st_threads<T>(), sig_next + c * cells);
             cp_async_commit();
         }
         if (MODE == M_STAGE1 && valid) {
@@ -525,7 +555,7 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             const double s3 = (double)s6[3], s4 = (double)s6[4], s5 = (double)s6[5];
             const double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
             const double tr = s0 + s3 + s5;
-            esum += sq - kc.cnu * tr * tr;
+            sums.energy(sq - kc.cnu * tr * tr, acc, st_threads<T>());
         }
         S[0][0] = (T)((double)s6[0] + ld[0]);
         S[1][1] = (T)((double)s6[3] + ld[1]);
@@ -816,20 +846,17 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
             T* o = cx.out;
 #pragma unroll
             for (int c = 0; c < 9; ++c) o[c * cells] = rhs[c];
-            double v = (double)spd;
-            if (!(v <= 1.0e300)) v = __longlong_as_double(0x7ff0000000000000LL);   // NaN/Inf -> +Inf
-            vmax = fmax(vmax, v);
-            zsum += (double)tv.center(8);   // mean b_zz of the step-start state
+            sums.speed(spd);
+            sums.bzz((double)tv.center(8), acc, st_threads<T>());   // mean b_zz of the step-start state
         }
     } else if constexpr (UPD) {
         if (valid && kc.active) {
             const T dt = (T)kc.dt;
             T* o = cx.out;
-            if constexpr (!PRE) {
-                const T* un = cx.bn;
+            T vn[9];
+            const T* un = cx.bn;
 #pragma unroll
-                for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
-            }
+            for (int c = 0; c < 9; ++c) vn[c] = un[c * cells];
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
                 T vs = tv.center(c);
@@ -859,6 +886,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
                                       double* __restrict__ bmax, double* __restrict__ bsum,
                                       int* __restrict__ status, const T* __restrict__ vac) {
     constexpr int RX = TileGeom<T>::RX, OX = TileGeom<T>::OX, PP = tile_pp<T>();
+    constexpr int TYS = TileGeom<T>::TY, RY = tile_ry<T>(), ST_THREADS = st_threads<T>();
     constexpr int NS = (ND == 3) ? TileGeom<T>::NS : 1;
     constexpr uint32_t PLANE_BYTES = 9u * PP * sizeof(T);
     const int nZ = (ND == 3) ? I.n0 : 1;
@@ -978,7 +1006,10 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
     __shared__ StageConst kc;   // FP32: read per cell from shared memory (keeps registers free)
     if (sizeof(T) == 4 && tid == 0) kc = stage_const<MODE>(I, clk[ii], t_flux);
     __syncthreads();
-    double vmax = 0.0, esum = 0.0, zsum = 0.0;
+    Stage1Acc<T> sums;
+    // FP32: this thread's FP64 sum slots after the stress slots
+    double* acc = reinterpret_cast<double*>(sm + NS * 9 * PP + 6 * ST_THREADS) + tid;
+    if (MODE == M_STAGE1) sums.start(acc, ST_THREADS);
     // this thread's cell in plane z0 (cell (z0, 0, 0) for threads outside the grid: in-bounds
     // loads, no stores)
     CellCtx<T> cx;
@@ -1027,7 +1058,16 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         } else {
             tv.so[2] = 0;
         }
-        stencil_cell<T, ND, MODE, VAR>(I, cx, own, tv, kc, clk[ii], t_flux, vmax, esum, zsum, sig, vac, ssm,
+        // FP32 stage updates read beta_n of their cell after the flux (no registers to hold it
+        // across): its rows of the next plane are requested into L2 now, one 128-byte row of 32
+        // cells per thread for the first 9 TYS threads (TMA-staged tiles lie inside the grid)
+        if constexpr (sizeof(T) == 4 && (MODE == M_STAGE2 || MODE == M_STAGE3)) {
+            if (use_tma && more && tid < 9 * TYS) {
+                const int c = tid / TYS, r = tid - c * TYS;
+                prefetch_l2(cx.bn + c * cells + plane + (long long)(r - ty) * nX - tx);
+            }
+        }
+        stencil_cell<T, ND, MODE, VAR>(I, cx, own, tv, kc, clk[ii], t_flux, sums, acc, sig, vac, ssm,
                                        more ? cx.sig + plane : nullptr);
         cx.sig += plane;
         if (cx.bn) cx.bn += plane;
@@ -1062,9 +1102,9 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
         return;
     }
     if (MODE == M_STAGE1) {
-        double m = block_reduce_max(vmax, red);
-        double es = block_reduce_sum(esum, red);
-        double zs = block_reduce_sum(zsum, red);
+        double m = block_reduce_max(sums.max_speed(), red);
+        double es = block_reduce_sum(sums.energy_sum(acc), red);
+        double zs = block_reduce_sum(sums.bzz_sum(acc, ST_THREADS), red);
         if (tid == 0) {
             bmax[blockIdx.x] = m;
             bsum[2 * blockIdx.x] = es;
@@ -1074,7 +1114,7 @@ __device__ __forceinline__ void march(const InstDev& I, int ii, int lb, T* sm, d
 }
 
 template <typename T, int MODE, int VAR>
-__global__ void __launch_bounds__(ST_THREADS, (sizeof(T) == 4) ? 3 : 2)
+__global__ void __launch_bounds__(st_threads<T>(), 2)
 k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__ pre,
           const T* __restrict__ bs, const T* bn, T* out, const T* __restrict__ sig,
           T* __restrict__ speed_out, const InstClock* __restrict__ clk, double t_flux,
@@ -1082,7 +1122,7 @@ k_stencil(const InstDev* __restrict__ insts, int n_inst, const int* __restrict__
           const T* __restrict__ vac, const __grid_constant__ StencilMapSet maps) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
-    __shared__ double red[ST_THREADS / 32];
+    __shared__ double red[st_threads<T>() / 32];
     __shared__ __align__(8) uint64_t bars[6];
     const int ii = find_instance(pre, n_inst, blockIdx.x);
     const InstDev& I = insts[ii];
@@ -1280,7 +1320,7 @@ static void stencil_dispatch(const PlanCore& P, int mode, const void* bs, const 
     // the plan has such instances
     const int var = (P.any_glide ? 1 : 0) | (P.any_vac ? 2 : 0);
 #define CDD_LAUNCH_V(M, V, SP)                                                                           \
-    k_stencil<T, M, V><<<L.blocks, ST_THREADS, L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP,     \
+    k_stencil<T, M, V><<<L.blocks, st_threads<T>(), L.smem, st>>>(P.d_inst, P.n_inst, L.d_pre, b, n, o, s, SP,     \
                                                              P.d_clock, t, P.d_bmax, P.d_bsum, P.d_status,    \
                                                              (const T*)P.d_vac, maps)
 #define CDD_LAUNCH_ST(M, SP)                                  \
@@ -1334,6 +1374,7 @@ cudaError_t launch_stencil(const PlanCore& P, int mode, const void* bs, const vo
 
 bool stencil_tma_eligible(const InstDev& I, int precision) {
     const int RX = precision == CDD_F32 ? TileGeom<float>::RX : TileGeom<double>::RX;
+    const int RY = precision == CDD_F32 ? tile_ry<float>() : tile_ry<double>();
     const int nX = (I.nd == 3) ? I.n2 : I.n1, nY = (I.nd == 3) ? I.n1 : I.n0;
     if (nX < RX || nY < RY) return false;
     if (precision == CDD_F32 && nX % 4) return false;   // 16-byte row strides
@@ -1365,6 +1406,7 @@ bool encode_stencil_maps(const PlanCore& P, const InstDev* insts, const void* ba
     const bool f32 = (P.precision == CDD_F32);
     const size_t elt = f32 ? sizeof(float) : sizeof(double);
     const cuuint32_t RX = f32 ? TileGeom<float>::RX : TileGeom<double>::RX;
+    const cuuint32_t RY = f32 ? tile_ry<float>() : tile_ry<double>();
     bool any = false;
     for (int i = 0; i < P.n_inst; ++i) {
         const InstDev& I = insts[i];
@@ -1454,24 +1496,27 @@ cudaError_t stencil_set_attributes(int precision, size_t smem) {
     return precision == CDD_F32 ? st_attr<float>(smem) : st_attr<double>(smem);
 }
 
-// The plane ring plus the 6 stress slots of every thread.
+// The plane ring plus the 6 stress slots of every thread (FP32: and its two FP64 sum slots).
 size_t stencil_smem_bytes(int precision, bool any3d) {
     if (precision == CDD_F32)
-        return ((size_t)(any3d ? TileGeom<float>::NS : 1) * 9 * tile_pp<float>() + 6 * ST_THREADS) * sizeof(float);
-    return ((size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() + 6 * ST_THREADS) * sizeof(double);
+        return ((size_t)(any3d ? TileGeom<float>::NS : 1) * 9 * tile_pp<float>() + 6 * st_threads<float>()) * sizeof(float) +
+               2 * st_threads<float>() * sizeof(double);
+    return ((size_t)(any3d ? TileGeom<double>::NS : 1) * 9 * tile_pp<double>() + 6 * st_threads<double>()) * sizeof(double);
 }
 
 // Blocks of the stencil: (x, y) tiles times chunks of planes along axis 0. Built-in rule: about
-// 1776 blocks (12 per SM) but at least 8 planes per block (each block first stages a 4-plane
-// halo, so shorter chunks spend most of their time on it); planes > 0 sets the chunk length.
-void stencil_geometry(InstDev& I, int planes) {
+// 227K threads (12 warps per SM) but at least 8 planes per block (each block first stages a
+// 4-plane halo, so shorter chunks spend most of their time on it); planes > 0 sets the chunk length.
+void stencil_geometry(InstDev& I, int precision, int planes) {
     const int nZ = (I.nd == 3) ? I.n0 : 1;
     const int nY = (I.nd == 3) ? I.n1 : I.n0;
     const int nX = (I.nd == 3) ? I.n2 : I.n1;
+    const int TYS = precision == CDD_F32 ? TileGeom<float>::TY : TileGeom<double>::TY;
     const int tiles = ((nX + TXS - 1) / TXS) * ((nY + TYS - 1) / TYS);
     int chunks = 1;
     if (I.nd == 3) {
-        chunks = (1776 + tiles - 1) / tiles;
+        const int target = 1776 * 4 / TYS;
+        chunks = (target + tiles - 1) / tiles;
         if (chunks > nZ / 8) chunks = nZ / 8;
         if (planes > 0) chunks = (nZ + planes - 1) / planes;
         if (chunks > nZ) chunks = nZ;
