@@ -63,10 +63,17 @@ class Rollout:
     sweep walks that segment backwards with cdd_step_adjoint straight away and re-runs each earlier
     segment from its checkpoint with records before walking it back. Nothing synchronises the host
     until the parameter cotangents are read at the end.
+
+    overlap (default): the re-run of the next segment back goes to a second CUDA stream with a
+    second plan of the same instance (its own scratch) and the other half of a double buffer of
+    records, so that it runs while the current segment is walked back on the caller's stream;
+    events order a segment's walk after its re-run and a buffer's reuse after the walk that read
+    it. The kernels and their inputs are those of the serial sweep (overlap=False), so the results
+    are bitwise the same.
     """
 
     def __init__(self, shape, mu, nu, rate_zz, dt, n_steps, precision="f32", checkpoint_every=20,
-                 t0=0.0, w_zz=10.0, Lambda=0.0, tuning=None):
+                 t0=0.0, w_zz=10.0, Lambda=0.0, tuning=None, overlap=True):
         self.shape = tuple(shape)
         self.mu, self.nu = float(mu), float(nu)
         self.rate_zz = None if rate_zz is None else float(rate_zz)
@@ -77,6 +84,9 @@ class Rollout:
         self.inst = Instance(self.shape, mu=self.mu, nu=self.nu, Lambda=Lambda, cfl=0.25, load_rate=load,
                              load_t0=self.t0)
         self.plan = Plan([self.inst], precision, tuning=tuning)
+        self.overlap = bool(overlap)
+        self.plan_rerun = None   # the overlapped sweep's second plan, made on its first use
+        self._side = None
         self.lib = self.plan.lib
         self.cells = int(np.prod(self.shape))
         self.checkpoints = {}
@@ -88,8 +98,9 @@ class Rollout:
         return self.t0 + n * self.dt
 
     # ------------------------------------------------------------------ forward
-    def _step(self, u, n, rec=None):
-        check(self.lib.cdd_step_record(self.plan.handle, _ptr(u), self.time(n), self.dt, _ptr(rec), _stream()))
+    def _step(self, u, n, rec=None, plan=None, stream=None):
+        plan = self.plan if plan is None else plan
+        check(self.lib.cdd_step_record(plan.handle, _ptr(u), self.time(n), self.dt, _ptr(rec), _stream(stream)))
 
     def forward(self, beta0):
         """Run n_steps from beta0 (packed field, plan dtype); returns (u_N, loss as float)."""
@@ -127,15 +138,17 @@ class Rollout:
         return out
 
     # ------------------------------------------------------------------ reverse
-    def _record_buffer(self, k):
-        if self._records is None or self._records.shape[0] < k:
+    def _record_buffer(self, k, half=0):
+        """k step records (256-byte aligned); half 1 is the second buffer of the overlapped sweep."""
+        nb = 2 if self.overlap else 1
+        if self._records is None or self._records.shape[0] < nb * k:
             el = torch.tensor([], dtype=self.plan.dtype).element_size()
             pad = 256 // el
-            raw = torch.empty(k * self.rec_elems + pad, dtype=self.plan.dtype, device=self.plan.device)
+            raw = torch.empty(nb * k * self.rec_elems + pad, dtype=self.plan.dtype, device=self.plan.device)
             off = (-raw.data_ptr() % 256) // el
             self._raw = raw
-            self._records = raw[off:off + k * self.rec_elems].view(k, self.rec_elems)
-        return self._records
+            self._records = raw[off:off + nb * k * self.rec_elems].view(nb * k, self.rec_elems)
+        return self._records[half * k:(half + 1) * k]
 
     def _record_parts(self, rec):
         """Views of the states u, F0, F1 inside a record (the first three 256-byte aligned parts)."""
@@ -165,17 +178,20 @@ class Rollout:
             (sE.double() * p.stress_view(s_nu, 0).double()).sum()
         # reverse sweep over checkpoint segments
         pbar = torch.zeros(_lib.CDD_PBAR, dtype=torch.float64, device=p.device)
-        recs = self._record_buffer(self.K)
-        for s0 in sorted(self.checkpoints, reverse=True):
-            s1 = min(s0 + self.K, self.n_steps)
-            if s0 != self._tail:
-                v = self.checkpoints[s0].clone()
-                for n in range(s0, s1):
-                    self._step(v, n, recs[n - s0])
-            self._tail = None
-            for n in range(s1 - 1, s0 - 1, -1):
-                check(self.lib.cdd_step_adjoint(p.handle, _ptr(recs[n - s0]), self.time(n), self.dt, _ptr(ub),
-                                                _ptr(pbar), _stream()))
+        if self.overlap:
+            self._sweep_overlapped(ub, pbar)
+        else:
+            recs = self._record_buffer(self.K)
+            for s0 in sorted(self.checkpoints, reverse=True):
+                s1 = min(s0 + self.K, self.n_steps)
+                if s0 != self._tail:
+                    v = self.checkpoints[s0].clone()
+                    for n in range(s0, s1):
+                        self._step(v, n, recs[n - s0])
+                self._tail = None
+                for n in range(s1 - 1, s0 - 1, -1):
+                    check(self.lib.cdd_step_adjoint(p.handle, _ptr(recs[n - s0]), self.time(n), self.dt, _ptr(ub),
+                                                    _ptr(pbar), _stream()))
         pb = pbar.cpu().numpy()
         lamb = 2.0 * mu * nu / (1.0 - 2.0 * nu)
         dlam = 2.0 * mu / (1.0 - 2.0 * nu) ** 2
@@ -191,7 +207,63 @@ class Rollout:
             grads["nu"] += float(Lt @ (dlam * rate.sum() * np.ones(3)))
             grads["rate_zz"] += float(Lt @ (lamb * CZZ.sum() + 2.0 * mu * CZZ))
         p.check_status()
+        if self.plan_rerun is not None:
+            self.plan_rerun.check_status()
         return ub, grads
+
+
+    def _sweep_overlapped(self, ub, pbar):
+        """Reverse sweep with the re-run of segment i + 1 (next one back) on a side stream while
+        segment i is walked back on the current stream. Segment i uses record buffer i % 2."""
+        p = self.plan
+        main = torch.cuda.current_stream(p.device)
+        if self.plan_rerun is None:
+            # the re-runs: same instance and launch shapes, separate scratch
+            self.plan_rerun = Plan([self.inst], p.precision, tuning=[p.tuning(0)])
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=p.device)
+        side = self._side
+        segs = sorted(self.checkpoints, reverse=True)
+        start = torch.cuda.Event()
+        start.record(main)          # the forward, checkpoints and loss terms are in main's order
+        side.wait_event(start)
+        ready, walked = {}, {}
+        held = []                   # re-run states, kept until the sweep ends (side-stream work)
+
+        def rerun(i):
+            s0 = segs[i]
+            s1 = min(s0 + self.K, self.n_steps)
+            recs = self._record_buffer(self.K, i % 2)
+            with torch.cuda.stream(side):
+                if i - 2 in walked:
+                    side.wait_event(walked[i - 2])   # buffer i % 2 was read by segment i - 2
+                v = self.checkpoints[s0].clone()
+                held.append(v)
+                for n in range(s0, s1):
+                    self._step(v, n, recs[n - s0], plan=self.plan_rerun, stream=side)
+                ev = torch.cuda.Event()
+                ev.record(side)
+            ready[i] = ev
+
+        if segs and segs[0] != self._tail:
+            rerun(0)
+        self._tail = None
+        for i, s0 in enumerate(segs):
+            if i + 1 < len(segs):
+                rerun(i + 1)
+            if i in ready:
+                main.wait_event(ready[i])
+            s1 = min(s0 + self.K, self.n_steps)
+            recs = self._record_buffer(self.K, i % 2)
+            for n in range(s1 - 1, s0 - 1, -1):
+                check(self.lib.cdd_step_adjoint(p.handle, _ptr(recs[n - s0]), self.time(n), self.dt, _ptr(ub),
+                                                _ptr(pbar), _stream(main)))
+            ev = torch.cuda.Event()
+            ev.record(main)
+            walked[i] = ev
+        # every side-stream re-run precedes a walk on main, so main's order now covers all of them;
+        # the re-run states (side-stream allocations) return to the side stream's pool
+        del held
 
 
 class RolloutLoss(torch.autograd.Function):
