@@ -264,6 +264,48 @@ def test_tma_staged_planes_against_oracle(shape, load):
     plan.check_status()
 
 
+@pytest.mark.parametrize("shape,load", [((12, 40, 72), None), ((10, 20, 64), (-0.025, -0.025, 0.05)),
+                                        ((8, 18, 48), (-0.025, -0.025, 0.05)), ((6, 12, 40), None),
+                                        ((18, 48), None), ((36, 64), (-0.025, -0.025, 0.05))])
+def test_tma_staged_planes_fp32_against_oracle(shape, load):
+    """The FP32 stencil's TMA plane path (32 x 8 tiles of 256 threads): edge tiles, partial last
+    tiles in x and y (y 20, 18, 12 and 36 are not multiples of 8: the last tile is shifted back
+    inside the grid), 2-D grids, and the stage updates whose beta_n rows are prefetched into L2,
+    against the FP64 oracle (FP32 rounding: 5e-6 rel-L2); a batch of the shapes equals the single
+    plans bitwise."""
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 33)
+    p = O.Params(mu=1.0, nu=0.3, load_rate=load)
+    plan = cdd.Plan([cdd.Instance(shape, load_rate=load)], "f32")
+    beta = plan.pack([b0])
+    rhs, speed = plan.flux(beta, 0.0)
+    ref_rhs, ref_speed = O.full_flux(b0, 0.0, p)
+    torch.cuda.synchronize()
+    assert rel(plan.field_view(rhs, 0).cpu().numpy().astype(np.float64), ref_rhs) < 5e-6
+    assert rel(speed.cpu().numpy().reshape(shape).astype(np.float64), ref_speed) < 5e-6
+    plan.set_time(0.0, 1e30)
+    plan.step(beta)
+    ref, _ = O.rk3_step(b0, 0.0, 1e30, p)
+    assert rel(plan.field_view(beta, 0).cpu().numpy().astype(np.float64), ref) < 5e-6
+    plan.check_status()
+
+
+def test_fp32_tma_batch_of_partial_tiles_equals_single_plans():
+    shapes = [(10, 20, 64), (8, 18, 48), (18, 48), (6, 12, 40)]
+    fields = [cdd.gaussian_random_field(s, 0.06, 0.05, 50 + i) for i, s in enumerate(shapes)]
+    insts = [cdd.Instance(s, load_rate=(-0.025, -0.025, 0.05)) for s in shapes]
+    batch = cdd.Plan(insts, "f32")
+    bb = batch.pack(fields)
+    batch.set_time(0.0, 1e30)
+    batch.run(bb, 3, graph=False)
+    batch.check_status()
+    for i in range(len(shapes)):
+        single = cdd.Plan([insts[i]], "f32")
+        bs = single.pack([fields[i]])
+        single.set_time(0.0, 1e30)
+        single.run(bs, 3, graph=False)
+        assert torch.equal(batch.field_view(bb, i), single.field_view(bs, 0)), i
+
+
 def test_tma_fp32_matches_fp64_and_batch_mixes_paths():
     """FP32 TMA path against FP64, and a batch mixing TMA-staged and thread-staged instances."""
     shapes = [(16, 24, 80), (12, 12, 12), (32, 32)]
