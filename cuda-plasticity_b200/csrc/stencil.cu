@@ -342,26 +342,48 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
     for (int d = 0; d < ND; ++d)
 #pragma unroll
         for (int l = 0; l < 3; ++l) Q[d][l] = z2;
+    if constexpr (ND == 3) {
+        // pair m = 2 sx + sy; T_m = w V over its two corners (lanes: sz). Q_z = sum_m T_m lane-wise,
+        // Q_x = lane sums of (T_0 + T_1, T_2 + T_3), Q_y = lane sums of (T_0 + T_2, T_1 + T_3)
+        float2 w2[4];
 #pragma unroll
-    for (int m = 0; m < NC / 2; ++m) {
-        const int c = 2 * m;
-        int sg[2];
-        sg[0] = (c >> (ND - 1)) & 1;
-        sg[1] = (ND == 3) ? ((c >> 1) & 1) : 0;
-        float wb = 1.0f;
-#pragma unroll
-        for (int d = 0; d < ND - 1; ++d) wb *= (sg[d] == 0) ? wm[d] : wp[d];
-        const float2 w2 = f2(wb * wm[ND - 1], wb * wp[ND - 1]);
+        for (int m = 0; m < 4; ++m) {
+            const float wb = ((m >> 1) ? wp[0] : wm[0]) * ((m & 1) ? wp[1] : wm[1]);
+            w2[m] = f2(wb * wm[2], wb * wp[2]);
+        }
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-            const float2 wv = __fmul2_rn(w2, V[m][l]);
-            const float sum = wv.x + wv.y;
+            float2 T4[4];
 #pragma unroll
-            for (int d = 0; d < ND - 1; ++d) {
-                if (sg[d] == 0) Q[d][l].x += sum;
-                else Q[d][l].y += sum;
+            for (int m = 0; m < 4; ++m) T4[m] = __fmul2_rn(w2[m], V[m][l]);
+            const float2 a01 = __fadd2_rn(T4[0], T4[1]), a23 = __fadd2_rn(T4[2], T4[3]);
+            const float2 b02 = __fadd2_rn(T4[0], T4[2]), b13 = __fadd2_rn(T4[1], T4[3]);
+            Q[0][l] = f2(a01.x + a01.y, a23.x + a23.y);
+            Q[1 % ND][l] = f2(b02.x + b02.y, b13.x + b13.y);
+            Q[2 % ND][l] = __fadd2_rn(a01, a23);
+        }
+    } else {
+#pragma unroll
+        for (int m = 0; m < NC / 2; ++m) {
+            const int c = 2 * m;
+            int sg[2];
+            sg[0] = (c >> (ND - 1)) & 1;
+            sg[1] = (ND == 3) ? ((c >> 1) & 1) : 0;
+            float wb = 1.0f;
+#pragma unroll
+            for (int d = 0; d < ND - 1; ++d) wb *= (sg[d] == 0) ? wm[d] : wp[d];
+            const float2 w2 = f2(wb * wm[ND - 1], wb * wp[ND - 1]);
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                const float2 wv = __fmul2_rn(w2, V[m][l]);
+                const float sum = wv.x + wv.y;
+#pragma unroll
+                for (int d = 0; d < ND - 1; ++d) {
+                    if (sg[d] == 0) Q[d][l].x += sum;
+                    else Q[d][l].y += sum;
+                }
+                Q[ND - 1][l] = __fadd2_rn(Q[ND - 1][l], wv);
             }
-            Q[ND - 1][l] = __fadd2_rn(Q[ND - 1][l], wv);
         }
     }
 
@@ -448,6 +470,7 @@ struct StageConst {
     double ld[3];
     double dt;
     double cnu;   // nu / (1 + nu) of the elastic energy density (|sigma|^2 - cnu tr^2) / (4 mu)
+    float cnu_f;  // the same rounded to FP32 (the FP32 form's per-cell density)
     bool active;
 };
 
@@ -460,6 +483,7 @@ __device__ __forceinline__ StageConst stage_const(const InstDev& I, const InstCl
     applied_load(I, tload, k.ld);
     k.dt = ck.dt;
     k.cnu = I.nu / (1.0 + I.nu);
+    k.cnu_f = (float)k.cnu;
     k.active = ck.active != 0;
     return k;
 }
@@ -550,12 +574,21 @@ __device__ __forceinline__ void stencil_cell(const InstDev& I, const CellCtx<T>&
         }
         if (MODE == M_STAGE1 && valid) {
             // observables of the step-start state: elastic energy of the internal stress (k_dt
-            // applies 1 / (4 mu) to the instance sum)
-            const double s0 = (double)s6[0], s1 = (double)s6[1], s2 = (double)s6[2];
-            const double s3 = (double)s6[3], s4 = (double)s6[4], s5 = (double)s6[5];
-            const double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
-            const double tr = s0 + s3 + s5;
-            sums.energy(sq - kc.cnu * tr * tr, acc, st_threads<T>());
+            // applies 1 / (4 mu) to the instance sum). FP32 forms the cell's density in FP32 (its
+            // stress is FP32; sq >= tr^2 / 3 > cnu tr^2, so nothing cancels) and adds it to the FP64
+            // sum; FP64 in FP64.
+            if constexpr (sizeof(T) == 4) {
+                const float d = fmaf(s6[0], s6[0], fmaf(s6[3], s6[3], s6[5] * s6[5]));
+                const float o = fmaf(s6[1], s6[1], fmaf(s6[2], s6[2], s6[4] * s6[4]));
+                const float tr = s6[0] + s6[3] + s6[5];
+                sums.energy((double)fmaf(-kc.cnu_f, tr * tr, fmaf(2.0f, o, d)), acc, st_threads<T>());
+            } else {
+                const double s0 = (double)s6[0], s1 = (double)s6[1], s2 = (double)s6[2];
+                const double s3 = (double)s6[3], s4 = (double)s6[4], s5 = (double)s6[5];
+                const double sq = s0 * s0 + s3 * s3 + s5 * s5 + 2.0 * (s1 * s1 + s2 * s2 + s4 * s4);
+                const double tr = s0 + s3 + s5;
+                sums.energy(sq - kc.cnu * tr * tr, acc, st_threads<T>());
+            }
         }
         S[0][0] = (T)((double)s6[0] + ld[0]);
         S[1][1] = (T)((double)s6[3] + ld[1]);
