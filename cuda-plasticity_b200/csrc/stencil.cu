@@ -193,6 +193,17 @@ __device__ __forceinline__ float2 derivs5_f2(const float* v, float ih) {
     return __fmul2_rn(__ffma2_rn(f2(dd0, ddm), f2(-0.5f, -0.5f), P), f2(ih, -ih));
 }
 __device__ __forceinline__ float lane(const float2& v, int s) { return s ? v.y : v.x; }
+// Maximum / minimum that return NaN when either argument is NaN (fmaxf / fminf drop it).
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+    float d;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fmin_nan(float a, float b) {
+    float d;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
 
 template <int ND, bool GLIDE>
 __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih, const float (&S)[3][3],
@@ -264,7 +275,23 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
 
     // corners: V = (A_x[sx] + A_y[sy] (+ A_z[sz])) / |rho|, paired along the last axis
     float2 V[NC / 2][3];
-    float2 vs2 = z2;   // NaN anywhere in V (fmax/fmin would drop it) must reach the CFL maximum
+    if constexpr (ND == 3 && !GLIDE) {
+        // pair m = 2 sx + sy, lanes sz = 0, 1: the x and y parts of |rho|^2 and of A are common to
+        // the pair, the z parts come as pairs
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int sx = m >> 1, sy = m & 1;
+            const float cr = (float)ME + lane(Pq[0], sx) + lane(Pq[1 % ND], sy) - 2.0f * Cp[0][sx][sy];
+            const float2 cz = f2(Cp[1 % NP][sy][0] + Cp[2 % NP][0][sx], Cp[1 % NP][sy][1] + Cp[2 % NP][1][sx]);
+            const float2 r2 = __ffma2_rn(cz, f2(-2.0f, -2.0f), __fadd2_rn(f2(cr, cr), Pq[2 % ND]));
+            const float2 inv2 = f2(inv_sqrt(r2.x), inv_sqrt(r2.y));
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                const float ca = lane(A[0][l], sx) + lane(A[1 % ND][l], sy);
+                V[m][l] = __fmul2_rn(__fadd2_rn(f2(ca, ca), A[2 % ND][l]), inv2);
+            }
+        }
+    } else {
 #pragma unroll
     for (int m = 0; m < NC / 2; ++m) {
         float av[2][3], inv[2];
@@ -307,13 +334,12 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
             }
         }
 #pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            V[m][l] = __fmul2_rn(f2(av[0][l], av[1][l]), f2(inv[0], inv[1]));
-            vs2 = __fadd2_rn(vs2, V[m][l]);
-        }
+        for (int l = 0; l < 3; ++l) V[m][l] = __fmul2_rn(f2(av[0][l], av[1][l]), f2(inv[0], inv[1]));
+    }
     }
     // one-sided speeds a+_d = max(0, max V_d), a-_d = -min(0, min V_d); weights normalised by
-    // tot_d = a+_d + a-_d + ME first (the product of the three totals can underflow FP32)
+    // tot_d = a+_d + a-_d + ME first (the product of the three totals can underflow FP32). The
+    // maxima and minima propagate NaN, so that a NaN anywhere in V reaches the CFL speed.
     float pp[ND], pm[ND], wm[ND], wp[ND];
     spd = 0.0f;
 #pragma unroll
@@ -321,8 +347,8 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
         float mx = 0.0f, mn = 0.0f;
 #pragma unroll
         for (int m = 0; m < NC / 2; ++m) {
-            mx = fmaxf(mx, fmaxf(V[m][d].x, V[m][d].y));
-            mn = fminf(mn, fminf(V[m][d].x, V[m][d].y));
+            mx = fmax_nan(mx, fmax_nan(V[m][d].x, V[m][d].y));
+            mn = fmin_nan(mn, fmin_nan(V[m][d].x, V[m][d].y));
         }
         pp[d] = mx;
         pm[d] = -mn;
@@ -332,8 +358,6 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
         wm[d] = pm[d] * it;
         wp[d] = pp[d] * it;
     }
-    const float vsum = vs2.x + vs2.y;
-    if (vsum != vsum) spd = vsum;
 
     // Q^s_dl = sum over corners with s_d = s of w_c V_cl (w_c: product of the weights a-_d / tot_d
     // or a+_d / tot_d of the corner's signs)
