@@ -204,6 +204,17 @@ __device__ __forceinline__ float fmin_nan(float a, float b) {
     asm("min.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
     return d;
 }
+// The same over three arguments in one instruction (three-input min / max, sm_100).
+__device__ __forceinline__ float fmax3_nan(float a, float b, float c) {
+    float d;
+    asm("max.NaN.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3_nan(float a, float b, float c) {
+    float d;
+    asm("min.NaN.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 
 template <int ND, bool GLIDE>
 __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih, const float (&S)[3][3],
@@ -345,10 +356,18 @@ __device__ __forceinline__ void flux_f32(const TileView<float, ND>& tv, float ih
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
         float mx = 0.0f, mn = 0.0f;
+        if constexpr (ND == 3) {
+            // the 8 corners and 0 in four three-input operations each way
+            mx = fmax3_nan(fmax3_nan(V[0][d].x, V[0][d].y, V[1][d].x), fmax3_nan(V[1][d].y, V[2][d].x, V[2][d].y),
+                           fmax3_nan(V[3][d].x, V[3][d].y, 0.0f));
+            mn = fmin3_nan(fmin3_nan(V[0][d].x, V[0][d].y, V[1][d].x), fmin3_nan(V[1][d].y, V[2][d].x, V[2][d].y),
+                           fmin3_nan(V[3][d].x, V[3][d].y, 0.0f));
+        } else {
 #pragma unroll
-        for (int m = 0; m < NC / 2; ++m) {
-            mx = fmax_nan(mx, fmax_nan(V[m][d].x, V[m][d].y));
-            mn = fmin_nan(mn, fmin_nan(V[m][d].x, V[m][d].y));
+            for (int m = 0; m < NC / 2; ++m) {
+                mx = fmax_nan(mx, fmax_nan(V[m][d].x, V[m][d].y));
+                mn = fmin_nan(mn, fmin_nan(V[m][d].x, V[m][d].y));
+            }
         }
         pp[d] = mx;
         pm[d] = -mn;
