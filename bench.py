@@ -527,23 +527,25 @@ def main():
 
     # ---------------- end to end: host buffers through the public API ----------------
     # every step copies its input in from pinned host memory and its result back (cdd.HostPipeline:
-    # the copies of neighbouring steps overlap the computation on separate streams)
+    # the copies of neighbouring steps overlap the computation on separate streams; three device
+    # fields, so that the copy-in of step k + 1 need not wait for the copy-out of step k - 1)
+    D = 3
     host_in = torch.empty(p32.field_elems, dtype=torch.float32, pin_memory=True)
     host_in.copy_(b0.reshape(-1).to(torch.float32).cpu())
-    host_outs = [torch.empty_like(host_in, pin_memory=True) for _ in range(2)]
+    host_outs = [torch.empty_like(host_in, pin_memory=True) for _ in range(D)]
     p32.set_time(0.0, 1e30)
-    pipe = cdd.HostPipeline(p32, depth=2)
+    pipe = cdd.HostPipeline(p32, depth=D)
     Ke = max(3, K)
-    for k in range(2):
-        pipe.step(host_in, host_outs[k % 2])
+    for k in range(D):
+        pipe.step(host_in, host_outs[k % D])
     pipe.synchronize()
     barrier()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev0.record(pipe.s_in)
     for k in range(Ke):
-        if k >= 2:
-            pipe.wait(pipe.count - 2)          # its host output buffer is about to be reused
-        last = pipe.step(host_in, host_outs[k % 2])
+        if k >= D:
+            pipe.wait(pipe.count - D)          # its host output buffer is about to be reused
+        last = pipe.step(host_in, host_outs[k % D])
     ev1 = torch.cuda.Event(enable_timing=True)
     ev1.record(pipe.s_out)                     # after the last copy-out (stream order)
     pipe.synchronize()

@@ -10,8 +10,8 @@ import cdd
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_pipeline_matches_serial_steps(prec):
+@pytest.mark.parametrize("prec,depth", [("f32", 2), ("f64", 2), ("f32", 3)])
+def test_pipeline_matches_serial_steps(prec, depth):
     from cdd.initial import gaussian_random_field
     shape = (32, 32, 32)
     inst = cdd.Instance(shape, load_rate=(-0.025, -0.025, 0.05))
@@ -29,7 +29,7 @@ def test_pipeline_matches_serial_steps(prec):
         want.append(buf.cpu().clone())
     plan = cdd.Plan([inst], prec)
     plan.set_time(0.0, 1e30)
-    pipe = cdd.HostPipeline(plan, depth=2)
+    pipe = cdd.HostPipeline(plan, depth=depth)
     outs = [torch.empty_like(h).pin_memory() for h in inputs]
     for h, o in zip(inputs, outs):
         pipe.step(h, o)
