@@ -29,11 +29,11 @@ UNIT = "cell-stage updates/s"
 WORDS_PER_CELL_STAGE = 48      # stress operator: read 9 + write 6; stencil + stage: read 24, write 9
 STRESS_WORDS = 15               # stress operator: read beta 9, write sigma 6
 FLUX_WORDS = 24                 # stencil, flux form: read beta 9 + sigma 6, write rhs 9
-FLUX_TRAFFIC_BYTES_PER_CELL = 93.0    # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
+FLUX_TRAFFIC_BYTES_PER_CELL = 94.9    # DRAM bytes per cell of the flux-form stencil (ncu, 192^3)
 # executed FP32 operations (add + mul + 2 fma, packed pairs counted per lane) and warp instructions
 # per cell of the FP32 flux-form stencil, from ncu's instruction counters at 192^3
-FLUX_FLOP_PER_CELL = 1338.2
-FLUX_WARP_INST_PER_CELL = 43.44
+FLUX_FLOP_PER_CELL = 1308.6
+FLUX_WARP_INST_PER_CELL = 39.60
 FLUX_COUNTS_SOURCE = "profiles/k_stencil_flux_192cube_fp32.md"
 
 
