@@ -551,10 +551,28 @@ def main():
     pipe.synchronize()
     barrier()
     ele = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    # the PCIe floor of that loop: the same copies alone, both directions at once on the pipeline's
+    # copy streams (no steps)
+    bufs = pipe.bufs
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(pipe.s_in)
+    pipe.s_out.wait_event(c0)
+    for k in range(Ke):
+        with torch.cuda.stream(pipe.s_in):
+            bufs[k % D].copy_(host_in, non_blocking=True)
+        with torch.cuda.stream(pipe.s_out):
+            host_outs[k % D].copy_(bufs[(k + 1) % D], non_blocking=True)
+    pipe.s_in.wait_stream(pipe.s_out)
+    c1.record(pipe.s_in)
+    torch.cuda.synchronize()
+    copies_ms = c0.elapsed_time(c1) / Ke
     e2e = {"value": world * cells * 3 * Ke / ele, "unit": UNIT,
            "h2d_bytes_per_step": host_in.numel() * 4, "d2h_bytes_per_step": host_outs[0].numel() * 4,
-           "path": "cdd.HostPipeline: cdd.Plan.step on a field copied in from pinned host memory and "
-                   "copied back every step, copies overlapped with the neighbouring steps' computation"}
+           "ms_per_step": 1e3 * ele / Ke, "copies_only_ms_per_step": copies_ms,
+           "pcie_gb_s_each_way": host_in.numel() * 4 / copies_ms / 1e6,
+           "path": "cdd.HostPipeline (3 device fields): cdd.Plan.step on a field copied in from pinned host "
+                   "memory and copied back every step, copies overlapped with the neighbouring steps' "
+                   "computation; copies_only = the same copies with no steps (the PCIe floor)"}
     del pipe
     clk = clocks.stop()
 
