@@ -203,11 +203,14 @@ def test_end_time_reached_then_inactive():
     assert torch.equal(before, beta)
 
 
-def test_nonfinite_state_is_reported_and_not_applied():
-    shape = (12, 12, 12)
+@pytest.mark.parametrize("prec,shape", [("f64", (12, 12, 12)), ("f32", (12, 12, 12)), ("f32", (8, 16, 48)),
+                                        ("f64", (8, 16, 48)), ("f32", (16, 48))])
+def test_nonfinite_state_is_reported_and_not_applied(prec, shape):
+    """A NaN in the field reaches the CFL maximum (FP32: through the NaN-propagating corner-speed
+    extremes) on thread-staged and TMA-staged planes: the step is not applied."""
     b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 3)
-    b0[4, 3, 3, 3] = np.nan
-    plan = cdd.Plan([cdd.Instance(shape)], "f64")
+    b0[(4,) + tuple(3 for _ in shape)] = np.nan
+    plan = cdd.Plan([cdd.Instance(shape)], prec)
     beta = plan.pack([b0])
     before = beta.clone()
     plan.set_time(0.0, 1e30)
@@ -217,6 +220,24 @@ def test_nonfinite_state_is_reported_and_not_applied():
     assert ei.value.code == 4
     assert torch.equal(torch.nan_to_num(before, nan=7.0), torch.nan_to_num(beta, nan=7.0))
     plan.check_status()   # cleared
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_nonfinite_stress_gives_nonfinite_speed(prec):
+    """A NaN in the stress handed to the flux makes the corner velocities of that cell NaN; its CFL
+    speed comes back non-finite and the other cells' speeds stay finite."""
+    shape = (8, 16, 48)
+    b0 = cdd.gaussian_random_field(shape, 0.06, 0.05, 5)
+    plan = cdd.Plan([cdd.Instance(shape)], prec)
+    beta = plan.pack([b0])
+    s6 = plan.stress(beta)
+    plan.stress_view(s6, 0)[1, 2, 5, 7] = float("nan")
+    _, speed = plan.flux(beta, 0.0, sigma=s6)
+    sp = speed.reshape(shape).cpu().numpy()
+    assert not np.isfinite(sp[2, 5, 7])
+    mask = np.ones(shape, dtype=bool)
+    mask[2, 5, 7] = False
+    assert np.isfinite(sp[mask]).all()
 
 
 def test_fp32_form_error_against_fp64():
