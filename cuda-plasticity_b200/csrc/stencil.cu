@@ -1613,8 +1613,9 @@ size_t stencil_smem_bytes(int precision, bool any3d) {
 }
 
 // Blocks of the stencil: (x, y) tiles times chunks of planes along axis 0. Built-in rule: about
-// 227K threads (12 warps per SM) but at least 8 planes per block (each block first stages a
-// 4-plane halo, so shorter chunks spend most of their time on it); planes > 0 sets the chunk length.
+// 227K threads in all (1776 blocks of 128 threads, 888 of 256) but at least 8 planes per block (each
+// block first stages a 4-plane halo, so shorter chunks spend most of their time on it); planes > 0
+// sets the chunk length.
 void stencil_geometry(InstDev& I, int precision, int planes) {
     const int nZ = (I.nd == 3) ? I.n0 : 1;
     const int nY = (I.nd == 3) ? I.n1 : I.n0;
