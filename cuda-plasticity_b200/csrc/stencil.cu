@@ -547,7 +547,7 @@ template <typename T> struct CellCtx {
 
 // Stage-1 observables of a thread's cells: the CFL speed maximum (NaN and Inf map to +Inf) and
 // the FP64 sums of the elastic energy density and of b_zz. FP64 keeps all three in registers.
-// FP32 (255 registers per thread would cost resident warps) keeps the maximum as a float (a
+// FP32 (its 256-thread tiles run at most 128 registers per thread) keeps the maximum as a float (a
 // maximum of floats is exact) and the two FP64 sums in this thread's two shared-memory slots
 // (`acc`, `acc + ST_THREADS`), so that nothing of them stays in registers across the march.
 template <typename T> struct Stage1Acc {
@@ -1006,7 +1006,7 @@ __device__ __forceinline__ void patch_box_edges(T* dst, const BoxGeomT<T>& g, in
 }
 
 // Out-of-line copies: FP64 calls these (its march is at the 255-register limit, and keeping the
-// rarely run staging code out of it removes most of its spills: 22.3 -> 21.5 ms per 256^3 step);
+// rarely run staging code out of it removes most of its spills: 22.3 -> 21.7 ms per 256^3 step);
 // FP32 inlines them (out of line measured 3% slower there).
 template <typename T> __device__ __noinline__ void stage_box_ool(T* dst, BoxGeomT<T> g, int zp, bool all) {
     stage_box<T>(dst, g, zp, all);
